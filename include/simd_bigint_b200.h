@@ -1,0 +1,105 @@
+/* simd_bigint_b200.h -- C ABI of the B200 large-operand multiplication path.
+ *
+ * Numbers are little-endian arrays of uint64_t limbs passed as pointer plus
+ * length, exactly as in the reference library (iamstupid/simd_bigint).
+ * Products are bit-exact: they are the integer products, computed by a
+ * five-prime number-theoretic transform on the GPU followed by Garner CRT and
+ * carry resolution, with no floating point anywhere.
+ *
+ * Two families of entry points:
+ *
+ *  1. Context entries (sbg_*): pointers are DEVICE memory; work is queued on
+ *     the context's CUDA stream and the call returns without waiting.  They
+ *     return a status code: SBG_OK (0) or one of the SBG_E* codes below.
+ *     NOTE the inversion against the reference, whose entries return 1 on
+ *     success and 0 on failure.  Errors detected on the device (carry scan
+ *     timeout, spill check) are sticky and reported by sbg_ctx_sync().
+ *
+ *  2. Reference-signature drop-ins (sbg_nt_mul, sbg_nt_sqr, ...): same
+ *     argument order, meaning and return convention as the reference
+ *     (1 = success, 0 = failure / out of band).  Pointers may be host or
+ *     device memory (classified with cudaPointerGetAttributes); the call is
+ *     synchronous and runs on a per-thread default context of the current
+ *     CUDA device.
+ *
+ * rp must not overlap the inputs (reference include/u64cvt.h:92-93).  Zero
+ * high limbs are allowed and are treated as values.  Transform band: one
+ * product may have an + bn - 1 <= 2^25 limbs (any shape inside that), which
+ * covers 2^24 x 2^24; sizes beyond return SBG_EBAND (drop-ins: 0).
+ */
+#ifndef SIMD_BIGINT_B200_H
+#define SIMD_BIGINT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    SBG_OK = 0,
+    SBG_EINVAL = 1,    /* bad argument (length <= 0, an < bn for mulmid, NULL) */
+    SBG_EBAND = 2,     /* beyond the transform band (an + bn - 1 > 2^25)      */
+    SBG_EALLOC = 3,    /* device allocation failed                             */
+    SBG_ECUDA = 4,     /* a CUDA runtime call failed                           */
+    SBG_ETIMEOUT = 5,  /* a bounded device-side wait expired                   */
+    SBG_ESPILL = 6,    /* the product spilled past its top limb (internal)     */
+    SBG_EADMIT = 7,    /* serving: request rejected by admission control       */
+    SBG_ENODEV = 8     /* no CUDA device / library built without device code  */
+};
+
+typedef struct sbg_ctx sbg_ctx;
+
+/* ---- context ------------------------------------------------------------
+ * A context owns one CUDA stream, the twiddle tables of every transform length
+ * used so far, and the device workspace (it replaces the reference's
+ * scratch* argument: include/ntmul.h:47 nt_mul_r, include/scratch.h:293-324).
+ */
+int sbg_ctx_create(int device, sbg_ctx **out);
+void sbg_ctx_destroy(sbg_ctx *ctx);
+/* Use an external cudaStream_t (NULL: the context's own stream). */
+int sbg_ctx_set_stream(sbg_ctx *ctx, void *cuda_stream);
+void *sbg_ctx_get_stream(sbg_ctx *ctx);
+/* Wait for queued work; returns and clears any sticky device-side error. */
+int sbg_ctx_sync(sbg_ctx *ctx);
+/* Build tables and size the workspace for products up to total_limbs limbs
+ * (an + bn), so later calls neither allocate nor generate tables. */
+int sbg_ctx_reserve(sbg_ctx *ctx, int64_t total_limbs);
+const char *sbg_strerror(int status);
+/* Largest an + bn accepted by one product (2^25 + 1). */
+int64_t sbg_max_total_limbs(void);
+
+/* ---- device-pointer entries ---------------------------------------------- */
+
+/* rp[0 .. an+bn) = {ap, an} * {bp, bn}.
+ * Replaces nt_mul / nt_mul_r (reference include/ntmul.h:47-75, 71). */
+int sbg_mul(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an, const uint64_t *bp,
+            int64_t bn);
+
+/* rp[0 .. 2an) = {ap, an}^2.
+ * Replaces nt_sqr / nt_sqr_r (reference include/ntmul.h:60-80). */
+int sbg_sqr(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an);
+
+/* Middle product, GMP mpn_mulmid convention: an >= bn >= 1, writes an-bn+3
+ * limbs  rp = sum_{bn-1 <= i+j <= an-1} ap[i] * bp[j] * 2^(64 (i+j-(bn-1))).
+ * Specification: reference bench/recip_mulmid_ref.c:11-16 and
+ * include/mulmid.h:5-18 (the reference has no library implementation). */
+int sbg_mulmid(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an, const uint64_t *bp,
+               int64_t bn);
+
+/* ---- reference-signature drop-ins ---------------------------------------- */
+
+/* int nt_mul(uint64_t *rp, const uint64_t *ap, ptrdiff_t an,
+ *            const uint64_t *bp, ptrdiff_t bn)   -- reference include/ntmul.h:71 */
+int sbg_nt_mul(uint64_t *rp, const uint64_t *ap, ptrdiff_t an, const uint64_t *bp, ptrdiff_t bn);
+
+/* int nt_sqr(uint64_t *rp, const uint64_t *ap, ptrdiff_t an)
+ *                                                  -- reference include/ntmul.h:77 */
+int sbg_nt_sqr(uint64_t *rp, const uint64_t *ap, ptrdiff_t an);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIMD_BIGINT_B200_H */

@@ -1,0 +1,214 @@
+"""simd_bigint_b200 -- B200 (sm_100a) large-operand multiplication for
+mpn-style little-endian uint64 limb arrays.
+
+The product is the native library ``_lib/libsimd_bigint_b200.so`` (C ABI,
+``include/simd_bigint_b200.h``).  This module is a thin ctypes host layer
+over it for Python callers, tests and the benchmark: it mirrors the
+reference's entry points (``nt_mul``, ``nt_sqr``; include/ntmul.h:71-80) with
+the same argument order and meaning, and exposes the context (stream +
+workspace) API for device-resident operands held in torch tensors.
+
+There is no CPU fallback: if the library or a CUDA device is missing, the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import build as _build
+
+__all__ = [
+    "SbgError", "lib", "Context", "nt_mul", "nt_sqr", "mpn_mulmid", "STATUS",
+]
+
+STATUS = {
+    0: "SBG_OK", 1: "SBG_EINVAL", 2: "SBG_EBAND", 3: "SBG_EALLOC", 4: "SBG_ECUDA",
+    5: "SBG_ETIMEOUT", 6: "SBG_ESPILL", 7: "SBG_EADMIT", 8: "SBG_ENODEV",
+}
+
+_lib = None
+_u64p = C.POINTER(C.c_uint64)
+_vp = C.c_void_p
+_i64 = C.c_int64
+
+
+class SbgError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, status)} ({status})")
+
+
+def lib_path() -> Path:
+    return _build.lib_path()
+
+
+def lib(build_if_missing: bool = False):
+    """Load the native library (raises if it is not built)."""
+    global _lib
+    if _lib is None:
+        path = lib_path()
+        if not path.exists():
+            if not build_if_missing:
+                raise FileNotFoundError(f"native library missing: {path} (run python -m simd_bigint_b200.build)")
+            _build.build()
+        L = C.CDLL(str(path))
+        L.sbg_ctx_create.argtypes = [C.c_int, C.POINTER(_vp)]
+        L.sbg_ctx_create.restype = C.c_int
+        L.sbg_ctx_destroy.argtypes = [_vp]
+        L.sbg_ctx_destroy.restype = None
+        L.sbg_ctx_set_stream.argtypes = [_vp, _vp]
+        L.sbg_ctx_set_stream.restype = C.c_int
+        L.sbg_ctx_get_stream.argtypes = [_vp]
+        L.sbg_ctx_get_stream.restype = _vp
+        L.sbg_ctx_sync.argtypes = [_vp]
+        L.sbg_ctx_sync.restype = C.c_int
+        L.sbg_ctx_reserve.argtypes = [_vp, _i64]
+        L.sbg_ctx_reserve.restype = C.c_int
+        L.sbg_strerror.argtypes = [C.c_int]
+        L.sbg_strerror.restype = C.c_char_p
+        L.sbg_max_total_limbs.argtypes = []
+        L.sbg_max_total_limbs.restype = _i64
+        for name in ("sbg_mul", "sbg_mulmid"):
+            getattr(L, name).argtypes = [_vp, _vp, _vp, _i64, _vp, _i64]
+            getattr(L, name).restype = C.c_int
+        L.sbg_sqr.argtypes = [_vp, _vp, _vp, _i64]
+        L.sbg_sqr.restype = C.c_int
+        L.sbg_nt_mul.argtypes = [_vp, _vp, C.c_ssize_t, _vp, C.c_ssize_t]
+        L.sbg_nt_mul.restype = C.c_int
+        L.sbg_nt_sqr.argtypes = [_vp, _vp, C.c_ssize_t]
+        L.sbg_nt_sqr.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _check(st: int, what: str):
+    if st != 0:
+        raise SbgError(st, what)
+
+
+def _dptr(t) -> int:
+    """Device address of a torch tensor (int64/uint64 limbs) or a raw int."""
+    if isinstance(t, int):
+        return t
+    if not t.is_cuda:
+        raise ValueError("device entry points need CUDA tensors")
+    if not t.is_contiguous():
+        raise ValueError("limb tensors must be contiguous")
+    return t.data_ptr()
+
+
+class Context:
+    """One CUDA stream + twiddle plans + device workspace (the reference's
+    scratch* argument, include/ntmul.h:47).  Device entry points queue work on
+    the context's stream and return immediately; sync() waits and raises any
+    sticky device-side error."""
+
+    def __init__(self, device: int = 0, stream=None):
+        self._L = lib()
+        h = _vp()
+        _check(self._L.sbg_ctx_create(device, C.byref(h)), "sbg_ctx_create")
+        self.handle = h
+        self.device = device
+        if stream is not None:
+            self.set_stream(stream)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._L.sbg_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream):
+        """stream: a torch.cuda.Stream, a raw cudaStream_t int, or None."""
+        raw = getattr(stream, "cuda_stream", stream)
+        _check(self._L.sbg_ctx_set_stream(self.handle, raw), "sbg_ctx_set_stream")
+
+    @property
+    def stream(self) -> int:
+        return self._L.sbg_ctx_get_stream(self.handle) or 0
+
+    def sync(self):
+        _check(self._L.sbg_ctx_sync(self.handle), "sbg_ctx_sync")
+
+    def reserve(self, total_limbs: int):
+        _check(self._L.sbg_ctx_reserve(self.handle, int(total_limbs)), "sbg_ctx_reserve")
+
+    # device entries (torch CUDA tensors of 64-bit limbs, or raw addresses)
+    def mul(self, r, a, b, an: int | None = None, bn: int | None = None):
+        an = a.numel() if an is None else an
+        bn = b.numel() if bn is None else bn
+        _check(self._L.sbg_mul(self.handle, _dptr(r), _dptr(a), an, _dptr(b), bn), "sbg_mul")
+
+    def sqr(self, r, a, an: int | None = None):
+        an = a.numel() if an is None else an
+        _check(self._L.sbg_sqr(self.handle, _dptr(r), _dptr(a), an), "sbg_sqr")
+
+    def mulmid(self, r, a, b, an: int | None = None, bn: int | None = None):
+        an = a.numel() if an is None else an
+        bn = b.numel() if bn is None else bn
+        _check(self._L.sbg_mulmid(self.handle, _dptr(r), _dptr(a), an, _dptr(b), bn), "sbg_mulmid")
+
+
+def _np_u64(x) -> np.ndarray:
+    return np.ascontiguousarray(x, dtype=np.uint64)
+
+
+def nt_mul(rp: np.ndarray, ap: np.ndarray, an: int, bp: np.ndarray, bn: int) -> int:
+    """Reference-signature multiply (include/ntmul.h:71): rp[0..an+bn) =
+    {ap,an} * {bp,bn} on host arrays; returns 1 on success, 0 on failure."""
+    for arr in (rp, ap, bp):
+        if not (isinstance(arr, np.ndarray) and arr.dtype == np.uint64 and arr.flags.c_contiguous):
+            raise TypeError("nt_mul wants contiguous uint64 numpy arrays")
+    if len(rp) < an + bn:
+        raise ValueError("rp too short")
+    return lib().sbg_nt_mul(rp.ctypes.data, ap.ctypes.data, an, bp.ctypes.data, bn)
+
+
+def nt_sqr(rp: np.ndarray, ap: np.ndarray, an: int) -> int:
+    """Reference-signature square (include/ntmul.h:77)."""
+    for arr in (rp, ap):
+        if not (isinstance(arr, np.ndarray) and arr.dtype == np.uint64 and arr.flags.c_contiguous):
+            raise TypeError("nt_sqr wants contiguous uint64 numpy arrays")
+    if len(rp) < 2 * an:
+        raise ValueError("rp too short")
+    return lib().sbg_nt_sqr(rp.ctypes.data, ap.ctypes.data, an)
+
+
+def mul(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Host convenience: returns {a} * {b} as len(a)+len(b) limbs."""
+    a, b = _np_u64(a), _np_u64(b)
+    r = np.zeros(len(a) + len(b), dtype=np.uint64)
+    if not nt_mul(r, a, len(a), b, len(b)):
+        raise SbgError(2, "nt_mul")
+    return r
+
+
+def sqr(a: np.ndarray) -> np.ndarray:
+    a = _np_u64(a)
+    r = np.zeros(2 * len(a), dtype=np.uint64)
+    if not nt_sqr(r, a, len(a)):
+        raise SbgError(2, "nt_sqr")
+    return r
+
+
+def mpn_mulmid(ctx: Context, a, b):
+    """Device middle product of torch tensors; returns a new tensor of
+    len(a)-len(b)+3 limbs (GMP mpn_mulmid convention)."""
+    import torch
+    r = torch.empty(a.numel() - b.numel() + 3, dtype=torch.int64, device=a.device)
+    ctx.mulmid(r, a, b)
+    return r

@@ -1,0 +1,336 @@
+// sbg_capi.cu -- the C ABI: contexts, plans, workspace, and the mul / sqr /
+// mulmid entry points (include/simd_bigint_b200.h).
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/simd_bigint_b200.h"
+#include "sbg_internal.h"
+
+using namespace sbg;
+
+struct sbg_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    uint2* tw_f = nullptr;          // master tables [q][2^12]
+    uint2* tw_i = nullptr;
+    LenPlan plans[SBG_MAX_LG + 1];
+    uint32_t* ws = nullptr;         // transform workspace (u32 words)
+    size_t ws_cap = 0;
+    uint32_t* flags = nullptr;      // carry look-back flags
+    size_t flags_cap = 0;
+    uint32_t* err = nullptr;        // sticky device error bits
+    // staging for the host-pointer drop-ins
+    uint64_t* d_stage = nullptr;
+    size_t stage_cap = 0;
+};
+
+static int cuda_fail(cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return SBG_OK;
+    if (getenv("SBG_DEBUG")) fprintf(stderr, "sbg: %s: %s\n", where, cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) return SBG_EALLOC;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return SBG_ENODEV;
+    return SBG_ECUDA;
+}
+#define CK(call)                                            \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+static int lg_ceil(int64_t n) {
+    int l = 0;
+    while (((int64_t)1 << l) < n) ++l;
+    return l;
+}
+
+// Transform length for a convolution whose wanted coefficients need L >= need.
+static int conv_lg(int64_t need) {
+    int l = lg_ceil(need);
+    return l < 4 ? 4 : l;
+}
+
+static int ensure_plan(sbg_ctx* c, int lgL) {
+    LenPlan* lp = &c->plans[lgL];
+    if (lp->lgL == lgL) return SBG_OK;
+    LenPlan np;
+    np.lgL = lgL;
+    if (lgL <= 12) {
+        np.lgN1 = 0;
+        np.lgN2 = lgL;
+    } else {
+        np.lgN2 = 12;
+        np.lgN1 = lgL - 12;
+        np.hi_n = 1 << (lgL - 13);
+        size_t lo_b = (size_t)SBG_NP * 8192 * sizeof(uint2);
+        size_t hi_b = (size_t)SBG_NP * np.hi_n * sizeof(uint2);
+        CK(cudaMalloc(&np.fs_lo_f, lo_b));
+        CK(cudaMalloc(&np.fs_lo_i, lo_b));
+        CK(cudaMalloc(&np.fs_hi_f, hi_b));
+        CK(cudaMalloc(&np.fs_hi_i, hi_b));
+        CK(gen_len_tables(&np, c->stream));
+    }
+    for (int q = 0; q < SBG_NP; ++q) np.scale[q] = host_scale(lgL, q);
+    *lp = np;
+    return SBG_OK;
+}
+
+static int ensure_ws(sbg_ctx* c, size_t words, size_t flag_words) {
+    if (words > c->ws_cap) {
+        CK(cudaStreamSynchronize(c->stream));
+        if (c->ws) cudaFree(c->ws);
+        c->ws = nullptr;
+        c->ws_cap = 0;
+        CK(cudaMalloc(&c->ws, words * sizeof(uint32_t)));
+        c->ws_cap = words;
+    }
+    if (flag_words > c->flags_cap) {
+        CK(cudaStreamSynchronize(c->stream));
+        if (c->flags) cudaFree(c->flags);
+        c->flags = nullptr;
+        c->flags_cap = 0;
+        size_t fw = flag_words < 4096 ? 4096 : flag_words;
+        CK(cudaMalloc(&c->flags, fw * sizeof(uint32_t)));
+        c->flags_cap = fw;
+    }
+    return SBG_OK;
+}
+
+// One windowed convolution: the limbs [off, off + nout) of
+// sum_{cmin <= j <= cmax} c_j 2^(64 j) where c = a * b (cyclic length 2^lgL).
+static int run_conv(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, const uint64_t* bp,
+                    int64_t bn, int sq, int lgL, int64_t cmin, int64_t cmax, int64_t off,
+                    int64_t nout) {
+    if (lgL > SBG_MAX_LG) return SBG_EBAND;
+    int st = ensure_plan(c, lgL);
+    if (st) return st;
+    st = ensure_ws(c, ws_words(lgL, sq), carry_flag_words(nout));
+    if (st) return st;
+    const LenPlan* lp = &c->plans[lgL];
+    CK(launch_conv(ap, an, bp, bn, sq, lgL, lp, c->tw_f, c->tw_i, c->ws, c->stream));
+    CK(launch_crt_carry(c->ws, lgL, lp, cmin, cmax, off, rp, nout, c->flags, c->err, c->stream));
+    return SBG_OK;
+}
+
+extern "C" {
+
+const char* sbg_strerror(int status) {
+    switch (status) {
+        case SBG_OK: return "ok";
+        case SBG_EINVAL: return "invalid argument";
+        case SBG_EBAND: return "operands beyond the transform band";
+        case SBG_EALLOC: return "device allocation failed";
+        case SBG_ECUDA: return "CUDA runtime error";
+        case SBG_ETIMEOUT: return "bounded device wait expired";
+        case SBG_ESPILL: return "product spilled past its top limb";
+        case SBG_EADMIT: return "request rejected by admission control";
+        case SBG_ENODEV: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+int64_t sbg_max_total_limbs(void) { return ((int64_t)1 << SBG_MAX_LG) + 1; }
+
+int sbg_ctx_create(int device, sbg_ctx** out) {
+    if (!out) return SBG_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return SBG_ENODEV;
+    if (device < 0 || device >= ndev) return SBG_EINVAL;
+    CK(cudaSetDevice(device));
+    sbg_ctx* c = new sbg_ctx();
+    c->device = device;
+    int st = SBG_OK;
+    do {
+        if ((st = cuda_fail(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking),
+                            "stream")))
+            break;
+        c->stream = c->own_stream;
+        if ((st = cuda_fail(set_kernel_attributes(), "attributes"))) break;
+        if ((st = cuda_fail(upload_constants(c->stream), "constants"))) break;
+        size_t tb = (size_t)SBG_NP * (1 << 12) * sizeof(uint2);
+        if ((st = cuda_fail(cudaMalloc(&c->tw_f, tb), "tw_f"))) break;
+        if ((st = cuda_fail(cudaMalloc(&c->tw_i, tb), "tw_i"))) break;
+        if ((st = cuda_fail(gen_master_tables(c->tw_f, c->tw_i, c->stream), "tables"))) break;
+        if ((st = cuda_fail(cudaMalloc(&c->err, sizeof(uint32_t)), "err"))) break;
+        if ((st = cuda_fail(cudaMemsetAsync(c->err, 0, sizeof(uint32_t), c->stream), "err0")))
+            break;
+        if ((st = cuda_fail(cudaStreamSynchronize(c->stream), "sync"))) break;
+    } while (0);
+    if (st) {
+        sbg_ctx_destroy(c);
+        return st;
+    }
+    *out = c;
+    return SBG_OK;
+}
+
+void sbg_ctx_destroy(sbg_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (int l = 0; l <= SBG_MAX_LG; ++l) {
+        LenPlan* lp = &c->plans[l];
+        cudaFree(lp->fs_lo_f);
+        cudaFree(lp->fs_lo_i);
+        cudaFree(lp->fs_hi_f);
+        cudaFree(lp->fs_hi_i);
+    }
+    cudaFree(c->tw_f);
+    cudaFree(c->tw_i);
+    cudaFree(c->ws);
+    cudaFree(c->flags);
+    cudaFree(c->err);
+    cudaFree(c->d_stage);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+int sbg_ctx_set_stream(sbg_ctx* c, void* stream) {
+    if (!c) return SBG_EINVAL;
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return SBG_OK;
+}
+
+void* sbg_ctx_get_stream(sbg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int sbg_ctx_sync(sbg_ctx* c) {
+    if (!c) return SBG_EINVAL;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    uint32_t h = 0;
+    CK(cudaMemcpy(&h, c->err, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h) {
+        CK(cudaMemset(c->err, 0, sizeof(uint32_t)));
+        if (h & 1u) return SBG_ETIMEOUT;
+        if (h & 2u) return SBG_ESPILL;
+        return SBG_ECUDA;
+    }
+    return SBG_OK;
+}
+
+int sbg_ctx_reserve(sbg_ctx* c, int64_t total) {
+    if (!c || total < 2) return SBG_EINVAL;
+    if (total - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
+    CK(cudaSetDevice(c->device));
+    int lg = conv_lg(total - 1);
+    for (int l = 4; l <= lg; ++l) {
+        int st = ensure_plan(c, l);
+        if (st) return st;
+    }
+    int st = ensure_ws(c, ws_words(lg, 0), carry_flag_words(total));
+    if (st) return st;
+    CK(cudaStreamSynchronize(c->stream));
+    return SBG_OK;
+}
+
+int sbg_mul(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, const uint64_t* bp,
+            int64_t bn) {
+    if (!c || !rp || !ap || !bp || an <= 0 || bn <= 0) return SBG_EINVAL;
+    if (an + bn - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
+    CK(cudaSetDevice(c->device));
+    int lgL = conv_lg(an + bn - 1);
+    return run_conv(c, rp, ap, an, bp, bn, 0, lgL, 0, an + bn - 2, 0, an + bn);
+}
+
+int sbg_sqr(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an) {
+    if (!c || !rp || !ap || an <= 0) return SBG_EINVAL;
+    if (2 * an - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
+    CK(cudaSetDevice(c->device));
+    int lgL = conv_lg(2 * an - 1);
+    return run_conv(c, rp, ap, an, ap, an, 1, lgL, 0, 2 * an - 2, 0, 2 * an);
+}
+
+int sbg_mulmid(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, const uint64_t* bp,
+               int64_t bn) {
+    if (!c || !rp || !ap || !bp || bn <= 0 || an < bn) return SBG_EINVAL;
+    if (an > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
+    CK(cudaSetDevice(c->device));
+    // the wanted coefficients [bn-1, an-1] are untouched by wrap-around once L >= an
+    int lgL = conv_lg(an);
+    return run_conv(c, rp, ap, an, bp, bn, 0, lgL, bn - 1, an - 1, bn - 1, an - bn + 3);
+}
+
+// ---- reference-signature drop-ins -----------------------------------------
+
+static std::mutex g_ctx_mu;
+static sbg_ctx* g_ctx[64];
+
+static sbg_ctx* default_ctx() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> g(g_ctx_mu);
+    if (!g_ctx[dev]) {
+        sbg_ctx* c = nullptr;
+        if (sbg_ctx_create(dev, &c) != SBG_OK) return nullptr;
+        g_ctx[dev] = c;
+    }
+    return g_ctx[dev];
+}
+
+static bool is_device_ptr(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static int ensure_stage(sbg_ctx* c, size_t limbs) {
+    if (limbs > c->stage_cap) {
+        CK(cudaStreamSynchronize(c->stream));
+        cudaFree(c->d_stage);
+        c->d_stage = nullptr;
+        c->stage_cap = 0;
+        CK(cudaMalloc(&c->d_stage, limbs * sizeof(uint64_t)));
+        c->stage_cap = limbs;
+    }
+    return SBG_OK;
+}
+
+// host-or-device mul/sqr through the default context; synchronous
+static int dropin(uint64_t* rp, const uint64_t* ap, int64_t an, const uint64_t* bp, int64_t bn,
+                  int sq) {
+    if (!rp || !ap || an <= 0 || (!sq && (!bp || bn <= 0))) return 0;
+    sbg_ctx* c = default_ctx();
+    if (!c) return 0;
+    std::lock_guard<std::mutex> g(g_ctx_mu);
+    bool dev = is_device_ptr(rp) && is_device_ptr(ap) && (sq || is_device_ptr(bp));
+    int st;
+    if (dev) {
+        st = sq ? sbg_sqr(c, rp, ap, an) : sbg_mul(c, rp, ap, an, bp, bn);
+    } else {
+        int64_t nb = sq ? 0 : bn;
+        size_t tot = (size_t)an + (size_t)nb + (size_t)(an + (sq ? an : bn));
+        if (ensure_stage(c, tot) != SBG_OK) return 0;
+        uint64_t* da = c->d_stage;
+        uint64_t* db = da + an;
+        uint64_t* dr = db + nb;
+        if (cudaMemcpyAsync(da, ap, an * 8, cudaMemcpyDefault, c->stream) != cudaSuccess) return 0;
+        if (!sq && cudaMemcpyAsync(db, bp, bn * 8, cudaMemcpyDefault, c->stream) != cudaSuccess)
+            return 0;
+        st = sq ? sbg_sqr(c, dr, da, an) : sbg_mul(c, dr, da, an, db, bn);
+        if (st == SBG_OK) {
+            size_t outl = (size_t)an + (size_t)(sq ? an : bn);
+            if (cudaMemcpyAsync(rp, dr, outl * 8, cudaMemcpyDefault, c->stream) != cudaSuccess)
+                return 0;
+        }
+    }
+    if (st != SBG_OK) return 0;
+    return sbg_ctx_sync(c) == SBG_OK ? 1 : 0;
+}
+
+int sbg_nt_mul(uint64_t* rp, const uint64_t* ap, ptrdiff_t an, const uint64_t* bp, ptrdiff_t bn) {
+    return dropin(rp, ap, (int64_t)an, bp, (int64_t)bn, 0);
+}
+
+int sbg_nt_sqr(uint64_t* rp, const uint64_t* ap, ptrdiff_t an) {
+    return dropin(rp, ap, (int64_t)an, nullptr, 0, 1);
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+// sbg_internal.h -- host-side declarations shared by the CUDA translation
+// units of the library (kernel launchers, plan tables, constants).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+
+#include "sbg_arith.cuh"
+
+namespace sbg {
+
+// A (w, shoup) pair as stored in device tables.
+struct ShoupPair {
+    uint32_t w, ws;
+};
+
+// Garner / compose constants (ascending primes).
+struct CrtConst {
+    // ppm[i][k] = (p_0 * ... * p_{k-1}) mod p_i, k = 1..i-1 (Shoup pairs)
+    uint32_t ppm[SBG_NP][SBG_NP];
+    uint32_t ppms[SBG_NP][SBG_NP];
+    // inv[i] = (p_0 * ... * p_{i-1})^-1 mod p_i
+    uint32_t inv[SBG_NP];
+    uint32_t invs[SBG_NP];
+};
+
+// Per-transform-length plan: the four-step twiddle tables (device) and the
+// CRT scale 2^32 * L^-1 mod p (host-side Shoup pairs passed by value).
+struct LenPlan {
+    int lgL = -1;
+    int lgN1 = 0, lgN2 = 0;       // column / row sizes (lgN1 = 0: single-CTA)
+    uint2* fs_lo_f = nullptr;     // [q][8192]      w_L^e, e < 2^13
+    uint2* fs_hi_f = nullptr;     // [q][L >> 13]   w_L^(e << 13)
+    uint2* fs_lo_i = nullptr;
+    uint2* fs_hi_i = nullptr;
+    int hi_n = 0;                 // entries in each hi table
+    ShoupPair scale[SBG_NP];
+};
+
+// Kernel-argument bundle for the four-step twiddles.
+struct FsTables {
+    const uint2* lo;   // + q * 8192
+    const uint2* hi;   // + q * hi_n
+    int hi_n;
+};
+
+struct ScaleArg {
+    uint32_t w[SBG_NP];
+    uint32_t ws[SBG_NP];
+};
+
+// one product / middle product of the batch engine
+struct ConvJob {
+    const uint64_t* a;
+    const uint64_t* b;      // == a for squaring
+    uint64_t* out;
+    int64_t an, bn;
+    int64_t cmin, cmax;     // coefficient window that contributes
+    int64_t off;            // out[m] = limb (m + off) of the window sum
+    int64_t nout;           // limbs written
+    int sq;
+    int lgL;
+};
+
+// ---- host helpers (sbg_plan.cu) ----
+uint32_t host_powmod(uint64_t a, uint64_t e, uint32_t p);
+uint32_t host_shoup(uint32_t w, uint32_t p);
+void host_prime_consts(PrimeConst out[SBG_NP]);
+void host_crt_consts(CrtConst* out);
+ShoupPair host_scale(int lgL, int q);
+
+// ---- launchers (sbg_kernels.cu) ----
+cudaError_t upload_constants(cudaStream_t st);
+cudaError_t set_kernel_attributes();
+cudaError_t gen_master_tables(uint2* tw_f, uint2* tw_i, cudaStream_t st);
+cudaError_t gen_len_tables(LenPlan* lp, cudaStream_t st);
+
+// Whole product through the transform pipeline.  Workspace `ws` must hold
+// ws_words(lgL) u32.  `err` is a device word that receives sticky error bits.
+size_t ws_words(int lgL, int sq);
+cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_t bn, int sq,
+                        int lgL, const LenPlan* lp, const uint2* tw_f, const uint2* tw_i,
+                        uint32_t* ws, cudaStream_t st);
+// CRT + carry of residues R (5 x L u32) into out[0..nout): out[m] = limb (m + off)
+// of sum_{cmin <= j <= cmax} c_j * 2^(64 j).
+cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int64_t cmin,
+                             int64_t cmax, int64_t off, uint64_t* out, int64_t nout,
+                             uint32_t* flags, uint32_t* err, cudaStream_t st);
+size_t carry_flag_words(int64_t nout);
+
+}  // namespace sbg
