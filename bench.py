@@ -1,0 +1,454 @@
+#!/usr/bin/env python3
+"""Benchmark of the large-operand multiply path (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mul2p24|sqr2p24|mul2p22|mul2p24x2p20|mul16k]
+
+A step is one product of the workload on one GPU (replicas across ranks: the
+path shards by instance, with no collective).  `value` is product limbs
+(an + bn) per second over all ranks with operands resident in HBM, timed with
+CUDA events on the library's stream; `e2e` is the same through the
+reference-signature C entry (sbg_nt_mul) on pinned HOST buffers, copies in
+and out inside the timed region.  The roofline names the dominant kernel,
+its algorithmic bytes and butterflies per launch divided by its average
+CUDA-event duration.  `cpu_baseline` times the reference's own nt_mul
+(compiled from its sources into oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: (op, an, bn)
+    "mul2p24": ("mul", 1 << 24, 1 << 24),
+    "sqr2p24": ("sqr", 1 << 24, 1 << 24),
+    "mul2p22": ("mul", 1 << 22, 1 << 22),
+    "mul2p24x2p20": ("mul", 1 << 24, 1 << 20),
+    "mul16k": ("mul", 16384, 16384),
+}
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def lg_ceil(n: int) -> int:
+    return max(4, (n - 1).bit_length())
+
+
+def kernel_model(op: str, an: int, bn: int) -> dict:
+    """Algorithmic HBM bytes and radix-2 butterflies per launch of each kernel
+    (5 primes x 4-byte residues per spectrum point)."""
+    sq = op == "sqr"
+    need = an + bn - 1
+    lgL = lg_ceil(need)
+    L = 1 << lgL
+    N = an + bn
+    nops = 1 if sq else 2
+    if lgL <= 12:
+        return {"k_small": {"bytes": 8 * (an + (0 if sq else bn)) + 20 * L,
+                            "bfly": 5 * (nops + 1) * (L // 2) * lgL}}
+    lgN1, lgN2 = lgL - 12, 12
+    limbs_in = an + (0 if sq else bn)
+    return {
+        "k_col_fwd": {"bytes": 8 * limbs_in + 20 * L * nops, "bfly": 5 * nops * (L // 2) * lgN1},
+        "k_row": {"bytes": 20 * L * (nops + 1), "bfly": 5 * (nops + 1) * (L // 2) * lgN2},
+        "k_col_inv": {"bytes": 40 * L, "bfly": 5 * (L // 2) * lgN1},
+        "k_crt_carry": {"bytes": 20 * L + 8 * N, "bfly": 0},
+    }
+
+
+def measured_peaks() -> tuple[float, str]:
+    try:
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms in the background."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.file = None
+        self.marks = []
+
+    def start(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def mark(self, tag: str):
+        self.marks.append((tag, time.time()))
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        self.proc.wait(timeout=5)
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[3], parts[4:]))
+            except ValueError:
+                continue
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [r for r in rows if r[2] not in ("[N/A]",)]
+        sm = [r[0] for r in load] or [r[0] for r in rows]
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for nm, v in zip(names[1:], r[3][1:]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        top = sorted(sm)[len(sm) // 2:]   # the upper half: samples taken under load
+        return {"sm_mhz": statistics.median(top), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=None)
+        pg = dist
+    return ws, rank, local, pg
+
+
+def barrier_max(pg, value: float, device) -> float:
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_inputs(an: int, bn: int, seed: int):
+    rng = np.random.default_rng(seed)
+    a = rng.integers(0, 2**64, size=an, dtype=np.uint64)
+    b = rng.integers(0, 2**64, size=bn, dtype=np.uint64)
+    a[-1] |= np.uint64(1)
+    b[-1] |= np.uint64(1)
+    return a, b
+
+
+# ------------------------------------------------------------- CPU baseline --
+def cpu_threads_for(an: int, bn: int, want: int | None = None, cap: int = 64) -> int:
+    cores = min(os.cpu_count() or 1, cap)
+    try:
+        avail = 0
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable"):
+                avail = int(line.split()[1]) * 1024
+    except OSError:
+        avail = 8 << 30
+    per = 140 * (an + bn) + (1 << 28)          # reference p50 working set per thread (~4.2 GB at 2^25)
+    t = max(1, min(cores, int(avail * 0.6 // per)))
+    if want:
+        t = min(t, want)
+    return t
+
+
+def _cpu_worker(op, an, bn, seed, steps, warmup, barrier, queue):
+    """One baseline process: its own inputs, its own reference plan (built in
+    the warm-up), then `steps` timed products between barriers."""
+    try:
+        from oracle import oracle as O
+        use_ref = O.ref_available()
+        a, b = make_inputs(an, bn, seed)
+        f = (lambda: O.ref_sqr(a)) if (use_ref and op == "sqr") else \
+            (lambda: O.ref_mul(a, b)) if use_ref else \
+            (lambda: O.port_sqr(a)) if op == "sqr" else (lambda: O.port_mul(a, b))
+        t0 = time.time()
+        for _ in range(max(1, warmup)):
+            f()
+        plan_s = time.time() - t0
+        times = []
+        for _ in range(steps):
+            barrier.wait(timeout=3600)
+            t = time.perf_counter()
+            f()
+            times.append(time.perf_counter() - t)
+        queue.put(("ok", plan_s, times))
+    except Exception as e:  # reported to the parent
+        try:
+            barrier.abort()
+        except Exception:
+            pass
+        queue.put(("err", repr(e), []))
+
+
+def cpu_run(op: str, an: int, bn: int, procs: int, steps: int, warmup: int, seed: int = 7) -> dict:
+    """The reference's own nt_mul / nt_sqr (oracle/_ref; the C restatement
+    where the reference cannot run on this host) on `procs` single-threaded
+    processes started with spawn, one independent product per process per
+    step, all processes released together at every step.
+
+    Processes, not pthreads: the reference's per-thread scratch arena is
+    MADV_HUGEPAGE-backed and several threads of one process faulting it in
+    serialise on the address-space lock (2^22 products: 0.74 s on one thread,
+    146 s per step on four threads of one process on this container), while
+    separate processes scale."""
+    import multiprocessing as mp
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs)
+    queue = ctx.Queue()
+    ps = [ctx.Process(target=_cpu_worker, args=(op, an, bn, seed + i, steps, warmup, barrier, queue))
+          for i in range(procs)]
+    for p in ps:
+        p.start()
+    res = [queue.get(timeout=7200) for _ in ps]
+    for p in ps:
+        p.join(timeout=60)
+    errs = [r[1] for r in res if r[0] != "ok"]
+    if errs:
+        raise RuntimeError("CPU baseline failed: " + errs[0])
+    plan_s = max(r[1] for r in res)
+    # per step: all processes ran one product concurrently; the step ends when
+    # the slowest one does
+    step_times = [max(r[2][k] for r in res) for k in range(steps)]
+    step = statistics.median(step_times)
+    cpu = O.host_cpu()
+    isa = [f for f in O.REF_ISA if f in cpu["flags"]]
+    return {"value": procs * (an + bn) / step / 1e6, "unit": "Mlimb/s", "cores": procs,
+            "kind": kind, "step_s": step,
+            "sample": f"{procs} single-threaded process(es) x one {op} {an}x{bn} per step, median of "
+                      f"{steps} steps (step = slowest process) after {max(1, warmup)} warm-up "
+                      f"(plan build {plan_s:.1f}s, excluded)",
+            "cpu_model": cpu["model"], "host_cores": cpu["cores"], "isa": isa}
+
+
+def cpu_bounded(op: str, an: int, bn: int) -> dict:
+    """Bounded CPU sample for the default run: a few steps on all usable cores."""
+    threads = cpu_threads_for(an, bn, want=int(os.environ.get("SBG_CPU_THREADS", "0")) or None, cap=32)
+    return cpu_run(op, an, bn, threads, steps=2, warmup=1)
+
+
+# ------------------------------------------------------------- our arm -----
+def run_ours(args, ws, rank, local, pg) -> dict | None:
+    import torch
+
+    import simd_bigint_b200 as sbg
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    op, an, bn = WORKLOADS[args.workload]
+    a, b = make_inputs(an, bn, 1000 + rank)
+    ta = torch.from_numpy(a.view(np.int64)).to(dev)
+    tb = torch.from_numpy(b.view(np.int64)).to(dev)
+    tr = torch.empty(an + bn, dtype=torch.int64, device=dev)
+    ctx = sbg.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream)
+    ctx.reserve(an + bn)
+
+    def step():
+        if op == "sqr":
+            ctx.sqr(tr, ta)
+        else:
+            ctx.mul(tr, ta, tb)
+
+    clocks = ClockSampler(local)
+    if rank == 0:
+        clocks.start()
+    for _ in range(args.warmup):
+        step()
+    ctx.sync()
+    # bit-exactness of what is timed: spot check of the warm-up product
+    from oracle import oracle as O
+    got = tr.cpu().numpy().view(np.uint64)
+    qs = [2305843009213693951, 2305843009213693921]
+    bb = a if op == "sqr" else b
+    exact = all((O.mod_u64(a, q) * O.mod_u64(bb, q)) % q == O.mod_u64(got, q) for q in qs)
+
+    # ---- device-timed region (operands resident in HBM) ----
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clocks.mark("timed")
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    ms_total = barrier_max(pg, e0.elapsed_time(e1), dev)
+    ms_step = ms_total / args.steps
+
+    # ---- per-kernel CUDA-event timing (separate pass, same stream) ----
+    ctx.set_timing(True)
+    ctx.kernel_times()
+    for _ in range(args.steps):
+        step()
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+
+    # ---- end to end through the C entry on pinned host buffers ----
+    ha = torch.from_numpy(a.view(np.int64)).pin_memory().numpy().view(np.uint64)
+    hb = torch.from_numpy(b.view(np.int64)).pin_memory().numpy().view(np.uint64)
+    hr = torch.empty(an + bn, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+    torch.cuda.set_device(local)
+    for _ in range(2):
+        (sbg.nt_sqr(hr, ha, an) if op == "sqr" else sbg.nt_mul(hr, ha, an, hb, bn))
+    if pg is not None:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ok = sbg.nt_sqr(hr, ha, an) if op == "sqr" else sbg.nt_mul(hr, ha, an, hb, bn)
+        if ok != 1:
+            raise RuntimeError("sbg_nt_mul failed")
+    e2e_s = time.perf_counter() - t0
+    e2e_s = barrier_max(pg, e2e_s, dev)
+    exact = exact and np.array_equal(hr, got)
+    clocks.mark("end")
+    clk = clocks.stop() if rank == 0 else None
+
+    if rank != 0:
+        ctx.close()
+        return None
+
+    # ---- roofline of the dominant kernel ----
+    model = kernel_model(op, an, bn)
+    rows = {}
+    total_ms = sum(v[0] for v in kt.values()) or 1.0
+    for name, (ms, cnt) in kt.items():
+        avg = ms / cnt
+        m = model.get(name, {"bytes": 0, "bfly": 0})
+        rows[name] = {"avg_ms": round(avg, 4), "launches": cnt, "share": round(ms / total_ms, 4),
+                      "alg_bytes": m["bytes"], "alg_bfly": m["bfly"],
+                      "gbs": round(m["bytes"] / (avg * 1e-3) / 1e9, 1)}
+    dom = max(rows, key=lambda k: rows[k]["share"])
+    hbm, hbm_src = measured_peaks()
+    bfly_peak = sbg.probe_bfly_peak(local)
+    d = rows[dom]
+    achieved = d["gbs"]
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get(args.workload, {}).get(dom)
+        except Exception:
+            traffic = None
+    bfly_rate = d["alg_bfly"] / (d["avg_ms"] * 1e-3) if d["alg_bfly"] else 0.0
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4), "traffic": traffic,
+            "peak_source": f"{hbm_src} (MEASURED_PEAKS.json hbm_gbs)" if hbm_src == "measured" else "fallback 6.65 TB/s",
+            "alg_bytes_per_launch": d["alg_bytes"],
+            "int_pipe": {"achieved_bfly_per_s": bfly_rate, "peak_bfly_per_s": bfly_peak,
+                         "frac": round(bfly_rate / bfly_peak, 4) if bfly_peak else None,
+                         "peak_source": "sbg_probe_bfly_peak (register-only butterfly loop, measured live)"},
+            "kernels": rows}
+    nlimbs = (an + bn) * ws
+    value = nlimbs / (ms_step * 1e-3) / 1e6
+    e2e_val = nlimbs * args.steps / e2e_s / 1e6
+    launches_per_step = sum(v["launches"] for v in rows.values()) / args.steps
+    result = {
+        "metric": "product Mlimb/s", "value": round(value, 2), "unit": "Mlimb/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic: seeded uniform u64 limbs, top limb nonzero",
+        "config": {"workload": f"{op} {an} x {bn} limbs, one product per step per GPU",
+                   "an": an, "bn": bn, "parallelism": f"replicas x{ws} (no collective)",
+                   "l2": "operands + 1.3 GB workspace exceed the 126 MB L2; no flush needed"},
+        "bit_exact": bool(exact),
+        "e2e": {"value": round(e2e_val, 2), "unit": "Mlimb/s", "h2d_bytes_per_step": 8 * (an + (0 if op == "sqr" else bn)),
+                "d2h_bytes_per_step": 8 * (an + bn), "entry": "sbg_nt_mul/sbg_nt_sqr on pinned host buffers"},
+        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "roofline": roof,
+        "clocks": clk,
+    }
+    ctx.close()
+    return result
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="mul2p24")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local, pg = (1, 0, 0, None)
+    op, an, bn = WORKLOADS[args.workload]
+
+    if args.impl == "reference":
+        # the reference is CPU code: rank 0 alone runs it, on all host threads
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        threads = cpu_threads_for(an, bn)
+        # bounded sample: one product per thread per step, few steps
+        steps = max(1, min(args.steps, 3))
+        r = cpu_run(op, an, bn, threads, steps=steps, warmup=1)
+        out = {"metric": "product Mlimb/s", "value": round(r["value"], 3), "unit": "Mlimb/s",
+               "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": round(r["step_s"] * 1e3, 1),
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+               "data": "synthetic: seeded uniform u64 limbs, top limb nonzero",
+               "config": {"workload": f"{op} {an} x {bn} limbs, one product per step per thread",
+                          "an": an, "bn": bn, "parallelism": f"{threads} host threads"},
+               "impl": "reference",
+               "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample", "cpu_model", "isa")},
+               "e2e": {"value": round(r["value"], 3), "unit": "Mlimb/s", "h2d_bytes_per_step": 0,
+                       "d2h_bytes_per_step": 0}}
+        print(json.dumps(out), flush=True)
+        return
+
+    ws, rank, local, pg = dist_init()
+    res = run_ours(args, ws, rank, local, pg)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    if not args.no_cpu:
+        try:
+            res["cpu_baseline"] = cpu_bounded(op, an, bn)
+        except Exception as e:  # recorded, not fatal
+            res["cpu_baseline"] = {"value": None, "unit": "Mlimb/s", "error": str(e)}
+    print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -67,6 +67,13 @@ int sbg_ctx_sync(sbg_ctx *ctx);
  * (an + bn), so later calls neither allocate nor generate tables. */
 int sbg_ctx_reserve(sbg_ctx *ctx, int64_t total_limbs);
 const char *sbg_strerror(int status);
+/* Per-launch CUDA-event timing of the library's kernels (off by default).
+ * sbg_ctx_kernel_times sums the recorded launches per kernel id since the
+ * last call (ids: 0 single-CTA product, 1 column forward, 2 row
+ * forward+pointwise+inverse, 3 column inverse, 4 CRT+carry, 5 batch,
+ * 6 division helpers), waiting for them; n must be >= 8. */
+int sbg_ctx_set_timing(sbg_ctx *ctx, int on);
+int sbg_ctx_kernel_times(sbg_ctx *ctx, double *ms, int64_t *counts, int n);
 /* Largest an + bn accepted by one product (2^25 + 1). */
 int64_t sbg_max_total_limbs(void);
 
@@ -97,6 +104,13 @@ int sbg_nt_mul(uint64_t *rp, const uint64_t *ap, ptrdiff_t an, const uint64_t *b
 /* int nt_sqr(uint64_t *rp, const uint64_t *ap, ptrdiff_t an)
  *                                                  -- reference include/ntmul.h:77 */
 int sbg_nt_sqr(uint64_t *rp, const uint64_t *ap, ptrdiff_t an);
+
+/* ---- diagnostics ---------------------------------------------------------- */
+
+/* Register-only throughput of the transform butterfly on `device`
+ * (butterflies per second): the integer-pipe ceiling of the NTT kernels.
+ * No counterpart in the reference (a measurement helper). */
+int sbg_probe_bfly_peak(int device, double *bfly_per_s);
 
 #ifdef __cplusplus
 }

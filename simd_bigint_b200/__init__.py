@@ -67,6 +67,10 @@ def lib(build_if_missing: bool = False):
         L.sbg_ctx_sync.restype = C.c_int
         L.sbg_ctx_reserve.argtypes = [_vp, _i64]
         L.sbg_ctx_reserve.restype = C.c_int
+        L.sbg_ctx_set_timing.argtypes = [_vp, C.c_int]
+        L.sbg_ctx_set_timing.restype = C.c_int
+        L.sbg_ctx_kernel_times.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]
+        L.sbg_ctx_kernel_times.restype = C.c_int
         L.sbg_strerror.argtypes = [C.c_int]
         L.sbg_strerror.restype = C.c_char_p
         L.sbg_max_total_limbs.argtypes = []
@@ -80,6 +84,8 @@ def lib(build_if_missing: bool = False):
         L.sbg_nt_mul.restype = C.c_int
         L.sbg_nt_sqr.argtypes = [_vp, _vp, C.c_ssize_t]
         L.sbg_nt_sqr.restype = C.c_int
+        L.sbg_probe_bfly_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+        L.sbg_probe_bfly_peak.restype = C.c_int
         _lib = L
     return _lib
 
@@ -144,6 +150,19 @@ class Context:
     def sync(self):
         _check(self._L.sbg_ctx_sync(self.handle), "sbg_ctx_sync")
 
+    KERNEL_NAMES = ("k_small", "k_col_fwd", "k_row", "k_col_inv", "k_crt_carry", "k_batch",
+                    "k_div", "k_other")
+
+    def set_timing(self, on: bool):
+        _check(self._L.sbg_ctx_set_timing(self.handle, int(bool(on))), "sbg_ctx_set_timing")
+
+    def kernel_times(self) -> dict:
+        """{kernel name: (total ms, launches)} since the previous call."""
+        ms = (C.c_double * 8)()
+        cnt = (C.c_int64 * 8)()
+        _check(self._L.sbg_ctx_kernel_times(self.handle, ms, cnt, 8), "sbg_ctx_kernel_times")
+        return {self.KERNEL_NAMES[i]: (ms[i], cnt[i]) for i in range(8) if cnt[i]}
+
     def reserve(self, total_limbs: int):
         _check(self._L.sbg_ctx_reserve(self.handle, int(total_limbs)), "sbg_ctx_reserve")
 
@@ -203,6 +222,13 @@ def sqr(a: np.ndarray) -> np.ndarray:
     if not nt_sqr(r, a, len(a)):
         raise SbgError(2, "nt_sqr")
     return r
+
+
+def probe_bfly_peak(device: int = 0) -> float:
+    """Butterflies/s of the transform butterfly on registers (integer ceiling)."""
+    v = C.c_double(0.0)
+    _check(lib().sbg_probe_bfly_peak(device, C.byref(v)), "sbg_probe_bfly_peak")
+    return v.value
 
 
 def mpn_mulmid(ctx: Context, a, b):

@@ -5,11 +5,67 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "../../include/simd_bigint_b200.h"
 #include "sbg_internal.h"
 
 using namespace sbg;
+
+// Per-launch CUDA event pairs, summed per kernel id by sbg_ctx_kernel_times.
+struct EventTimer : KTimer {
+    struct Rec {
+        int kid;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t take() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(int kid, cudaStream_t st) override {
+        Rec r{kid, take(), nullptr};
+        cudaEventRecord(r.a, st);
+        recs.push_back(r);
+    }
+    void end(int kid, cudaStream_t st) override {
+        for (size_t i = recs.size(); i-- > 0;)
+            if (recs[i].kid == kid && recs[i].b == nullptr) {
+                recs[i].b = take();
+                cudaEventRecord(recs[i].b, st);
+                return;
+            }
+    }
+    void collect(double* ms, int64_t* cnt) {
+        for (auto& r : recs) {
+            if (r.b) {
+                float t = 0.f;
+                if (cudaEventSynchronize(r.b) == cudaSuccess &&
+                    cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
+                    ms[r.kid] += t;
+                    cnt[r.kid] += 1;
+                }
+                pool.push_back(r.b);
+            }
+            pool.push_back(r.a);
+        }
+        recs.clear();
+    }
+    ~EventTimer() override {
+        for (auto& r : recs) {
+            cudaEventDestroy(r.a);
+            if (r.b) cudaEventDestroy(r.b);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
 
 struct sbg_ctx {
     int device = 0;
@@ -26,6 +82,7 @@ struct sbg_ctx {
     // staging for the host-pointer drop-ins
     uint64_t* d_stage = nullptr;
     size_t stage_cap = 0;
+    EventTimer* timer = nullptr;    // non-null while kernel timing is on
 };
 
 static int cuda_fail(cudaError_t e, const char* where) {
@@ -110,8 +167,9 @@ static int run_conv(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, co
     st = ensure_ws(c, ws_words(lgL, sq), carry_flag_words(nout));
     if (st) return st;
     const LenPlan* lp = &c->plans[lgL];
-    CK(launch_conv(ap, an, bp, bn, sq, lgL, lp, c->tw_f, c->tw_i, c->ws, c->stream));
-    CK(launch_crt_carry(c->ws, lgL, lp, cmin, cmax, off, rp, nout, c->flags, c->err, c->stream));
+    CK(launch_conv(ap, an, bp, bn, sq, lgL, lp, c->tw_f, c->tw_i, c->ws, c->stream, c->timer));
+    CK(launch_crt_carry(c->ws, lgL, lp, cmin, cmax, off, rp, nout, c->flags, c->err, c->stream,
+                        c->timer));
     return SBG_OK;
 }
 
@@ -186,6 +244,7 @@ void sbg_ctx_destroy(sbg_ctx* c) {
     cudaFree(c->flags);
     cudaFree(c->err);
     cudaFree(c->d_stage);
+    delete c->timer;
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -210,6 +269,30 @@ int sbg_ctx_sync(sbg_ctx* c) {
         if (h & 2u) return SBG_ESPILL;
         return SBG_ECUDA;
     }
+    return SBG_OK;
+}
+
+int sbg_ctx_set_timing(sbg_ctx* c, int on) {
+    if (!c) return SBG_EINVAL;
+    CK(cudaSetDevice(c->device));
+    if (on && !c->timer) c->timer = new EventTimer();
+    if (!on && c->timer) {
+        cudaStreamSynchronize(c->stream);
+        delete c->timer;
+        c->timer = nullptr;
+    }
+    return SBG_OK;
+}
+
+int sbg_ctx_kernel_times(sbg_ctx* c, double* ms, int64_t* counts, int n) {
+    if (!c || !ms || !counts || n < KID_COUNT) return SBG_EINVAL;
+    for (int i = 0; i < n; ++i) {
+        ms[i] = 0.0;
+        counts[i] = 0;
+    }
+    if (!c->timer) return SBG_OK;
+    CK(cudaSetDevice(c->device));
+    c->timer->collect(ms, counts);
     return SBG_OK;
 }
 

@@ -62,6 +62,33 @@ struct ConvJob {
     int lgL;
 };
 
+// Kernel ids for the optional per-launch event timing (sbg_ctx_kernel_times).
+enum KernelId {
+    KID_SMALL = 0,
+    KID_COL_FWD = 1,
+    KID_ROW = 2,
+    KID_COL_INV = 3,
+    KID_CRT = 4,
+    KID_BATCH = 5,
+    KID_DIV = 6,
+    KID_COUNT = 8
+};
+
+// Records a CUDA event pair around each launch when attached to a context.
+struct KTimer {
+    virtual void begin(int kid, cudaStream_t st) = 0;
+    virtual void end(int kid, cudaStream_t st) = 0;
+    virtual ~KTimer() {}
+};
+#define KT_BEGIN(kt, kid, st) \
+    do {                       \
+        if (kt) (kt)->begin((kid), (st)); \
+    } while (0)
+#define KT_END(kt, kid, st) \
+    do {                     \
+        if (kt) (kt)->end((kid), (st)); \
+    } while (0)
+
 // ---- host helpers (sbg_plan.cu) ----
 uint32_t host_powmod(uint64_t a, uint64_t e, uint32_t p);
 uint32_t host_shoup(uint32_t w, uint32_t p);
@@ -80,12 +107,13 @@ cudaError_t gen_len_tables(LenPlan* lp, cudaStream_t st);
 size_t ws_words(int lgL, int sq);
 cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_t bn, int sq,
                         int lgL, const LenPlan* lp, const uint2* tw_f, const uint2* tw_i,
-                        uint32_t* ws, cudaStream_t st);
+                        uint32_t* ws, cudaStream_t st, KTimer* kt = nullptr);
 // CRT + carry of residues R (5 x L u32) into out[0..nout): out[m] = limb (m + off)
 // of sum_{cmin <= j <= cmax} c_j * 2^(64 j).
 cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int64_t cmin,
                              int64_t cmax, int64_t off, uint64_t* out, int64_t nout,
-                             uint32_t* flags, uint32_t* err, cudaStream_t st);
+                             uint32_t* flags, uint32_t* err, cudaStream_t st,
+                             KTimer* kt = nullptr);
 size_t carry_flag_words(int64_t nout);
 
 }  // namespace sbg

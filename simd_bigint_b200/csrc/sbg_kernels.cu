@@ -517,13 +517,15 @@ size_t ws_words(int lgL, int sq) {
 
 cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_t bn, int sq,
                         int lgL, const LenPlan* lp, const uint2* tw_f, const uint2* tw_i,
-                        uint32_t* ws, cudaStream_t st) {
+                        uint32_t* ws, cudaStream_t st, KTimer* kt) {
     const size_t L = (size_t)1 << lgL;
     uint32_t* YA = ws;
     uint32_t* YB = ws + SBG_NP * L;
     if (lgL <= SBG_SMALL_MAX_LG) {
         size_t smem = (size_t)2 * padded_len((int)L) * 4;
+        KT_BEGIN(kt, KID_SMALL, st);
         k_small<<<SBG_NP, 256, smem, st>>>(a, an, b, bn, sq, lgL, tw_f, tw_i, YA);
+        KT_END(kt, KID_SMALL, st);
         return cudaGetLastError();
     }
     const int lgN2 = lp->lgN2, lgN1 = lp->lgN1;
@@ -535,15 +537,21 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
     FsTables fsi{lp->fs_lo_i, lp->fs_hi_i, lp->hi_n};
     size_t col_smem = (size_t)(1 << lgw) * (padded_len(1 << lgN1) + 1) * 4;
     int nops = sq ? 1 : 2;
+    KT_BEGIN(kt, KID_COL_FWD, st);
     k_col_fwd<<<nops * ntiles * SBG_NP, 512, col_smem, st>>>(a, an, b, bn, lgN1, lgN2, lgw, fsf,
                                                              tw_f, YA, YB);
+    KT_END(kt, KID_COL_FWD, st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     size_t row_smem = (size_t)2 * padded_len(1 << lgN2) * 4;
+    KT_BEGIN(kt, KID_ROW, st);
     k_row<<<(1 << lgN1) * SBG_NP, 256, row_smem, st>>>(YA, YB, sq, lgN1, lgN2, tw_f, tw_i);
+    KT_END(kt, KID_ROW, st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    KT_BEGIN(kt, KID_COL_INV, st);
     k_col_inv<<<ntiles * SBG_NP, 512, col_smem, st>>>(YA, lgN1, lgN2, lgw, fsi, tw_i);
+    KT_END(kt, KID_COL_INV, st);
     return cudaGetLastError();
 }
 
@@ -551,7 +559,8 @@ size_t carry_flag_words(int64_t nout) { return 1 + (size_t)((nout + CRT_BLK) / C
 
 cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int64_t cmin,
                              int64_t cmax, int64_t off, uint64_t* out, int64_t nout,
-                             uint32_t* flags, uint32_t* err, cudaStream_t st) {
+                             uint32_t* flags, uint32_t* err, cudaStream_t st,
+                             KTimer* kt) {
     ScaleArg sc;
     for (int q = 0; q < SBG_NP; ++q) {
         sc.w[q] = lp->scale[q].w;
@@ -561,8 +570,10 @@ cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int6
     int64_t nblk = (nout + 1 + CRT_BLK - 1) / CRT_BLK;
     cudaError_t e = cudaMemsetAsync(flags, 0, (1 + nblk) * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
+    KT_BEGIN(kt, KID_CRT, st);
     k_crt_carry<<<(unsigned)nblk, CRT_T, 0, st>>>(R, lgL, cmin, cmax, off, out, nout, sc, flags,
                                                   err);
+    KT_END(kt, KID_CRT, st);
     return cudaGetLastError();
 }
 
