@@ -210,7 +210,7 @@ int sbg_ctx_create(int device, sbg_ctx** out) {
         c->stream = c->own_stream;
         if ((st = cuda_fail(set_kernel_attributes(), "attributes"))) break;
         if ((st = cuda_fail(upload_constants(c->stream), "constants"))) break;
-        size_t tb = (size_t)SBG_NP * (1 << 12) * sizeof(uint2);
+        size_t tb = master_table_entries() * sizeof(uint2);
         if ((st = cuda_fail(cudaMalloc(&c->tw_f, tb), "tw_f"))) break;
         if ((st = cuda_fail(cudaMalloc(&c->tw_i, tb), "tw_i"))) break;
         if ((st = cuda_fail(gen_master_tables(c->tw_f, c->tw_i, c->stream), "tables"))) break;

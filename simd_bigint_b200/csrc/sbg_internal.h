@@ -99,6 +99,7 @@ ShoupPair host_scale(int lgL, int q);
 // ---- launchers (sbg_kernels.cu) ----
 cudaError_t upload_constants(cudaStream_t st);
 cudaError_t set_kernel_attributes();
+size_t master_table_entries();
 cudaError_t gen_master_tables(uint2* tw_f, uint2* tw_i, cudaStream_t st);
 cudaError_t gen_len_tables(LenPlan* lp, cudaStream_t st);
 

@@ -48,13 +48,27 @@ __global__ void k_gen_pow(uint2* out, int n, const uint32_t* roots, uint32_t str
     }
 }
 
+// per-resolution table: out[q * 2^13 + (S/2 - 1 + j)] = (w_S^j, shoup), S = 2..2^13
+__global__ void k_gen_res(uint2* out, const uint32_t* roots13) {
+    int q = blockIdx.y;
+    uint32_t p = c_pr[q].p;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < SBG_TW_N - 1;
+         idx += gridDim.x * blockDim.x) {
+        int lgS = 32 - __clz(idx + 1);                 // S/2 - 1 <= idx < S - 1
+        int j = idx - ((1 << (lgS - 1)) - 1);
+        uint32_t e = (uint32_t)j << (SBG_TW_LG - lgS);
+        uint32_t w = pow_mod_dev(roots13[q], e, p);
+        out[(size_t)q * SBG_TW_N + idx] = make_uint2(w, shoup_of(w, p));
+    }
+}
+
 // ------------------------------------------------------------------------
 // K0: single-CTA product for L <= 2^12 (one CTA per prime)
 // ------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_small(const uint64_t* __restrict__ a, int64_t an,
                                                const uint64_t* __restrict__ b, int64_t bn, int sq,
                                                int lgL, const uint2* __restrict__ twf,
-                                               const uint2* __restrict__ twi,
+                                               const uint2* __restrict__ twi, ScaleArg sc,
                                                uint32_t* __restrict__ R) {
     extern __shared__ uint32_t sm[];
     const int q = blockIdx.x;
@@ -72,7 +86,7 @@ __global__ void __launch_bounds__(256) k_small(const uint64_t* __restrict__ a, i
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
         uint32_t x = A[pad_idx(i)];
         uint32_t y = sq ? x : B[pad_idx(i)];
-        A[pad_idx(i)] = mont_mul(x, y, pc.p, pc.pinv);
+        A[pad_idx(i)] = mul_shoup(mont_mul(x, y, pc.p, pc.pinv), sc.w[q], sc.ws[q], pc.p);
     }
     __syncthreads();
     ntt_inverse(sm, ld, 1, lgL, twi + q * SBG_TW_N, pc.p);
@@ -80,117 +94,269 @@ __global__ void __launch_bounds__(256) k_small(const uint64_t* __restrict__ a, i
 }
 
 // ------------------------------------------------------------------------
-// K1: limb unpack + column DIF + four-step twiddle.
-// The length-L sequence is an N1 x N2 row-major matrix (n = n1*N2 + n2).
-// A CTA owns w adjacent columns of one operand for one prime.
+// Four-step layout: the length-L sequence is an N1 x N2 row-major matrix
+// (n = n1*N2 + n2).  K1 runs the column DIFs, K2 the row DIFs (after the
+// four-step twiddle w_L^(k1*n2)), the pointwise product and the row DITs
+// (followed by the inverse twiddle and the CRT scale), K3 the column DITs.
 // ------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t fs_twiddle(uint32_t v, uint32_t e, const uint2* lo,
-                                               const uint2* hi, uint32_t p) {
-    uint2 a = __ldg(&lo[e & (SBG_FS_LO_N - 1)]);
-    uint2 b = __ldg(&hi[e >> SBG_FS_LO_LG]);
-    return mul_shoup(mul_shoup(v, a.x, a.y, p), b.x, b.y, p);
+__device__ __forceinline__ uint32_t fs_value(const FsTables& fs, int q, uint32_t e, uint32_t p) {
+    uint2 a = __ldg(&fs.lo[(size_t)q * SBG_FS_LO_N + (e & (SBG_FS_LO_N - 1))]);
+    uint2 b = __ldg(&fs.hi[(size_t)q * fs.hi_n + (e >> SBG_FS_LO_LG)]);
+    return mul_shoup(a.x, b.x, b.y, p);
 }
 
+// Column tiles: w adjacent columns, interleaved in shared memory
+// (point (i, g) at linear index i*w + g, padded one word per 16) so that a
+// warp's lanes -- column fastest -- touch consecutive words at every pass.
+__device__ __forceinline__ int col_addr(int i, int g, int lgw) { return pad_idx((i << lgw) + g); }
+
+// One column pass of radix R over the tile.  FWD: DIF; else DIT.
+// SRC/DST: 0 = shared memory, 1 = global.  Forward global source = limbs
+// (residue taken on the fly); inverse global source / both global
+// destinations = the residue array Y (+ q * L already applied).
+template <int R, bool FWD>
+__device__ __forceinline__ void col_pass(uint32_t* sm, int lgN1, int lgN2, int lgw, int lgM,
+                                         bool src_global, bool dst_global,
+                                         const uint64_t* __restrict__ X, int64_t xn,
+                                         uint32_t* __restrict__ Y, int c0,
+                                         const uint2* __restrict__ tw, const PrimeConst& pc) {
+    constexpr int r = RLog<R>::v;
+    const int lgst = lgM - r;
+    const int st = 1 << lgst;
+    const int w = 1 << lgw;
+    const int total = 1 << (lgw + lgN1 - r);
+    for (int gid = threadIdx.x; gid < total; gid += blockDim.x) {
+        const int g = gid & (w - 1);
+        const int rest = gid >> lgw;
+        const int j0 = rest & (st - 1);
+        const int blk = rest >> lgst;
+        const int i0 = (blk << lgM) + j0;
+        uint32_t x[R];
+        if (src_global) {
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int64_t n = ((int64_t)(i0 + st * t) << lgN2) + c0 + g;
+                if (FWD)
+                    x[t] = n < xn ? limb_residue(__ldg(&X[n]), pc) : 0u;
+                else
+                    x[t] = Y[n];
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < R; ++t) x[t] = sm[col_addr(i0 + st * t, g, lgw)];
+        }
+        if (FWD)
+            dif_regs<R>(x, tw, j0, st, lgM, pc.p);
+        else
+            dit_regs<R>(x, tw, j0, st, lgM, pc.p);
+        if (dst_global) {
+#pragma unroll
+            for (int t = 0; t < R; ++t) Y[((size_t)(i0 + st * t) << lgN2) + c0 + g] = x[t];
+        } else {
+#pragma unroll
+            for (int t = 0; t < R; ++t) sm[col_addr(i0 + st * t, g, lgw)] = x[t];
+        }
+    }
+}
+
+template <bool FWD>
+__device__ __forceinline__ void col_pass_dispatch(int rlg, uint32_t* sm, int lgN1, int lgN2,
+                                                  int lgw, int lgM, bool sg, bool dg,
+                                                  const uint64_t* X, int64_t xn, uint32_t* Y,
+                                                  int c0, const uint2* tw, const PrimeConst& pc) {
+    switch (rlg) {
+        case 4: col_pass<16, FWD>(sm, lgN1, lgN2, lgw, lgM, sg, dg, X, xn, Y, c0, tw, pc); break;
+        case 3: col_pass<8, FWD>(sm, lgN1, lgN2, lgw, lgM, sg, dg, X, xn, Y, c0, tw, pc); break;
+        case 2: col_pass<4, FWD>(sm, lgN1, lgN2, lgw, lgM, sg, dg, X, xn, Y, c0, tw, pc); break;
+        case 1: col_pass<2, FWD>(sm, lgN1, lgN2, lgw, lgM, sg, dg, X, xn, Y, c0, tw, pc); break;
+        default: break;
+    }
+}
+
+// K1: limbs -> residues -> column DIF (bit-reversed rows) for one operand,
+// one prime, one tile of w columns.  Block order: prime slowest, so the CTAs
+// resident on an SM share one prime's twiddle table.
 __global__ void __launch_bounds__(512) k_col_fwd(const uint64_t* __restrict__ a, int64_t an,
                                                  const uint64_t* __restrict__ b, int64_t bn,
-                                                 int lgN1, int lgN2, int lgw, FsTables fs,
+                                                 int lgN1, int lgN2, int lgw,
                                                  const uint2* __restrict__ twf,
                                                  uint32_t* __restrict__ YA,
-                                                 uint32_t* __restrict__ YB) {
+                                                 uint32_t* __restrict__ YB, int nops) {
     extern __shared__ uint32_t sm[];
-    const int q = blockIdx.x % SBG_NP;
-    const int rest = blockIdx.x / SBG_NP;
     const int ntiles = 1 << (lgN2 - lgw);
+    const int per_q = ntiles * nops;
+    const int q = blockIdx.x / per_q;
+    const int rest = blockIdx.x - q * per_q;
     const int tile = rest % ntiles;
     const int op = rest / ntiles;
     const uint64_t* X = op ? b : a;
     const int64_t xn = op ? bn : an;
     uint32_t* Y = (op ? YB : YA) + ((size_t)q << (lgN1 + lgN2));
     const PrimeConst pc = c_pr[q];
-    const int w = 1 << lgw;
-    const int ld = padded_len(1 << lgN1) + 1;
+    const uint2* tw = twf + (size_t)q * SBG_TW_N;
     const int c0 = tile << lgw;
-    const int npts = 1 << (lgN1 + lgw);
-    for (int idx = threadIdx.x; idx < npts; idx += blockDim.x) {
-        int g = idx & (w - 1), i = idx >> lgw;
-        int64_t n = ((int64_t)i << lgN2) + c0 + g;
-        sm[g * ld + pad_idx(i)] = n < xn ? limb_residue(__ldg(&X[n]), pc) : 0u;
-    }
-    __syncthreads();
-    ntt_forward(sm, ld, w, lgN1, twf + q * SBG_TW_N, pc.p);
-    const uint2* lo = fs.lo + (size_t)q * SBG_FS_LO_N;
-    const uint2* hi = fs.hi + (size_t)q * fs.hi_n;
-    for (int idx = threadIdx.x; idx < npts; idx += blockDim.x) {
-        int g = idx & (w - 1), i = idx >> lgw;
-        uint32_t k1 = bitrev((uint32_t)i, lgN1);
-        uint32_t n2 = (uint32_t)(c0 + g);
-        uint32_t v = fs_twiddle(sm[g * ld + pad_idx(i)], k1 * n2, lo, hi, pc.p);
-        Y[((size_t)i << lgN2) + n2] = v;
+    const int np = num_passes(lgN1);
+    int lgM = lgN1;
+    for (int k = 0; k < np; ++k) {
+        const int rlg = pass_radix_lg(lgN1, k);
+        col_pass_dispatch<true>(rlg, sm, lgN1, lgN2, lgw, lgM, k == 0, k == np - 1, X, xn, Y, c0,
+                                tw, pc);
+        if (k < np - 1) __syncthreads();
+        lgM -= rlg;
     }
 }
 
-// ------------------------------------------------------------------------
-// K2: one row (N2 points) of one prime: forward DIF of A's and B's rows,
-// pointwise Montgomery product, inverse DIT, written back over A.
-// ------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_row(uint32_t* __restrict__ YA,
-                                             const uint32_t* __restrict__ YB, int sq, int lgN1,
-                                             int lgN2, const uint2* __restrict__ twf,
-                                             const uint2* __restrict__ twi) {
-    extern __shared__ uint32_t sm[];
-    const int q = blockIdx.x % SBG_NP;
-    const int row = blockIdx.x / SBG_NP;
-    const PrimeConst pc = c_pr[q];
-    const int N2 = 1 << lgN2;
-    const int ld = padded_len(N2);
-    const size_t base = ((size_t)q << (lgN1 + lgN2)) + ((size_t)row << lgN2);
-    uint32_t* Ar = YA + base;
-    const uint32_t* Br = YB + base;
-    for (int i = threadIdx.x; i < N2; i += blockDim.x) {
-        sm[pad_idx(i)] = Ar[i];
-        if (!sq) sm[ld + pad_idx(i)] = __ldg(&Br[i]);
-    }
-    __syncthreads();
-    ntt_forward(sm, ld, sq ? 1 : 2, lgN2, twf + q * SBG_TW_N, pc.p);
-    for (int i = threadIdx.x; i < N2; i += blockDim.x) {
-        uint32_t x = sm[pad_idx(i)];
-        uint32_t y = sq ? x : sm[ld + pad_idx(i)];
-        sm[pad_idx(i)] = mont_mul(x, y, pc.p, pc.pinv);
-    }
-    __syncthreads();
-    ntt_inverse(sm, ld, 1, lgN2, twi + q * SBG_TW_N, pc.p);
-    for (int i = threadIdx.x; i < N2; i += blockDim.x) Ar[i] = sm[pad_idx(i)];
-}
-
-// ------------------------------------------------------------------------
-// K3: inverse four-step twiddle + column DIT, in place; natural order out.
-// ------------------------------------------------------------------------
+// K3: column DIT (reverse of K1), in place, natural row order out.
 __global__ void __launch_bounds__(512) k_col_inv(uint32_t* __restrict__ YA, int lgN1, int lgN2,
-                                                 int lgw, FsTables fs,
-                                                 const uint2* __restrict__ twi) {
+                                                 int lgw, const uint2* __restrict__ twi) {
     extern __shared__ uint32_t sm[];
-    const int q = blockIdx.x % SBG_NP;
-    const int tile = blockIdx.x / SBG_NP;
+    const int ntiles = 1 << (lgN2 - lgw);
+    const int q = blockIdx.x / ntiles;
+    const int tile = blockIdx.x - q * ntiles;
     uint32_t* Y = YA + ((size_t)q << (lgN1 + lgN2));
     const PrimeConst pc = c_pr[q];
-    const int w = 1 << lgw;
-    const int ld = padded_len(1 << lgN1) + 1;
+    const uint2* tw = twi + (size_t)q * SBG_TW_N;
     const int c0 = tile << lgw;
-    const int npts = 1 << (lgN1 + lgw);
-    const uint2* lo = fs.lo + (size_t)q * SBG_FS_LO_N;
-    const uint2* hi = fs.hi + (size_t)q * fs.hi_n;
-    for (int idx = threadIdx.x; idx < npts; idx += blockDim.x) {
-        int g = idx & (w - 1), i = idx >> lgw;
-        uint32_t k1 = bitrev((uint32_t)i, lgN1);
-        uint32_t n2 = (uint32_t)(c0 + g);
-        uint32_t v = Y[((size_t)i << lgN2) + n2];
-        sm[g * ld + pad_idx(i)] = fs_twiddle(v, k1 * n2, lo, hi, pc.p);
+    const int np = num_passes(lgN1);
+    for (int k = np - 1; k >= 0; --k) {
+        int lgM = lgN1;
+        for (int kk = 0; kk < k; ++kk) lgM -= pass_radix_lg(lgN1, kk);
+        const int rlg = pass_radix_lg(lgN1, k);
+        col_pass_dispatch<false>(rlg, sm, lgN1, lgN2, lgw, lgM, k == np - 1, k == 0, nullptr, 0,
+                                 Y, c0, tw, pc);
+        if (k > 0) __syncthreads();
+    }
+}
+
+// K2: one row of N2 = 2^12 points for one prime, 256 threads.
+//   P1  global -> four-step twiddle -> DIF levels 1-4 (A and B) -> smem
+//   P2  DIF levels 5-8 (A and B)
+//   P3  DIF levels 9-12, pointwise Montgomery product, DIT levels 12-9
+//   P2' DIT levels 8-5
+//   P1' DIT levels 4-1 -> inverse twiddle x CRT scale -> global (over A)
+// The last forward pass, the product and the first inverse pass share one
+// register group, so that stage never touches shared memory.
+#define ROW_LG 12
+#define ROW_N (1 << ROW_LG)
+__global__ void __launch_bounds__(256) k_row12(uint32_t* __restrict__ YA,
+                                               const uint32_t* __restrict__ YB, int sq, int lgN1,
+                                               FsTables fsf, FsTables fsi, ScaleArg sc,
+                                               const uint2* __restrict__ twf,
+                                               const uint2* __restrict__ twi) {
+    __shared__ uint32_t smA[padded_len(ROW_N)];
+    __shared__ uint32_t smB[padded_len(ROW_N)];
+    __shared__ uint2 s_f[16];
+    __shared__ uint2 s_i[16];
+    const int tid = threadIdx.x;
+    const int N1 = 1 << lgN1;
+    const int q = blockIdx.x >> lgN1;
+    const int row = blockIdx.x & (N1 - 1);
+    const PrimeConst pc = c_pr[q];
+    const uint32_t p = pc.p;
+    const uint32_t Lmask = (1u << (lgN1 + ROW_LG)) - 1u;
+    const size_t base = ((size_t)q << (lgN1 + ROW_LG)) + ((size_t)row << ROW_LG);
+    const uint2* tf = twf + (size_t)q * SBG_TW_N;
+    const uint2* ti = twi + (size_t)q * SBG_TW_N;
+    const uint32_t k1 = bitrev((uint32_t)row, lgN1);
+    // four-step twiddles: w_L^(k1 (tid + 256 t)) = b * s^t
+    if (tid < 16) {
+        uint32_t e = (k1 * 256u * (uint32_t)tid) & Lmask;
+        uint32_t v = fs_value(fsf, q, e, p);
+        s_f[tid] = make_uint2(v, shoup_of(v, p));
+        uint32_t vi = mul_shoup(fs_value(fsi, q, e, p), sc.w[q], sc.ws[q], p);
+        s_i[tid] = make_uint2(vi, shoup_of(vi, p));
+    }
+    const uint32_t eb = k1 * (uint32_t)tid;
+    const uint32_t bf = fs_value(fsf, q, eb, p), bfs = shoup_of(bf, p);
+    const uint32_t bi = fs_value(fsi, q, eb, p), bis = shoup_of(bi, p);
+    __syncthreads();
+
+    uint32_t xa[16], xb[16];
+    // P1
+    {
+        const uint32_t* Ar = YA + base;
+        const uint32_t* Br = YB + base;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            uint2 s = s_f[t];
+            xa[t] = mul_shoup(mul_shoup(Ar[tid + 256 * t], s.x, s.y, p), bf, bfs, p);
+            if (!sq) xb[t] = mul_shoup(mul_shoup(__ldg(&Br[tid + 256 * t]), s.x, s.y, p), bf, bfs, p);
+        }
+        if (sq) {
+            dif_regs<16>(xa, tf, tid, 256, 12, p);
+        } else {
+            dif_regs2<16>(xa, xb, tf, tid, 256, 12, p);
+        }
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            smA[pad_idx(tid + 256 * t)] = xa[t];
+            if (!sq) smB[pad_idx(tid + 256 * t)] = xb[t];
+        }
     }
     __syncthreads();
-    ntt_inverse(sm, ld, w, lgN1, twi + q * SBG_TW_N, pc.p);
-    for (int idx = threadIdx.x; idx < npts; idx += blockDim.x) {
-        int g = idx & (w - 1), i = idx >> lgw;
-        Y[((size_t)i << lgN2) + c0 + g] = sm[g * ld + pad_idx(i)];
+    // P2: M = 256, st = 16
+    {
+        const int j0 = tid & 15, i0 = ((tid >> 4) << 8) + j0;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            xa[t] = smA[pad_idx(i0 + 16 * t)];
+            if (!sq) xb[t] = smB[pad_idx(i0 + 16 * t)];
+        }
+        if (sq) {
+            dif_regs<16>(xa, tf, j0, 16, 8, p);
+        } else {
+            dif_regs2<16>(xa, xb, tf, j0, 16, 8, p);
+        }
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            smA[pad_idx(i0 + 16 * t)] = xa[t];
+            if (!sq) smB[pad_idx(i0 + 16 * t)] = xb[t];
+        }
+    }
+    __syncthreads();
+    // P3: M = 16, st = 1, fused product
+    {
+        const int i0 = tid << 4;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            xa[t] = smA[pad_idx(i0 + t)];
+            if (!sq) xb[t] = smB[pad_idx(i0 + t)];
+        }
+        if (sq) {
+            dif_regs<16>(xa, tf, 0, 1, 4, p);
+#pragma unroll
+            for (int t = 0; t < 16; ++t) xa[t] = mont_mul(xa[t], xa[t], p, pc.pinv);
+        } else {
+            dif_regs2<16>(xa, xb, tf, 0, 1, 4, p);
+#pragma unroll
+            for (int t = 0; t < 16; ++t) xa[t] = mont_mul(xa[t], xb[t], p, pc.pinv);
+        }
+        dit_regs<16>(xa, ti, 0, 1, 4, p);
+#pragma unroll
+        for (int t = 0; t < 16; ++t) smA[pad_idx(i0 + t)] = xa[t];
+    }
+    __syncthreads();
+    // P2'
+    {
+        const int j0 = tid & 15, i0 = ((tid >> 4) << 8) + j0;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) xa[t] = smA[pad_idx(i0 + 16 * t)];
+        dit_regs<16>(xa, ti, j0, 16, 8, p);
+#pragma unroll
+        for (int t = 0; t < 16; ++t) smA[pad_idx(i0 + 16 * t)] = xa[t];
+    }
+    __syncthreads();
+    // P1'
+    {
+#pragma unroll
+        for (int t = 0; t < 16; ++t) xa[t] = smA[pad_idx(tid + 256 * t)];
+        dit_regs<16>(xa, ti, tid, 256, 12, p);
+        uint32_t* Ar = YA + base;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            uint2 s = s_i[t];
+            Ar[tid + 256 * t] = mul_shoup(mul_shoup(xa[t], s.x, s.y, p), bi, bis, p);
+        }
     }
 }
 
@@ -216,16 +382,13 @@ __global__ void __launch_bounds__(512) k_col_inv(uint32_t* __restrict__ YA, int 
 #define FLAG_AGG 1u
 #define FLAG_INC 2u
 
-__device__ __forceinline__ void crt_coeff(const uint32_t* __restrict__ R, size_t L, int64_t j,
-                                          const ScaleArg& sc, uint64_t& lo, uint64_t& mid,
-                                          uint32_t& hi) {
+// Garner (ascending primes) + Horner compose of one coefficient from its
+// five residues (already scaled to the true coefficient residues).
+__device__ __forceinline__ void garner(const uint32_t (&r)[SBG_NP], uint64_t& lo, uint64_t& mid,
+                                       uint32_t& hi) {
     uint32_t v[SBG_NP];
 #pragma unroll
-    for (int q = 0; q < SBG_NP; ++q) {
-        uint32_t p = c_pr[q].p;
-        uint32_t r = __ldg(&R[(size_t)q * L + (size_t)j]);
-        v[q] = mul_shoup(r, sc.w[q], sc.ws[q], p);
-    }
+    for (int q = 0; q < SBG_NP; ++q) v[q] = r[q];
 #pragma unroll
     for (int i = 1; i < SBG_NP; ++i) {
         uint32_t p = c_pr[i].p;
@@ -284,31 +447,54 @@ __device__ __forceinline__ uint32_t gp_compose(uint32_t left, uint32_t right) {
 __global__ void __launch_bounds__(CRT_T) k_crt_carry(const uint32_t* __restrict__ R, int lgL,
                                                      int64_t cmin, int64_t cmax, int64_t off,
                                                      uint64_t* __restrict__ out, int64_t nout,
-                                                     ScaleArg sc, uint32_t* flags,
-                                                     uint32_t* err) {
+                                                     uint32_t* flags, uint32_t* err) {
     __shared__ uint32_t s_bid;
     __shared__ uint32_t s_warp[CRT_T / 32];
     __shared__ uint32_t s_cin;
-    const size_t L = (size_t)1 << lgL;
+    const int64_t L = (int64_t)1 << lgL;
     if (threadIdx.x == 0) s_bid = atomicAdd(&flags[0], 1u);
     __syncthreads();
     const uint32_t bid = s_bid;
     const int64_t m0 = (int64_t)bid * CRT_BLK + (int64_t)threadIdx.x * CRT_PER;
-
-    // sliding window over coefficients j = m + off - 2 .. m + off
-    auto coeff = [&](int64_t j, uint64_t& lo, uint64_t& mid, uint32_t& hi) {
+    const int64_t j0 = m0 + off;
+    // residues of coefficients j0-4 .. j0+15 arrive in 5 chunks of 4: one
+    // 16-byte load per prime when aligned and in range, else guarded scalars
+    const bool vec = ((j0 & 3) == 0) && (j0 >= 4) && (j0 + CRT_PER <= L);
+    uint32_t rr[SBG_NP][4];
+    auto fetch = [&](int c) {
+        const int64_t jb = j0 - 4 + 4 * c;
+        if (vec) {
+#pragma unroll
+            for (int q = 0; q < SBG_NP; ++q) {
+                uint4 v = __ldg(reinterpret_cast<const uint4*>(R + (size_t)q * L + jb));
+                rr[q][0] = v.x; rr[q][1] = v.y; rr[q][2] = v.z; rr[q][3] = v.w;
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int64_t j = jb + u;
+                const bool in = j >= cmin && j <= cmax;
+#pragma unroll
+                for (int q = 0; q < SBG_NP; ++q) rr[q][u] = in ? __ldg(&R[(size_t)q * L + j]) : 0u;
+            }
+        }
+    };
+    auto coeff = [&](int u, int64_t j, uint64_t& lo, uint64_t& mid, uint32_t& hi) {
         if (j >= cmin && j <= cmax) {
-            crt_coeff(R, L, j, sc, lo, mid, hi);
+            uint32_t r[SBG_NP];
+#pragma unroll
+            for (int q = 0; q < SBG_NP; ++q) r[q] = rr[q][u];
+            garner(r, lo, mid, hi);
         } else {
             lo = 0; mid = 0; hi = 0;
         }
     };
     uint64_t lo_a, mid_a, lo_b, mid_b, lo_c, mid_c;   // a = j-2, b = j-1, c = j
     uint32_t hi_a, hi_b, hi_c;
-    int64_t j0 = m0 + off;
-    coeff(j0 - 3, lo_a, mid_a, hi_a);   // slot j-3 -> becomes "a" after shift below
-    coeff(j0 - 2, lo_b, mid_b, hi_b);
-    coeff(j0 - 1, lo_c, mid_c, hi_c);
+    fetch(0);
+    coeff(1, j0 - 3, lo_a, mid_a, hi_a);
+    coeff(2, j0 - 2, lo_b, mid_b, hi_b);
+    coeff(3, j0 - 1, lo_c, mid_c, hi_c);
     // kk of limb m0 - 1: S = lo_{j0-1} + mid_{j0-2} + hi_{j0-3}
     uint32_t kk_prev;
     {
@@ -328,9 +514,10 @@ __global__ void __launch_bounds__(CRT_T) k_crt_carry(const uint32_t* __restrict_
     for (int k = 0; k < CRT_PER; ++k) {
         const int64_t m = m0 + k;
         if (m > nout) break;
+        if ((k & 3) == 0) fetch(1 + (k >> 2));
         lo_a = lo_b; mid_a = mid_b; hi_a = hi_b;
         lo_b = lo_c; mid_b = mid_c; hi_b = hi_c;
-        coeff(j0 + k, lo_c, mid_c, hi_c);
+        coeff(k & 3, j0 + k, lo_c, mid_c, hi_c);
         uint64_t s1 = lo_c + mid_b;
         uint32_t c1 = s1 < lo_c;
         uint64_t t = s1 + hi_a;
@@ -455,8 +642,6 @@ cudaError_t set_kernel_attributes() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_col_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_row, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     return e;
 }
@@ -472,7 +657,7 @@ cudaError_t upload_constants(cudaStream_t st) {
 }
 
 static cudaError_t gen_table(uint2* out, int n, int lgRoot, bool inverse, uint32_t stride,
-                             cudaStream_t st) {
+                             cudaStream_t st, bool per_resolution = false) {
     uint32_t roots[SBG_NP];
     for (int q = 0; q < SBG_NP; ++q) {
         uint32_t p = kPrimes[q];
@@ -486,17 +671,22 @@ static cudaError_t gen_table(uint2* out, int n, int lgRoot, bool inverse, uint32
     e = cudaMemcpyAsync(droots, roots, sizeof(roots), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         dim3 grid((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024, SBG_NP);
-        k_gen_pow<<<grid, 256, 0, st>>>(out, n, droots, stride);
+        if (per_resolution)
+            k_gen_res<<<grid, 256, 0, st>>>(out, droots);
+        else
+            k_gen_pow<<<grid, 256, 0, st>>>(out, n, droots, stride);
         e = cudaGetLastError();
     }
     cudaFreeAsync(droots, st);
     return e;
 }
 
+size_t master_table_entries() { return (size_t)SBG_NP * SBG_TW_N; }
+
 cudaError_t gen_master_tables(uint2* tw_f, uint2* tw_i, cudaStream_t st) {
-    cudaError_t e = gen_table(tw_f, SBG_TW_N, SBG_TW_LG, false, 1, st);
+    cudaError_t e = gen_table(tw_f, SBG_TW_N, SBG_TW_LG, false, 1, st, true);
     if (e != cudaSuccess) return e;
-    return gen_table(tw_i, SBG_TW_N, SBG_TW_LG, true, 1, st);
+    return gen_table(tw_i, SBG_TW_N, SBG_TW_LG, true, 1, st, true);
 }
 
 cudaError_t gen_len_tables(LenPlan* lp, cudaStream_t st) {
@@ -521,36 +711,41 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
     const size_t L = (size_t)1 << lgL;
     uint32_t* YA = ws;
     uint32_t* YB = ws + SBG_NP * L;
+    ScaleArg sc;
+    for (int q = 0; q < SBG_NP; ++q) {
+        sc.w[q] = lp->scale[q].w;
+        sc.ws[q] = lp->scale[q].ws;
+    }
     if (lgL <= SBG_SMALL_MAX_LG) {
         size_t smem = (size_t)2 * padded_len((int)L) * 4;
         KT_BEGIN(kt, KID_SMALL, st);
-        k_small<<<SBG_NP, 256, smem, st>>>(a, an, b, bn, sq, lgL, tw_f, tw_i, YA);
+        k_small<<<SBG_NP, 256, smem, st>>>(a, an, b, bn, sq, lgL, tw_f, tw_i, sc, YA);
         KT_END(kt, KID_SMALL, st);
         return cudaGetLastError();
     }
-    const int lgN2 = lp->lgN2, lgN1 = lp->lgN1;
+    const int lgN2 = lp->lgN2, lgN1 = lp->lgN1;   // lgN2 == ROW_LG
     int lgw = SBG_COL_POINTS_LG - lgN1;
     if (lgw > lgN2) lgw = lgN2;
     if (lgw < 0) lgw = 0;
     const int ntiles = 1 << (lgN2 - lgw);
     FsTables fsf{lp->fs_lo_f, lp->fs_hi_f, lp->hi_n};
     FsTables fsi{lp->fs_lo_i, lp->fs_hi_i, lp->hi_n};
-    size_t col_smem = (size_t)(1 << lgw) * (padded_len(1 << lgN1) + 1) * 4;
+    size_t col_smem = (size_t)padded_len(1 << (lgN1 + lgw)) * 4;
+    if (num_passes(lgN1) == 1) col_smem = 0;
     int nops = sq ? 1 : 2;
     KT_BEGIN(kt, KID_COL_FWD, st);
-    k_col_fwd<<<nops * ntiles * SBG_NP, 512, col_smem, st>>>(a, an, b, bn, lgN1, lgN2, lgw, fsf,
-                                                             tw_f, YA, YB);
+    k_col_fwd<<<nops * ntiles * SBG_NP, 512, col_smem, st>>>(a, an, b, bn, lgN1, lgN2, lgw, tw_f,
+                                                             YA, YB, nops);
     KT_END(kt, KID_COL_FWD, st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    size_t row_smem = (size_t)2 * padded_len(1 << lgN2) * 4;
     KT_BEGIN(kt, KID_ROW, st);
-    k_row<<<(1 << lgN1) * SBG_NP, 256, row_smem, st>>>(YA, YB, sq, lgN1, lgN2, tw_f, tw_i);
+    k_row12<<<(1 << lgN1) * SBG_NP, 256, 0, st>>>(YA, YB, sq, lgN1, fsf, fsi, sc, tw_f, tw_i);
     KT_END(kt, KID_ROW, st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     KT_BEGIN(kt, KID_COL_INV, st);
-    k_col_inv<<<ntiles * SBG_NP, 512, col_smem, st>>>(YA, lgN1, lgN2, lgw, fsi, tw_i);
+    k_col_inv<<<ntiles * SBG_NP, 512, col_smem, st>>>(YA, lgN1, lgN2, lgw, tw_i);
     KT_END(kt, KID_COL_INV, st);
     return cudaGetLastError();
 }
@@ -561,18 +756,13 @@ cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int6
                              int64_t cmax, int64_t off, uint64_t* out, int64_t nout,
                              uint32_t* flags, uint32_t* err, cudaStream_t st,
                              KTimer* kt) {
-    ScaleArg sc;
-    for (int q = 0; q < SBG_NP; ++q) {
-        sc.w[q] = lp->scale[q].w;
-        sc.ws[q] = lp->scale[q].ws;
-    }
+    (void)lp;
     // blocks cover limbs [0, nout] (limb nout is the spill check)
     int64_t nblk = (nout + 1 + CRT_BLK - 1) / CRT_BLK;
     cudaError_t e = cudaMemsetAsync(flags, 0, (1 + nblk) * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     KT_BEGIN(kt, KID_CRT, st);
-    k_crt_carry<<<(unsigned)nblk, CRT_T, 0, st>>>(R, lgL, cmin, cmax, off, out, nout, sc, flags,
-                                                  err);
+    k_crt_carry<<<(unsigned)nblk, CRT_T, 0, st>>>(R, lgL, cmin, cmax, off, out, nout, flags, err);
     KT_END(kt, KID_CRT, st);
     return cudaGetLastError();
 }
