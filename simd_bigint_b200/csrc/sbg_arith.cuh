@@ -27,6 +27,8 @@ struct PrimeConst {
     uint32_t c32s;     // Shoup companion of c32: floor(c32 * 2^32 / p)
     uint32_t ones;     // Shoup companion of 1: floor(2^32 / p)
     uint32_t g;        // a generator of (Z/p)^*
+    uint32_t mu_lo;    // floor(2^64 / p), low and high words: division-free
+    uint32_t mu_hi;    //   Shoup companions (shoup_fast)
 };
 
 // host-side copy of the primes (ascending)
@@ -53,6 +55,14 @@ __device__ __forceinline__ uint32_t mul_shoup_lazy(uint32_t x, uint32_t w, uint3
 }
 __device__ __forceinline__ uint32_t mul_shoup(uint32_t x, uint32_t w, uint32_t ws, uint32_t p) {
     return red1(mul_shoup_lazy(x, w, ws, p), p);
+}
+
+// floor(w * 2^32 / p) for w < p without a division: w * floor(2^64 / p) / 2^32
+// underestimates by at most one, which the remainder test corrects.
+__device__ __forceinline__ uint32_t shoup_fast(uint32_t w, const PrimeConst& c) {
+    uint32_t est = __umulhi(w, c.mu_lo) + w * c.mu_hi;
+    uint32_t r = 0u - est * c.p;                // (w * 2^32 - est * p) mod 2^32, in [0, 2p)
+    return est + (r >= c.p ? 1u : 0u);
 }
 
 // Montgomery product a * b * 2^-32 mod p for a, b < p; result in [0, p).

@@ -20,7 +20,6 @@ __constant__ CrtConst c_crt;
 
 #define SBG_SMALL_MAX_LG 12
 #define SBG_ROW_LG 12
-#define SBG_COL_POINTS_LG 14     // points per column-pass CTA
 #define SBG_FS_LO_LG 13
 #define SBG_FS_LO_N (1 << SBG_FS_LO_LG)
 
@@ -105,127 +104,238 @@ __device__ __forceinline__ uint32_t fs_value(const FsTables& fs, int q, uint32_t
     return mul_shoup(a.x, b.x, b.y, p);
 }
 
-// Column tiles: w adjacent columns, interleaved in shared memory
-// (point (i, g) at linear index i*w + g, padded one word per 16) so that a
-// warp's lanes -- column fastest -- touch consecutive words at every pass.
-__device__ __forceinline__ int col_addr(int i, int g, int lgw) { return pad_idx((i << lgw) + g); }
+// Column tiles.  A CTA owns w adjacent columns (all N1 rows) of one operand
+// and one prime: 2^14 points (fewer when N1 * N2 is smaller).  Each thread
+// owns a PAIR of adjacent columns of one group per pass, so one twiddle load
+// serves two columns and the global accesses are 16-byte (two limbs) or
+// 8-byte (two residues) per row.  Columns live in shared memory as separate
+// planes (padded one word per 16, plane stride COL_LD), and every stride is a
+// compile-time constant of the column length.
+__host__ __device__ constexpr int col_lgw(int lgN1) {
+    return (14 - lgN1) > 12 ? 12 : ((14 - lgN1) < 1 ? 1 : (14 - lgN1));
+}
+__host__ __device__ constexpr int col_ld(int lgN1) { return padded_len(1 << lgN1) + 1; }
+// Column radix schedule: passes of 16 from the top, the remainder last.  (A
+// radix-32 last pass that absorbs a one-level remainder measured slower on
+// B200: 32 live points per thread under the 64-register cap spill.)
+#define SBG_COL_R32 0
+__host__ __device__ constexpr int col_np(int lg) {
+    return (SBG_COL_R32 && (lg & 3) == 1 && lg >= 5) ? (lg >> 2) : num_passes(lg);
+}
+__host__ __device__ constexpr int prl(int lg, int k) {
+    return (SBG_COL_R32 && (lg & 3) == 1 && lg >= 5) ? (k < (lg >> 2) - 1 ? 4 : 5)
+                                                     : (k < (lg >> 2) ? 4 : (lg & 3));
+}
+__host__ __device__ constexpr int lgm_of(int lg, int k) {
+    int m = lg;
+    for (int i = 0; i < k; ++i) m -= prl(lg, i);
+    return m;
+}
+__host__ __device__ constexpr int col_smem_bytes(int lgN1) {
+    return col_np(lgN1) > 1 ? (1 << col_lgw(lgN1)) * col_ld(lgN1) * 4 : 0;
+}
 
-// One column pass of radix R over the tile.  FWD: DIF; else DIT.
-// SRC/DST: 0 = shared memory, 1 = global.  Forward global source = limbs
-// (residue taken on the fly); inverse global source / both global
-// destinations = the residue array Y (+ q * L already applied).
-template <int R, bool FWD>
-__device__ __forceinline__ void col_pass(uint32_t* sm, int lgN1, int lgN2, int lgw, int lgM,
-                                         bool src_global, bool dst_global,
-                                         const uint64_t* __restrict__ X, int64_t xn,
-                                         uint32_t* __restrict__ Y, int c0,
-                                         const uint2* __restrict__ tw, const PrimeConst& pc) {
-    constexpr int r = RLog<R>::v;
-    const int lgst = lgM - r;
-    const int st = 1 << lgst;
-    const int w = 1 << lgw;
-    const int total = 1 << (lgw + lgN1 - r);
-    for (int gid = threadIdx.x; gid < total; gid += blockDim.x) {
-        const int g = gid & (w - 1);
-        const int rest = gid >> lgw;
-        const int j0 = rest & (st - 1);
-        const int blk = rest >> lgst;
-        const int i0 = (blk << lgM) + j0;
-        uint32_t x[R];
-        if (src_global) {
-#pragma unroll
-            for (int t = 0; t < R; ++t) {
-                const int64_t n = ((int64_t)(i0 + st * t) << lgN2) + c0 + g;
-                if (FWD)
-                    x[t] = n < xn ? limb_residue(__ldg(&X[n]), pc) : 0u;
-                else
-                    x[t] = Y[n];
-            }
-        } else {
-#pragma unroll
-            for (int t = 0; t < R; ++t) x[t] = sm[col_addr(i0 + st * t, g, lgw)];
-        }
-        if (FWD)
-            dif_regs<R>(x, tw, j0, st, lgM, pc.p);
-        else
-            dit_regs<R>(x, tw, j0, st, lgM, pc.p);
-        if (dst_global) {
-#pragma unroll
-            for (int t = 0; t < R; ++t) Y[((size_t)(i0 + st * t) << lgN2) + c0 + g] = x[t];
-        } else {
-#pragma unroll
-            for (int t = 0; t < R; ++t) sm[col_addr(i0 + st * t, g, lgw)] = x[t];
-        }
+template <int LGST>
+__device__ __forceinline__ int padded_at(int i0, int t) {
+    constexpr int ST = 1 << LGST;
+    if constexpr (LGST >= 4) {
+        return pad_idx(i0) + t * (ST + (ST >> 4));
+    } else {
+        return pad_idx(i0 + ST * t);
     }
 }
 
-template <bool FWD>
-__device__ __forceinline__ void col_pass_dispatch(int rlg, uint32_t* sm, int lgN1, int lgN2,
-                                                  int lgw, int lgM, bool sg, bool dg,
-                                                  const uint64_t* X, int64_t xn, uint32_t* Y,
-                                                  int c0, const uint2* tw, const PrimeConst& pc) {
-    switch (rlg) {
-        case 4: col_pass<16, FWD>(sm, lgN1, lgN2, lgw, lgM, sg, dg, X, xn, Y, c0, tw, pc); break;
-        case 3: col_pass<8, FWD>(sm, lgN1, lgN2, lgw, lgM, sg, dg, X, xn, Y, c0, tw, pc); break;
-        case 2: col_pass<4, FWD>(sm, lgN1, lgN2, lgw, lgM, sg, dg, X, xn, Y, c0, tw, pc); break;
-        case 1: col_pass<2, FWD>(sm, lgN1, lgN2, lgw, lgM, sg, dg, X, xn, Y, c0, tw, pc); break;
-        default: break;
+// Pass K (0-based, forward numbering) of the column transform.
+template <int LGN1, int K, bool FWD>
+__device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restrict__ X,
+                                           int64_t xn, uint32_t* __restrict__ Y, int c0,
+                                           const uint2* __restrict__ tw, const PrimeConst& pc) {
+    constexpr int NP = col_np(LGN1);
+    constexpr int r = prl(LGN1, K);
+    constexpr int R = 1 << r;
+    constexpr int LGM = lgm_of(LGN1, K);
+    constexpr int LGST = LGM - r;
+    constexpr int ST = 1 << LGST;
+    constexpr int LGW = col_lgw(LGN1);
+    constexpr int LD = col_ld(LGN1);
+    constexpr int TOTAL = (1 << (LGW - 1)) << (LGN1 - r);
+    constexpr bool SRC_G = FWD ? (K == 0) : (K == NP - 1);
+    constexpr bool DST_G = FWD ? (K == NP - 1) : (K == 0);
+    const uint32_t p = pc.p;
+    if constexpr (R == 32) {
+        // single-column groups, column index fastest across lanes
+        constexpr int TOT1 = 1 << (LGW + LGN1 - 5);
+#pragma unroll 1
+        for (int gid = threadIdx.x; gid < TOT1; gid += blockDim.x) {
+            const int g = gid & ((1 << LGW) - 1);
+            const int rest = gid >> LGW;
+            const int j0 = rest & (ST - 1);
+            const int blk = rest >> LGST;
+            const int i0 = (blk << LGM) + j0;
+            uint32_t x[32];
+            if constexpr (SRC_G) {
+                const int64_t n0 = ((int64_t)i0 << SBG_ROW_LG) + c0 + g;
+#pragma unroll
+                for (int t = 0; t < 32; ++t) {
+                    const int64_t n = n0 + ((int64_t)(ST * t) << SBG_ROW_LG);
+                    if constexpr (FWD)
+                        x[t] = n < xn ? limb_residue(__ldg(&X[n]), pc) : 0u;
+                    else
+                        x[t] = Y[n];
+                }
+            } else {
+                const uint32_t* s0 = sm + g * LD;
+#pragma unroll
+                for (int t = 0; t < 32; ++t) x[t] = s0[padded_at<LGST>(i0, t)];
+            }
+            if constexpr (FWD)
+                dif_regs<32>(x, tw, j0, ST, LGM, p);
+            else
+                dit_regs<32>(x, tw, j0, ST, LGM, p);
+            if constexpr (DST_G) {
+                const int64_t n0 = ((int64_t)i0 << SBG_ROW_LG) + c0 + g;
+#pragma unroll
+                for (int t = 0; t < 32; ++t) Y[n0 + ((int64_t)(ST * t) << SBG_ROW_LG)] = x[t];
+            } else {
+                uint32_t* s0 = sm + g * LD;
+#pragma unroll
+                for (int t = 0; t < 32; ++t) s0[padded_at<LGST>(i0, t)] = x[t];
+            }
+        }
+    } else {
+#pragma unroll 1
+    for (int gid = threadIdx.x; gid < TOTAL; gid += blockDim.x) {
+        const int j0 = gid & (ST - 1);
+        const int rest = gid >> LGST;
+        const int blk = rest & ((1 << (LGN1 - LGM)) - 1);
+        const int cp = rest >> (LGN1 - LGM);
+        const int i0 = (blk << LGM) + j0;
+        const int g0 = 2 * cp;
+        uint32_t x[R], y[R];
+        if constexpr (SRC_G) {
+            const int64_t n0 = ((int64_t)i0 << SBG_ROW_LG) + c0 + g0;
+            if constexpr (FWD) {
+                const bool al16 = (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+#pragma unroll
+                for (int t = 0; t < R; ++t) {
+                    const int64_t n = n0 + ((int64_t)(ST * t) << SBG_ROW_LG);
+                    if (al16 && n + 1 < xn) {
+                        ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(X + n));
+                        x[t] = limb_residue(v.x, pc);
+                        y[t] = limb_residue(v.y, pc);
+                    } else {
+                        x[t] = n < xn ? limb_residue(__ldg(&X[n]), pc) : 0u;
+                        y[t] = n + 1 < xn ? limb_residue(__ldg(&X[n + 1]), pc) : 0u;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int t = 0; t < R; ++t) {
+                    const int64_t n = n0 + ((int64_t)(ST * t) << SBG_ROW_LG);
+                    uint2 v = *reinterpret_cast<const uint2*>(Y + n);
+                    x[t] = v.x;
+                    y[t] = v.y;
+                }
+            }
+        } else {
+            const uint32_t* s0 = sm + g0 * LD;
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int a = padded_at<LGST>(i0, t);
+                x[t] = s0[a];
+                y[t] = s0[LD + a];
+            }
+        }
+        if constexpr (FWD)
+            dif_regs2<R>(x, y, tw, j0, ST, LGM, p);
+        else
+            dit_regs2<R>(x, y, tw, j0, ST, LGM, p);
+        if constexpr (DST_G) {
+            const int64_t n0 = ((int64_t)i0 << SBG_ROW_LG) + c0 + g0;
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int64_t n = n0 + ((int64_t)(ST * t) << SBG_ROW_LG);
+                *reinterpret_cast<uint2*>(Y + n) = make_uint2(x[t], y[t]);
+            }
+        } else {
+            uint32_t* s0 = sm + g0 * LD;
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int a = padded_at<LGST>(i0, t);
+                s0[a] = x[t];
+                s0[LD + a] = y[t];
+            }
+        }
+    }
     }
 }
 
 // K1: limbs -> residues -> column DIF (bit-reversed rows) for one operand,
-// one prime, one tile of w columns.  Block order: prime slowest, so the CTAs
-// resident on an SM share one prime's twiddle table.
-__global__ void __launch_bounds__(512) k_col_fwd(const uint64_t* __restrict__ a, int64_t an,
+// one prime, one tile.  Block order: prime slowest, so the CTAs resident on
+// an SM share one prime's twiddle table.
+template <int LGN1>
+__global__ void __launch_bounds__(512, 2) k_col_fwd(const uint64_t* __restrict__ a, int64_t an,
                                                  const uint64_t* __restrict__ b, int64_t bn,
-                                                 int lgN1, int lgN2, int lgw,
                                                  const uint2* __restrict__ twf,
                                                  uint32_t* __restrict__ YA,
                                                  uint32_t* __restrict__ YB, int nops) {
     extern __shared__ uint32_t sm[];
-    const int ntiles = 1 << (lgN2 - lgw);
-    const int per_q = ntiles * nops;
+    constexpr int NP = col_np(LGN1);
+    constexpr int LGW = col_lgw(LGN1);
+    constexpr int NTILES = 1 << (SBG_ROW_LG - LGW);
+    const int per_q = NTILES * nops;
     const int q = blockIdx.x / per_q;
     const int rest = blockIdx.x - q * per_q;
-    const int tile = rest % ntiles;
-    const int op = rest / ntiles;
+    const int tile = rest % NTILES;
+    const int op = rest / NTILES;
     const uint64_t* X = op ? b : a;
     const int64_t xn = op ? bn : an;
-    uint32_t* Y = (op ? YB : YA) + ((size_t)q << (lgN1 + lgN2));
+    uint32_t* Y = (op ? YB : YA) + ((size_t)q << (LGN1 + SBG_ROW_LG));
     const PrimeConst pc = c_pr[q];
     const uint2* tw = twf + (size_t)q * SBG_TW_N;
-    const int c0 = tile << lgw;
-    const int np = num_passes(lgN1);
-    int lgM = lgN1;
-    for (int k = 0; k < np; ++k) {
-        const int rlg = pass_radix_lg(lgN1, k);
-        col_pass_dispatch<true>(rlg, sm, lgN1, lgN2, lgw, lgM, k == 0, k == np - 1, X, xn, Y, c0,
-                                tw, pc);
-        if (k < np - 1) __syncthreads();
-        lgM -= rlg;
+    const int c0 = tile << LGW;
+    col_pass_t<LGN1, 0, true>(sm, X, xn, Y, c0, tw, pc);
+    if constexpr (NP > 1) {
+        __syncthreads();
+        col_pass_t<LGN1, (NP > 1 ? 1 : 0), true>(sm, X, xn, Y, c0, tw, pc);
+    }
+    if constexpr (NP > 2) {
+        __syncthreads();
+        col_pass_t<LGN1, (NP > 2 ? 2 : 0), true>(sm, X, xn, Y, c0, tw, pc);
+    }
+    if constexpr (NP > 3) {
+        __syncthreads();
+        col_pass_t<LGN1, (NP > 3 ? 3 : 0), true>(sm, X, xn, Y, c0, tw, pc);
     }
 }
 
 // K3: column DIT (reverse of K1), in place, natural row order out.
-__global__ void __launch_bounds__(512) k_col_inv(uint32_t* __restrict__ YA, int lgN1, int lgN2,
-                                                 int lgw, const uint2* __restrict__ twi) {
+template <int LGN1>
+__global__ void __launch_bounds__(512, 2) k_col_inv(uint32_t* __restrict__ YA,
+                                                 const uint2* __restrict__ twi) {
     extern __shared__ uint32_t sm[];
-    const int ntiles = 1 << (lgN2 - lgw);
-    const int q = blockIdx.x / ntiles;
-    const int tile = blockIdx.x - q * ntiles;
-    uint32_t* Y = YA + ((size_t)q << (lgN1 + lgN2));
+    constexpr int NP = col_np(LGN1);
+    constexpr int LGW = col_lgw(LGN1);
+    constexpr int NTILES = 1 << (SBG_ROW_LG - LGW);
+    const int q = blockIdx.x / NTILES;
+    const int tile = blockIdx.x - q * NTILES;
+    uint32_t* Y = YA + ((size_t)q << (LGN1 + SBG_ROW_LG));
     const PrimeConst pc = c_pr[q];
     const uint2* tw = twi + (size_t)q * SBG_TW_N;
-    const int c0 = tile << lgw;
-    const int np = num_passes(lgN1);
-    for (int k = np - 1; k >= 0; --k) {
-        int lgM = lgN1;
-        for (int kk = 0; kk < k; ++kk) lgM -= pass_radix_lg(lgN1, kk);
-        const int rlg = pass_radix_lg(lgN1, k);
-        col_pass_dispatch<false>(rlg, sm, lgN1, lgN2, lgw, lgM, k == np - 1, k == 0, nullptr, 0,
-                                 Y, c0, tw, pc);
-        if (k > 0) __syncthreads();
+    const int c0 = tile << LGW;
+    if constexpr (NP > 3) {
+        col_pass_t<LGN1, (NP > 3 ? 3 : 0), false>(sm, nullptr, 0, Y, c0, tw, pc);
+        __syncthreads();
     }
+    if constexpr (NP > 2) {
+        col_pass_t<LGN1, (NP > 2 ? 2 : 0), false>(sm, nullptr, 0, Y, c0, tw, pc);
+        __syncthreads();
+    }
+    if constexpr (NP > 1) {
+        col_pass_t<LGN1, (NP > 1 ? 1 : 0), false>(sm, nullptr, 0, Y, c0, tw, pc);
+        __syncthreads();
+    }
+    col_pass_t<LGN1, 0, false>(sm, nullptr, 0, Y, c0, tw, pc);
 }
 
 // K2: one row of N2 = 2^12 points for one prime, 256 threads.
@@ -238,7 +348,7 @@ __global__ void __launch_bounds__(512) k_col_inv(uint32_t* __restrict__ YA, int 
 // register group, so that stage never touches shared memory.
 #define ROW_LG 12
 #define ROW_N (1 << ROW_LG)
-__global__ void __launch_bounds__(256) k_row12(uint32_t* __restrict__ YA,
+__global__ void __launch_bounds__(256, 4) k_row12(uint32_t* __restrict__ YA,
                                                const uint32_t* __restrict__ YB, int sq, int lgN1,
                                                FsTables fsf, FsTables fsi, ScaleArg sc,
                                                const uint2* __restrict__ twf,
@@ -262,13 +372,13 @@ __global__ void __launch_bounds__(256) k_row12(uint32_t* __restrict__ YA,
     if (tid < 16) {
         uint32_t e = (k1 * 256u * (uint32_t)tid) & Lmask;
         uint32_t v = fs_value(fsf, q, e, p);
-        s_f[tid] = make_uint2(v, shoup_of(v, p));
+        s_f[tid] = make_uint2(v, shoup_fast(v, pc));
         uint32_t vi = mul_shoup(fs_value(fsi, q, e, p), sc.w[q], sc.ws[q], p);
-        s_i[tid] = make_uint2(vi, shoup_of(vi, p));
+        s_i[tid] = make_uint2(vi, shoup_fast(vi, pc));
     }
     const uint32_t eb = k1 * (uint32_t)tid;
-    const uint32_t bf = fs_value(fsf, q, eb, p), bfs = shoup_of(bf, p);
-    const uint32_t bi = fs_value(fsi, q, eb, p), bis = shoup_of(bi, p);
+    const uint32_t bf = fs_value(fsf, q, eb, p), bfs = shoup_fast(bf, pc);
+    const uint32_t bi = fs_value(fsi, q, eb, p), bis = shoup_fast(bi, pc);
     __syncthreads();
 
     uint32_t xa[16], xb[16];
@@ -510,7 +620,7 @@ __global__ void __launch_bounds__(CRT_T) k_crt_carry(const uint32_t* __restrict_
     bool has_v = false;         // owns limb nout (the spill limb, never stored)
     uint64_t zv = 0;
     uint32_t kv = 0;
-#pragma unroll 1
+#pragma unroll
     for (int k = 0; k < CRT_PER; ++k) {
         const int64_t m = m0 + k;
         if (m > nout) break;
@@ -636,11 +746,23 @@ __global__ void __launch_bounds__(CRT_T) k_crt_carry(const uint32_t* __restrict_
 // launchers
 // ------------------------------------------------------------------------
 // per-device kernel attributes (called once per context, device current)
+template <int LGN1>
+static cudaError_t col_attr() {
+    const int big = 200 * 1024;
+    cudaError_t e = cudaFuncSetAttribute(k_col_fwd<LGN1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_col_inv<LGN1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    return e;
+}
+
+#define SBG_COL_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13)
+
 cudaError_t set_kernel_attributes() {
     const int big = 200 * 1024;
-    cudaError_t e = cudaFuncSetAttribute(k_col_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_col_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaError_t e = cudaSuccess;
+#define SBG_ATTR(n) if (e == cudaSuccess) e = col_attr<n>();
+    SBG_COL_CASES(SBG_ATTR)
+#undef SBG_ATTR
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     return e;
@@ -723,19 +845,23 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
         KT_END(kt, KID_SMALL, st);
         return cudaGetLastError();
     }
-    const int lgN2 = lp->lgN2, lgN1 = lp->lgN1;   // lgN2 == ROW_LG
-    int lgw = SBG_COL_POINTS_LG - lgN1;
-    if (lgw > lgN2) lgw = lgN2;
-    if (lgw < 0) lgw = 0;
-    const int ntiles = 1 << (lgN2 - lgw);
+    const int lgN1 = lp->lgN1;   // rows: 2^lgN1, columns: 2^12
     FsTables fsf{lp->fs_lo_f, lp->fs_hi_f, lp->hi_n};
     FsTables fsi{lp->fs_lo_i, lp->fs_hi_i, lp->hi_n};
-    size_t col_smem = (size_t)padded_len(1 << (lgN1 + lgw)) * 4;
-    if (num_passes(lgN1) == 1) col_smem = 0;
-    int nops = sq ? 1 : 2;
+    const int nops = sq ? 1 : 2;
+    const int ntiles = 1 << (SBG_ROW_LG - col_lgw(lgN1));
+    const size_t col_smem = (size_t)col_smem_bytes(lgN1);
     KT_BEGIN(kt, KID_COL_FWD, st);
-    k_col_fwd<<<nops * ntiles * SBG_NP, 512, col_smem, st>>>(a, an, b, bn, lgN1, lgN2, lgw, tw_f,
-                                                             YA, YB, nops);
+    switch (lgN1) {
+#define SBG_LAUNCH_F(n)                                                                  \
+    case n:                                                                              \
+        k_col_fwd<n><<<nops * ntiles * SBG_NP, 512, col_smem, st>>>(a, an, b, bn, tw_f, YA, \
+                                                                    YB, nops);           \
+        break;
+        SBG_COL_CASES(SBG_LAUNCH_F)
+#undef SBG_LAUNCH_F
+        default: return cudaErrorInvalidValue;
+    }
     KT_END(kt, KID_COL_FWD, st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -745,7 +871,13 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     KT_BEGIN(kt, KID_COL_INV, st);
-    k_col_inv<<<ntiles * SBG_NP, 512, col_smem, st>>>(YA, lgN1, lgN2, lgw, tw_i);
+    switch (lgN1) {
+#define SBG_LAUNCH_I(n)                                                          \
+    case n: k_col_inv<n><<<ntiles * SBG_NP, 512, col_smem, st>>>(YA, tw_i); break;
+        SBG_COL_CASES(SBG_LAUNCH_I)
+#undef SBG_LAUNCH_I
+        default: return cudaErrorInvalidValue;
+    }
     KT_END(kt, KID_COL_INV, st);
     return cudaGetLastError();
 }

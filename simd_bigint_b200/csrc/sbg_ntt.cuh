@@ -139,11 +139,11 @@ __device__ __forceinline__ void ntt_pass(uint32_t* buf, int ld, int G, int lgS, 
 }
 
 // Radix schedule: passes of 16 from the top, the remainder (1..3 levels) last.
-__host__ __device__ __forceinline__ int pass_radix_lg(int lgS, int k) {
+__host__ __device__ constexpr int pass_radix_lg(int lgS, int k) {
     int full = lgS >> 2;
     return k < full ? 4 : (lgS & 3);
 }
-__host__ __device__ __forceinline__ int num_passes(int lgS) {
+__host__ __device__ constexpr int num_passes(int lgS) {
     return (lgS >> 2) + ((lgS & 3) ? 1 : 0);
 }
 

@@ -38,6 +38,9 @@ void host_prime_consts(PrimeConst out[SBG_NP]) {
         c.c32s = host_shoup(c.c32, p);
         c.ones = host_shoup(1u, p);
         c.g = kGenerators[q];
+        unsigned __int128 mu = (((unsigned __int128)1) << 64) / p;
+        c.mu_lo = (uint32_t)(uint64_t)mu;
+        c.mu_hi = (uint32_t)((uint64_t)mu >> 32);
         out[q] = c;
     }
 }
