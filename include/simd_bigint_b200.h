@@ -105,6 +105,24 @@ int sbg_nt_mul(uint64_t *rp, const uint64_t *ap, ptrdiff_t an, const uint64_t *b
  *                                                  -- reference include/ntmul.h:77 */
 int sbg_nt_sqr(uint64_t *rp, const uint64_t *ap, ptrdiff_t an);
 
+/* ---- allocation-free multiply -------------------------------------------------
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory when they multiply -- programs that reserve all GPU memory up front,
+ * plug-ins inside a host that owns the device allocator, latency-critical
+ * loops that cannot take cudaMalloc's implicit synchronisation.
+ * rp[0 .. an+bn) = {ap, an} * {bp, bn} on DEVICE pointers, queued on `stream`
+ * (NULL: the default stream), for an + bn <= SBG_NOALLOC_MAX_LIMBS; larger
+ * products return SBG_EBAND.  Its scratch and twiddle tables are static
+ * device arrays of the library (about 740 KB, held on every GPU that loads it
+ * until exit); the first call on a device fills the tables and synchronises
+ * `stream`, so make that first call before any stream capture.  All calls
+ * share one scratch array: calls that overlap on the GPU race and must be
+ * ordered by the caller.  Makes no cudaMalloc / cudaFree call. */
+#define SBG_NOALLOC_MAX_LIMBS 4097
+int sbg_mul_noalloc(uint64_t *rp, const uint64_t *ap, int64_t an, const uint64_t *bp, int64_t bn,
+                    void *stream);
+int64_t sbg_noalloc_max_limbs(void);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 
 /* Register-only throughput of the transform butterfly on `device`
