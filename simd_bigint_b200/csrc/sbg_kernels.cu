@@ -115,17 +115,12 @@ __host__ __device__ constexpr int col_lgw(int lgN1) {
     return (14 - lgN1) > 12 ? 12 : ((14 - lgN1) < 1 ? 1 : (14 - lgN1));
 }
 __host__ __device__ constexpr int col_ld(int lgN1) { return padded_len(1 << lgN1) + 1; }
-// Column radix schedule: passes of 16 from the top, the remainder last.  (A
-// radix-32 last pass that absorbs a one-level remainder measured slower on
-// B200: 32 live points per thread under the 64-register cap spill.)
-#define SBG_COL_R32 0
-__host__ __device__ constexpr int col_np(int lg) {
-    return (SBG_COL_R32 && (lg & 3) == 1 && lg >= 5) ? (lg >> 2) : num_passes(lg);
-}
-__host__ __device__ constexpr int prl(int lg, int k) {
-    return (SBG_COL_R32 && (lg & 3) == 1 && lg >= 5) ? (k < (lg >> 2) - 1 ? 4 : 5)
-                                                     : (k < (lg >> 2) ? 4 : (lg & 3));
-}
+// Column radix schedule: passes of 16 from the top, the remainder (1..3
+// levels) last.  (Measured alternatives on B200 at 2^25 points: a radix-32
+// last pass spills under the 64-register cap, and the remainder first costs
+// an extra shared-memory round trip in the forward kernel; both were slower.)
+__host__ __device__ constexpr int col_np(int lg) { return num_passes(lg); }
+__host__ __device__ constexpr int prl(int lg, int k) { return k < (lg >> 2) ? 4 : (lg & 3); }
 __host__ __device__ constexpr int lgm_of(int lg, int k) {
     int m = lg;
     for (int i = 0; i < k; ++i) m -= prl(lg, i);
@@ -134,6 +129,8 @@ __host__ __device__ constexpr int lgm_of(int lg, int k) {
 __host__ __device__ constexpr int col_smem_bytes(int lgN1) {
     return col_np(lgN1) > 1 ? (1 << col_lgw(lgN1)) * col_ld(lgN1) * 4 : 0;
 }
+
+#define COL_THREADS 512
 
 template <int LGST>
 __device__ __forceinline__ int padded_at(int i0, int t) {
@@ -166,7 +163,7 @@ __device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restr
         // single-column groups, column index fastest across lanes
         constexpr int TOT1 = 1 << (LGW + LGN1 - 5);
 #pragma unroll 1
-        for (int gid = threadIdx.x; gid < TOT1; gid += blockDim.x) {
+        for (int gid = threadIdx.x; gid < TOT1; gid += COL_THREADS) {
             const int g = gid & ((1 << LGW) - 1);
             const int rest = gid >> LGW;
             const int j0 = rest & (ST - 1);
@@ -203,8 +200,14 @@ __device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restr
             }
         }
     } else {
-#pragma unroll 1
-    for (int gid = threadIdx.x; gid < TOTAL; gid += blockDim.x) {
+    // groups per thread is a compile-time constant (TOTAL / COL_THREADS, or 1
+    // when the tile has fewer groups than threads): unrolled, so every
+    // group's global loads are in flight together
+    constexpr int ITER = TOTAL >= COL_THREADS ? TOTAL / COL_THREADS : 1;
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int gid = threadIdx.x + it * COL_THREADS;
+        if (TOTAL < COL_THREADS && gid >= TOTAL) break;
         const int j0 = gid & (ST - 1);
         const int rest = gid >> LGST;
         const int blk = rest & ((1 << (LGN1 - LGM)) - 1);
@@ -271,8 +274,7 @@ __device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restr
 }
 
 // K1: limbs -> residues -> column DIF (bit-reversed rows) for one operand,
-// one prime, one tile.  Block order: prime slowest, so the CTAs resident on
-// an SM share one prime's twiddle table.
+// one prime, one tile.
 template <int LGN1>
 __global__ void __launch_bounds__(512, 2) k_col_fwd(const uint64_t* __restrict__ a, int64_t an,
                                                  const uint64_t* __restrict__ b, int64_t bn,
@@ -283,6 +285,7 @@ __global__ void __launch_bounds__(512, 2) k_col_fwd(const uint64_t* __restrict__
     constexpr int NP = col_np(LGN1);
     constexpr int LGW = col_lgw(LGN1);
     constexpr int NTILES = 1 << (SBG_ROW_LG - LGW);
+    // prime slowest: the CTAs resident on an SM share one prime's twiddles
     const int per_q = NTILES * nops;
     const int q = blockIdx.x / per_q;
     const int rest = blockIdx.x - q * per_q;
