@@ -38,6 +38,7 @@ WORKLOADS = {
     "mul2p22": ("mul", 1 << 22, 1 << 22),
     "mul2p24x2p20": ("mul", 1 << 24, 1 << 20),
     "mul16k": ("mul", 16384, 16384),
+    "batch4096": ("batch", 4096, 0),     # the batched mixed-size configuration
 }
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
@@ -261,6 +262,210 @@ def cpu_bounded(op: str, an: int, bn: int) -> dict:
     return cpu_run(op, an, bn, threads, steps=2, warmup=1)
 
 
+# ------------------------------------------------------- batched workload --
+def _batch_worker(shapes, seed, steps, warmup, barrier, queue):
+    """One baseline process: its share of the batch through the reference
+    router (simd_mpn_mul while 2(an+bn) <= 2^19, else nt_mul / nt_sqr)."""
+    try:
+        from oracle import oracle as O
+        from simd_bigint_b200.workloads import fill_limbs
+        rng = np.random.default_rng(seed)
+        ops = []
+        for kind, an, bn in shapes:
+            a = fill_limbs(an, rng)
+            b = a if kind == 1 else fill_limbs(bn, rng)
+            ops.append((kind, a, b))
+        use_ref = O.ref_available()
+
+        def one():
+            for kind, a, b in ops:
+                if use_ref:
+                    r = np.zeros(len(a) + len(b) + 2, dtype=np.uint64)
+                    O.ref().sbref_mul_router(kind, O._ptr(r), O._ptr(a), len(a), O._ptr(b), len(b))
+                else:
+                    (O.port_sqr(a) if kind == 1 else O.port_mul(a, b))
+        t0 = time.time()
+        for _ in range(max(1, warmup)):
+            one()
+        plan_s = time.time() - t0
+        times = []
+        for _ in range(steps):
+            barrier.wait(timeout=3600)
+            t = time.perf_counter()
+            one()
+            times.append(time.perf_counter() - t)
+        queue.put(("ok", plan_s, times))
+    except Exception as e:
+        try:
+            barrier.abort()
+        except Exception:
+            pass
+        queue.put(("err", repr(e), []))
+
+
+def cpu_run_batch(shapes, procs: int, steps: int, warmup: int) -> dict:
+    import multiprocessing as mp
+    from oracle import oracle as O
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs)
+    queue = ctx.Queue()
+    # deal the jobs round-robin by size so every process gets a similar load
+    order = sorted(range(len(shapes)), key=lambda i: -(shapes[i][1] + shapes[i][2]))
+    parts = [[shapes[i] for i in order[k::procs]] for k in range(procs)]
+    ps = [ctx.Process(target=_batch_worker, args=(parts[k], 100 + k, steps, warmup, barrier, queue))
+          for k in range(procs)]
+    for p in ps:
+        p.start()
+    res = [queue.get(timeout=7200) for _ in ps]
+    for p in ps:
+        p.join(timeout=60)
+    errs = [r[1] for r in res if r[0] != "ok"]
+    if errs:
+        raise RuntimeError("CPU batch baseline failed: " + errs[0])
+    step = statistics.median([max(r[2][k] for r in res) for k in range(steps)])
+    total = sum(an + bn for _, an, bn in shapes)
+    cpu = O.host_cpu()
+    return {"value": total / step / 1e6, "unit": "Mlimb/s", "cores": procs,
+            "kind": "reference" if O.ref_available() else "port", "step_s": step,
+            "sample": f"the {len(shapes)}-product batch dealt over {procs} single-threaded processes "
+                      f"(reference router: simd_mpn_mul while 2(an+bn) <= 2^19, else nt_mul/nt_sqr), "
+                      f"median of {steps} steps, plans warmed",
+            "cpu_model": cpu["model"], "host_cores": cpu["cores"],
+            "isa": [f for f in O.REF_ISA if f in cpu["flags"]]}
+
+
+def run_batch(args, ws, rank, local, pg) -> dict | None:
+    import ctypes as C
+
+    import torch
+
+    import simd_bigint_b200 as sbg
+    from simd_bigint_b200.workloads import fill_limbs, mixed_batch_shapes
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    shapes = mixed_batch_shapes(4096, seed=12345)
+    rng = np.random.default_rng(777 + rank)
+    a_off, b_off, r_off = [], [], []
+    na = nr = 0
+    for kind, an, bn in shapes:
+        a_off.append(na)
+        na += an
+        b_off.append(na)
+        na += 0 if kind == sbg.JOB_SQR else bn
+        r_off.append(nr)
+        nr += sbg.out_limbs(kind, an, bn)
+    host_in = np.empty(na, dtype=np.uint64)
+    for (kind, an, bn), ao, bo in zip(shapes, a_off, b_off):
+        host_in[ao:ao + an] = fill_limbs(an, rng)
+        if kind != sbg.JOB_SQR:
+            host_in[bo:bo + bn] = fill_limbs(bn, rng)
+    d_in = torch.from_numpy(host_in.view(np.int64)).to(dev)
+    d_out = torch.empty(nr, dtype=torch.int64, device=dev)
+    ctx = sbg.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream)
+    ib, ob = d_in.data_ptr(), d_out.data_ptr()
+    jobs = [(kind, ob + 8 * ro, ib + 8 * ao, ib + 8 * (bo if kind != sbg.JOB_SQR else ao), an, bn)
+            for (kind, an, bn), ao, bo, ro in zip(shapes, a_off, b_off, r_off)]
+    batch = sbg.Batch(ctx, jobs)
+    batch.capture()
+    clocks = ClockSampler(local)
+    if rank == 0:
+        clocks.start()
+    for _ in range(args.warmup):
+        batch.run()
+    ctx.sync()
+    # bit-exactness of the timed products: every job through the modular spot check
+    from oracle import oracle as O
+    got = d_out.cpu().numpy().view(np.uint64)
+    q = 2305843009213693951
+    exact = True
+    for (kind, an, bn), ao, bo, ro in zip(shapes, a_off, b_off, r_off):
+        a = host_in[ao:ao + an]
+        b = a if kind == sbg.JOB_SQR else host_in[bo:bo + bn]
+        if (O.mod_u64(a, q) * O.mod_u64(b, q)) % q != O.mod_u64(got[ro:ro + an + bn], q):
+            exact = False
+            break
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.run()
+    e1.record(stream)
+    ctx.sync()
+    ms_step = barrier_max(pg, e0.elapsed_time(e1), dev) / args.steps
+    # one multiply per launch over the same batch
+    L = sbg.lib()
+    h = ctx.handle
+    o0, o1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for rep in range(2):
+        o0.record(stream)
+        for kind, r, a, b, an, bn in jobs:
+            st = L.sbg_sqr(h, r, a, an) if kind == sbg.JOB_SQR else L.sbg_mul(h, r, a, an, b, bn)
+            if st:
+                raise RuntimeError(f"sbg_mul failed: {st}")
+        o1.record(stream)
+        ctx.sync()
+    ms_single = barrier_max(pg, o0.elapsed_time(o1), dev)
+    # end to end: pinned host operands in, products out, every step
+    h_in = torch.from_numpy(host_in.view(np.int64)).pin_memory()
+    h_out = torch.empty(nr, dtype=torch.int64).pin_memory()
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            d_in.copy_(h_in, non_blocking=True)
+            batch.run()
+            h_out.copy_(d_out, non_blocking=True)
+        ctx.sync()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            d_in.copy_(h_in, non_blocking=True)
+            batch.run()
+            h_out.copy_(d_out, non_blocking=True)
+        stream.synchronize()
+        e2e_s = barrier_max(pg, time.perf_counter() - t0, dev)
+    exact = exact and np.array_equal(h_out.numpy().view(np.uint64), got)
+    clk = clocks.stop() if rank == 0 else None
+    total = sum(an + bn for _, an, bn in shapes)
+    if rank != 0:
+        batch.close()
+        ctx.close()
+        return None
+    hbm, hbm_src = measured_peaks()
+    alg_bytes = sum(sum(v["bytes"] for v in kernel_model("sqr" if k == sbg.JOB_SQR else "mul", an, bn).values())
+                    for k, an, bn in shapes)
+    value = total * ws / (ms_step * 1e-3) / 1e6
+    single = total / (ms_single * 1e-3) / 1e6
+    res = {
+        "metric": "product Mlimb/s (batched)", "value": round(value, 2), "unit": "Mlimb/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic: seeded uniform u64 limbs, top limb nonzero",
+        "config": {"workload": "4096 independent products, an log-uniform [64, 65536], bn = an/r, "
+                               "r log-uniform [1, 8], 20% squarings (seed 12345); one captured batch per step",
+                   "product_limbs": total, "parallelism": f"replicas x{ws}",
+                   "l2": "0.9 GB of operands/products + batch workspace exceed L2; no flush"},
+        "bit_exact": bool(exact),
+        "one_per_launch": {"value": round(single, 2), "unit": "Mlimb/s", "ms": round(ms_single, 3),
+                           "ratio_batched_vs_single": round(value / ws / single, 2)},
+        "e2e": {"value": round(total * ws * args.steps / e2e_s / 1e6, 2), "unit": "Mlimb/s",
+                "h2d_bytes_per_step": int(host_in.nbytes), "d2h_bytes_per_step": int(nr * 8),
+                "entry": "sbg_batch_run (captured graph) between pinned host copies"},
+        "gpu_launches": None,
+        "roofline": {"bound": "hbm", "kernel": "batch (all stages)",
+                     "achieved": round(alg_bytes / (ms_step * 1e-3) / 1e9, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(alg_bytes / (ms_step * 1e-3) / 1e9 / hbm, 4), "traffic": None,
+                     "peak_source": hbm_src, "alg_bytes_per_launch": alg_bytes},
+        "clocks": clk,
+    }
+    nclasses = len({max(4, (sbg.out_limbs(k, an, bn) - 2).bit_length()) for k, an, bn in shapes})
+    res["gpu_launches"] = int(args.steps * nclasses * 5)
+    batch.close()
+    ctx.close()
+    return res
+
+
 # ------------------------------------------------------------- our arm -----
 def run_ours(args, ws, rank, local, pg) -> dict | None:
     import torch
@@ -418,10 +623,15 @@ def main():
         # the reference is CPU code: rank 0 alone runs it, on all host threads
         if int(os.environ.get("RANK", "0")) != 0:
             return
-        threads = cpu_threads_for(an, bn)
+        threads = cpu_threads_for(an, bn) if op != "batch" else cpu_threads_for(1 << 16, 1 << 16)
         # bounded sample: one product per thread per step, few steps
         steps = max(1, min(args.steps, 3))
-        r = cpu_run(op, an, bn, threads, steps=steps, warmup=1)
+        if op == "batch":
+            from simd_bigint_b200.workloads import mixed_batch_shapes
+            r = cpu_run_batch(mixed_batch_shapes(4096, seed=12345), threads, steps, 1)
+            an, bn = 4096, 0
+        else:
+            r = cpu_run(op, an, bn, threads, steps=steps, warmup=1)
         out = {"metric": "product Mlimb/s", "value": round(r["value"], 3), "unit": "Mlimb/s",
                "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": round(r["step_s"] * 1e3, 1),
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
@@ -436,7 +646,10 @@ def main():
         return
 
     ws, rank, local, pg = dist_init()
-    res = run_ours(args, ws, rank, local, pg)
+    if op == "batch":
+        res = run_batch(args, ws, rank, local, pg)
+    else:
+        res = run_ours(args, ws, rank, local, pg)
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
@@ -444,7 +657,12 @@ def main():
         return
     if not args.no_cpu:
         try:
-            res["cpu_baseline"] = cpu_bounded(op, an, bn)
+            if op == "batch":
+                from simd_bigint_b200.workloads import mixed_batch_shapes
+                res["cpu_baseline"] = cpu_run_batch(mixed_batch_shapes(4096, seed=12345),
+                                                    cpu_threads_for(1 << 16, 1 << 16, cap=32), 2, 1)
+            else:
+                res["cpu_baseline"] = cpu_bounded(op, an, bn)
         except Exception as e:  # recorded, not fatal
             res["cpu_baseline"] = {"value": None, "unit": "Mlimb/s", "error": str(e)}
     print(json.dumps(res), flush=True)

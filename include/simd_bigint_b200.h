@@ -95,6 +95,34 @@ int sbg_sqr(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an);
 int sbg_mulmid(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an, const uint64_t *bp,
                int64_t bn);
 
+/* ---- batches ---------------------------------------------------------------
+ * Thousands of independent products of uneven sizes in a few launches: jobs
+ * are grouped by transform length, each group runs one launch per stage for
+ * all its jobs, groups run concurrently.  No counterpart in the reference
+ * (which multiplies one pair per call); the per-job semantics are those of
+ * sbg_mul / sbg_sqr / sbg_mulmid.  All pointers are device memory. */
+enum { SBG_JOB_MUL = 0, SBG_JOB_SQR = 1, SBG_JOB_MULMID = 2 };
+typedef struct {
+    uint64_t *rp;          /* an+bn limbs (mul), 2an (sqr), an-bn+3 (mulmid) */
+    const uint64_t *ap;
+    const uint64_t *bp;    /* ignored for SBG_JOB_SQR */
+    int64_t an, bn;        /* bn ignored for SBG_JOB_SQR */
+    int32_t kind;          /* SBG_JOB_* */
+    int32_t reserved;
+} sbg_job;
+typedef struct sbg_batch sbg_batch;
+/* Plan a batch: validates jobs, builds missing twiddle tables, allocates the
+ * batch workspace and uploads the job table (synchronous). */
+int sbg_batch_create(sbg_ctx *ctx, const sbg_job *jobs, int64_t count, sbg_batch **out);
+/* Record the batch's launches into a CUDA graph; later runs replay it. */
+int sbg_batch_capture(sbg_batch *batch);
+/* Queue the whole batch on the context stream (stream-ordered, async). */
+int sbg_batch_run(sbg_batch *batch);
+/* Waits for queued runs, then frees. */
+void sbg_batch_destroy(sbg_batch *batch);
+/* create + run + destroy: returns when the products are written. */
+int sbg_mul_batch(sbg_ctx *ctx, const sbg_job *jobs, int64_t count);
+
 /* ---- reference-signature drop-ins ---------------------------------------- */
 
 /* int nt_mul(uint64_t *rp, const uint64_t *ap, ptrdiff_t an,

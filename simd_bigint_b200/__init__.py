@@ -86,6 +86,16 @@ def lib(build_if_missing: bool = False):
         L.sbg_nt_sqr.restype = C.c_int
         L.sbg_probe_bfly_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
         L.sbg_probe_bfly_peak.restype = C.c_int
+        L.sbg_batch_create.argtypes = [_vp, _vp, _i64, C.POINTER(_vp)]
+        L.sbg_batch_create.restype = C.c_int
+        L.sbg_batch_capture.argtypes = [_vp]
+        L.sbg_batch_capture.restype = C.c_int
+        L.sbg_batch_run.argtypes = [_vp]
+        L.sbg_batch_run.restype = C.c_int
+        L.sbg_batch_destroy.argtypes = [_vp]
+        L.sbg_batch_destroy.restype = None
+        L.sbg_mul_batch.argtypes = [_vp, _vp, _i64]
+        L.sbg_mul_batch.restype = C.c_int
         _lib = L
     return _lib
 
@@ -180,6 +190,56 @@ class Context:
         an = a.numel() if an is None else an
         bn = b.numel() if bn is None else bn
         _check(self._L.sbg_mulmid(self.handle, _dptr(r), _dptr(a), an, _dptr(b), bn), "sbg_mulmid")
+
+
+JOB_MUL, JOB_SQR, JOB_MULMID = 0, 1, 2
+
+
+class Job(C.Structure):
+    """sbg_job (include/simd_bigint_b200.h)."""
+    _fields_ = [("rp", C.c_void_p), ("ap", C.c_void_p), ("bp", C.c_void_p),
+                ("an", C.c_int64), ("bn", C.c_int64), ("kind", C.c_int32), ("reserved", C.c_int32)]
+
+
+def out_limbs(kind: int, an: int, bn: int) -> int:
+    return an + bn if kind == JOB_MUL else (2 * an if kind == JOB_SQR else an - bn + 3)
+
+
+class Batch:
+    """A planned batch of independent products on device pointers (raw
+    addresses), run in a few launches per size class; optionally captured
+    into a CUDA graph (capture()) and replayed by run()."""
+
+    def __init__(self, ctx: Context, jobs: list[tuple]):
+        """jobs: (kind, r_ptr, a_ptr, b_ptr, an, bn) with raw device addresses."""
+        self._L = lib()
+        self.ctx = ctx
+        arr = (Job * max(1, len(jobs)))()
+        for i, (kind, r, a, b, an, bn) in enumerate(jobs):
+            arr[i].kind, arr[i].rp, arr[i].ap, arr[i].bp = kind, r, a, b
+            arr[i].an, arr[i].bn = an, bn
+        self._jobs = arr
+        h = _vp()
+        _check(self._L.sbg_batch_create(ctx.handle, C.cast(arr, _vp), len(jobs), C.byref(h)),
+               "sbg_batch_create")
+        self.handle = h
+
+    def capture(self):
+        _check(self._L.sbg_batch_capture(self.handle), "sbg_batch_capture")
+
+    def run(self):
+        _check(self._L.sbg_batch_run(self.handle), "sbg_batch_run")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._L.sbg_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _np_u64(x) -> np.ndarray:

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -173,6 +174,76 @@ static int run_conv(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, co
     return SBG_OK;
 }
 
+// ---- batch engine -----------------------------------------------------------
+// Jobs are bucketed by transform length; each size class is one launch per
+// stage covering all its jobs (blocks -> job by index arithmetic), and the
+// classes run on forked streams.  A batch can be captured into a CUDA graph
+// once and replayed.
+
+#define SBG_BATCH_STREAMS 4
+
+struct sbg_batch {
+    sbg_ctx* ctx = nullptr;
+    struct Cls {
+        int lgL;
+        int njobs;
+        int64_t max_nout;
+        JobDesc* djobs;
+        uint32_t* flags;
+        size_t flag_words;
+    };
+    std::vector<Cls> classes;
+    void* dmem = nullptr;
+    cudaStream_t aux[SBG_BATCH_STREAMS] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[SBG_BATCH_STREAMS] = {};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t count = 0;
+};
+
+static int job_shape(const sbg_job& j, int* lgL, int64_t* cmin, int64_t* cmax, int64_t* off,
+                     int64_t* nout, int* sq) {
+    if (!j.rp || !j.ap || j.an <= 0) return SBG_EINVAL;
+    switch (j.kind) {
+        case SBG_JOB_MUL:
+            if (!j.bp || j.bn <= 0) return SBG_EINVAL;
+            if (j.an + j.bn - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
+            *lgL = conv_lg(j.an + j.bn - 1);
+            *cmin = 0; *cmax = j.an + j.bn - 2; *off = 0; *nout = j.an + j.bn; *sq = 0;
+            return SBG_OK;
+        case SBG_JOB_SQR:
+            if (2 * j.an - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
+            *lgL = conv_lg(2 * j.an - 1);
+            *cmin = 0; *cmax = 2 * j.an - 2; *off = 0; *nout = 2 * j.an; *sq = 1;
+            return SBG_OK;
+        case SBG_JOB_MULMID:
+            if (!j.bp || j.bn <= 0 || j.an < j.bn) return SBG_EINVAL;
+            if (j.an > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
+            *lgL = conv_lg(j.an);
+            *cmin = j.bn - 1; *cmax = j.an - 1; *off = j.bn - 1; *nout = j.an - j.bn + 3; *sq = 0;
+            return SBG_OK;
+        default: return SBG_EINVAL;
+    }
+}
+
+static int batch_launch(sbg_batch* b, KTimer* kt) {
+    sbg_ctx* c = b->ctx;
+    CK(cudaEventRecord(b->fork, c->stream));
+    for (int k = 0; k < SBG_BATCH_STREAMS; ++k) CK(cudaStreamWaitEvent(b->aux[k], b->fork, 0));
+    for (size_t i = 0; i < b->classes.size(); ++i) {
+        const auto& cl = b->classes[i];
+        cudaStream_t st = b->aux[i % SBG_BATCH_STREAMS];
+        CK(launch_batch_class(cl.djobs, cl.njobs, cl.lgL, &c->plans[cl.lgL], c->tw_f, c->tw_i,
+                              cl.max_nout, cl.flags, cl.flag_words, c->err, st, kt));
+    }
+    for (int k = 0; k < SBG_BATCH_STREAMS; ++k) {
+        CK(cudaEventRecord(b->join[k], b->aux[k]));
+        CK(cudaStreamWaitEvent(c->stream, b->join[k], 0));
+    }
+    return SBG_OK;
+}
+
 extern "C" {
 
 const char* sbg_strerror(int status) {
@@ -326,6 +397,157 @@ int sbg_sqr(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an) {
     CK(cudaSetDevice(c->device));
     int lgL = conv_lg(2 * an - 1);
     return run_conv(c, rp, ap, an, ap, an, 1, lgL, 0, 2 * an - 2, 0, 2 * an);
+}
+
+void sbg_batch_destroy(sbg_batch* b) {
+    if (!b) return;
+    if (b->ctx) {
+        cudaSetDevice(b->ctx->device);
+        cudaStreamSynchronize(b->ctx->stream);
+    }
+    for (int k = 0; k < SBG_BATCH_STREAMS; ++k) {
+        if (b->aux[k]) cudaStreamSynchronize(b->aux[k]);
+    }
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (int k = 0; k < SBG_BATCH_STREAMS; ++k) {
+        if (b->aux[k]) cudaStreamDestroy(b->aux[k]);
+        if (b->join[k]) cudaEventDestroy(b->join[k]);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    cudaFree(b->dmem);
+    delete b;
+}
+
+int sbg_batch_create(sbg_ctx* c, const sbg_job* jobs, int64_t count, sbg_batch** out) {
+    if (!c || !out || (count > 0 && !jobs) || count < 0) return SBG_EINVAL;
+    *out = nullptr;
+    CK(cudaSetDevice(c->device));
+    // bucket by transform length
+    std::vector<std::vector<JobDesc>> by_lg(SBG_MAX_LG + 1);
+    std::vector<int64_t> max_nout(SBG_MAX_LG + 1, 0);
+    for (int64_t i = 0; i < count; ++i) {
+        int lgL, sq;
+        int64_t cmin, cmax, off, nout;
+        int st = job_shape(jobs[i], &lgL, &cmin, &cmax, &off, &nout, &sq);
+        if (st) return st;
+        JobDesc d{};
+        d.a = jobs[i].ap;
+        d.b = sq ? jobs[i].ap : jobs[i].bp;
+        d.out = jobs[i].rp;
+        d.an = jobs[i].an;
+        d.bn = sq ? jobs[i].an : jobs[i].bn;
+        d.cmin = cmin; d.cmax = cmax; d.off = off; d.nout = nout;
+        d.sq = sq;
+        by_lg[lgL].push_back(d);
+        if (nout > max_nout[lgL]) max_nout[lgL] = nout;
+    }
+    // sizes: workspace, flags, descriptors -- one allocation
+    size_t ws_total = 0, flag_total = 0, desc_total = 0;
+    for (int l = 0; l <= SBG_MAX_LG; ++l) {
+        if (by_lg[l].empty()) continue;
+        int st = ensure_plan(c, l);
+        if (st) return st;
+        const size_t bpj = (size_t)crt_blocks(max_nout[l]);
+        for (auto& d : by_lg[l]) ws_total += ws_words(l, d.sq);
+        flag_total += by_lg[l].size() * (bpj + 1 + 3) / 4 * 4;
+        desc_total += by_lg[l].size();
+    }
+    sbg_batch* b = new sbg_batch();
+    b->ctx = c;
+    b->count = count;
+    size_t bytes = ws_total * 4 + flag_total * 4 + desc_total * sizeof(JobDesc) + 1024;
+    int st = cuda_fail(cudaMalloc(&b->dmem, bytes), "batch workspace");
+    if (st) {
+        sbg_batch_destroy(b);
+        return st;
+    }
+    uint32_t* ws = (uint32_t*)b->dmem;
+    uint32_t* fl = ws + ws_total;
+    JobDesc* dd = (JobDesc*)(((uintptr_t)(fl + flag_total) + 255) & ~(uintptr_t)255);
+    std::vector<JobDesc> host_all;
+    host_all.reserve(desc_total);
+    for (int l = 0; l <= SBG_MAX_LG; ++l) {
+        if (by_lg[l].empty()) continue;
+        const size_t bpj = (size_t)crt_blocks(max_nout[l]);
+        const size_t fpj = (bpj + 1 + 3) / 4 * 4;
+        sbg_batch::Cls cl;
+        cl.lgL = l;
+        cl.njobs = (int)by_lg[l].size();
+        cl.max_nout = max_nout[l];
+        cl.djobs = dd + host_all.size();
+        cl.flags = fl;
+        cl.flag_words = fpj * by_lg[l].size();
+        for (auto& d : by_lg[l]) {
+            d.ws = ws;
+            ws += ws_words(l, d.sq);
+            d.flags = fl;
+            fl += fpj;
+            host_all.push_back(d);
+        }
+        b->classes.push_back(cl);
+    }
+    // largest classes first: they start early on the forked streams
+    std::stable_sort(b->classes.begin(), b->classes.end(),
+                     [](const sbg_batch::Cls& x, const sbg_batch::Cls& y) {
+                         return ((int64_t)x.njobs << x.lgL) > ((int64_t)y.njobs << y.lgL);
+                     });
+    do {
+        if ((st = cuda_fail(cudaMemcpy(dd, host_all.data(), host_all.size() * sizeof(JobDesc),
+                                       cudaMemcpyHostToDevice), "batch descriptors")))
+            break;
+        for (int k = 0; k < SBG_BATCH_STREAMS && !st; ++k) {
+            st = cuda_fail(cudaStreamCreateWithFlags(&b->aux[k], cudaStreamNonBlocking), "aux");
+            if (!st) st = cuda_fail(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming), "ev");
+        }
+        if (!st) st = cuda_fail(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "ev");
+        if (!st) st = cuda_fail(cudaStreamSynchronize(c->stream), "sync");
+    } while (0);
+    if (st) {
+        sbg_batch_destroy(b);
+        return st;
+    }
+    *out = b;
+    return SBG_OK;
+}
+
+int sbg_batch_capture(sbg_batch* b) {
+    if (!b) return SBG_EINVAL;
+    sbg_ctx* c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    if (b->exec) return SBG_OK;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int st = batch_launch(b, nullptr);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (st) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    CK(e);
+    b->graph = g;
+    CK(cudaGraphInstantiate(&b->exec, g, 0));
+    return SBG_OK;
+}
+
+int sbg_batch_run(sbg_batch* b) {
+    if (!b) return SBG_EINVAL;
+    sbg_ctx* c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    if (b->exec) {
+        CK(cudaGraphLaunch(b->exec, c->stream));
+        return SBG_OK;
+    }
+    return batch_launch(b, c->timer);
+}
+
+int sbg_mul_batch(sbg_ctx* c, const sbg_job* jobs, int64_t count) {
+    sbg_batch* b = nullptr;
+    int st = sbg_batch_create(c, jobs, count, &b);
+    if (st) return st;
+    st = sbg_batch_run(b);
+    sbg_batch_destroy(b);      // waits for the batch
+    return st;
 }
 
 int sbg_mulmid(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, const uint64_t* bp,

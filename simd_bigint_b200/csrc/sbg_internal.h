@@ -49,17 +49,21 @@ struct ScaleArg {
     uint32_t ws[SBG_NP];
 };
 
-// one product / middle product of the batch engine
-struct ConvJob {
+// One windowed convolution of the batch engine (device-resident array).
+// out[m] = limb (m + off) of sum_{cmin <= j <= cmax} c_j 2^(64 j), m < nout,
+// where c = a * b cyclic of the launch's length 2^lgL.
+struct JobDesc {
     const uint64_t* a;
     const uint64_t* b;      // == a for squaring
     uint64_t* out;
     int64_t an, bn;
-    int64_t cmin, cmax;     // coefficient window that contributes
-    int64_t off;            // out[m] = limb (m + off) of the window sum
-    int64_t nout;           // limbs written
-    int sq;
-    int lgL;
+    int64_t cmin, cmax;
+    int64_t off;
+    int64_t nout;
+    uint32_t* ws;           // YA (5 x 2^lgL u32); YB follows it (mul only)
+    uint32_t* flags;        // carry look-back: ticket + one word per block
+    int32_t sq;
+    int32_t pad;
 };
 
 // Kernel ids for the optional per-launch event timing (sbg_ctx_kernel_times).
@@ -116,5 +120,12 @@ cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int6
                              uint32_t* flags, uint32_t* err, cudaStream_t st,
                              KTimer* kt = nullptr);
 size_t carry_flag_words(int64_t nout);
+int64_t crt_blocks(int64_t nout);
+// All stages of one size class of the batch engine (every job of length
+// 2^lgL); `flags` holds flag_words zero-initialised words, job regions inside.
+cudaError_t launch_batch_class(const JobDesc* djobs, int njobs, int lgL, const LenPlan* lp,
+                               const uint2* tw_f, const uint2* tw_i, int64_t max_nout,
+                               uint32_t* flags, size_t flag_words, uint32_t* err,
+                               cudaStream_t st, KTimer* kt = nullptr);
 
 }  // namespace sbg

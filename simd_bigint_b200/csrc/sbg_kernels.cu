@@ -64,13 +64,12 @@ __global__ void k_gen_res(uint2* out, const uint32_t* roots13) {
 // ------------------------------------------------------------------------
 // K0: single-CTA product for L <= 2^12 (one CTA per prime)
 // ------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_small(const uint64_t* __restrict__ a, int64_t an,
-                                               const uint64_t* __restrict__ b, int64_t bn, int sq,
-                                               int lgL, const uint2* __restrict__ twf,
-                                               const uint2* __restrict__ twi, ScaleArg sc,
-                                               uint32_t* __restrict__ R) {
+__device__ __forceinline__ void small_body(int q, const uint64_t* __restrict__ a, int64_t an,
+                                           const uint64_t* __restrict__ b, int64_t bn, int sq,
+                                           int lgL, const uint2* __restrict__ twf,
+                                           const uint2* __restrict__ twi, const ScaleArg& sc,
+                                           uint32_t* __restrict__ R) {
     extern __shared__ uint32_t sm[];
-    const int q = blockIdx.x;
     const PrimeConst pc = c_pr[q];
     const int L = 1 << lgL;
     const int ld = padded_len(L);
@@ -90,6 +89,22 @@ __global__ void __launch_bounds__(256) k_small(const uint64_t* __restrict__ a, i
     __syncthreads();
     ntt_inverse(sm, ld, 1, lgL, twi + q * SBG_TW_N, pc.p);
     for (int i = threadIdx.x; i < L; i += blockDim.x) R[(size_t)q * L + i] = A[pad_idx(i)];
+}
+
+__global__ void __launch_bounds__(256) k_small(const uint64_t* __restrict__ a, int64_t an,
+                                               const uint64_t* __restrict__ b, int64_t bn, int sq,
+                                               int lgL, const uint2* __restrict__ twf,
+                                               const uint2* __restrict__ twi, ScaleArg sc,
+                                               uint32_t* __restrict__ R) {
+    small_body(blockIdx.x, a, an, b, bn, sq, lgL, twf, twi, sc, R);
+}
+
+// batched: one CTA per (job, prime); every job of the launch has length 2^lgL
+__global__ void __launch_bounds__(256) k_small_b(const JobDesc* __restrict__ jobs, int lgL,
+                                                 const uint2* __restrict__ twf,
+                                                 const uint2* __restrict__ twi, ScaleArg sc) {
+    const JobDesc& J = jobs[blockIdx.x / SBG_NP];
+    small_body(blockIdx.x % SBG_NP, J.a, J.an, J.b, J.bn, J.sq, lgL, twf, twi, sc, J.ws);
 }
 
 // ------------------------------------------------------------------------
@@ -276,21 +291,15 @@ __device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restr
 // K1: limbs -> residues -> column DIF (bit-reversed rows) for one operand,
 // one prime, one tile.
 template <int LGN1>
-__global__ void __launch_bounds__(512, 2) k_col_fwd(const uint64_t* __restrict__ a, int64_t an,
-                                                 const uint64_t* __restrict__ b, int64_t bn,
-                                                 const uint2* __restrict__ twf,
-                                                 uint32_t* __restrict__ YA,
-                                                 uint32_t* __restrict__ YB, int nops) {
+__device__ __forceinline__ void col_fwd_body(int q, int tile, int op,
+                                             const uint64_t* __restrict__ a, int64_t an,
+                                             const uint64_t* __restrict__ b, int64_t bn,
+                                             const uint2* __restrict__ twf,
+                                             uint32_t* __restrict__ YA,
+                                             uint32_t* __restrict__ YB) {
     extern __shared__ uint32_t sm[];
     constexpr int NP = col_np(LGN1);
     constexpr int LGW = col_lgw(LGN1);
-    constexpr int NTILES = 1 << (SBG_ROW_LG - LGW);
-    // prime slowest: the CTAs resident on an SM share one prime's twiddles
-    const int per_q = NTILES * nops;
-    const int q = blockIdx.x / per_q;
-    const int rest = blockIdx.x - q * per_q;
-    const int tile = rest % NTILES;
-    const int op = rest / NTILES;
     const uint64_t* X = op ? b : a;
     const int64_t xn = op ? bn : an;
     uint32_t* Y = (op ? YB : YA) + ((size_t)q << (LGN1 + SBG_ROW_LG));
@@ -312,16 +321,46 @@ __global__ void __launch_bounds__(512, 2) k_col_fwd(const uint64_t* __restrict__
     }
 }
 
+// K1: limbs -> residues -> column DIF (bit-reversed rows) for one operand,
+// one prime, one tile.  Block order: prime slowest, so the CTAs resident on an
+// SM share one prime's twiddles.
+template <int LGN1>
+__global__ void __launch_bounds__(512, 2) k_col_fwd(const uint64_t* __restrict__ a, int64_t an,
+                                                    const uint64_t* __restrict__ b, int64_t bn,
+                                                    const uint2* __restrict__ twf,
+                                                    uint32_t* __restrict__ YA,
+                                                    uint32_t* __restrict__ YB, int nops) {
+    constexpr int NTILES = 1 << (SBG_ROW_LG - col_lgw(LGN1));
+    const int per_q = NTILES * nops;
+    const int q = blockIdx.x / per_q;
+    const int rest = blockIdx.x - q * per_q;
+    col_fwd_body<LGN1>(q, rest % NTILES, rest / NTILES, a, an, b, bn, twf, YA, YB);
+}
+
+// batched: blocks (job, prime, operand, tile), job slowest; the second
+// operand's blocks of a squaring exit at once
+template <int LGN1>
+__global__ void __launch_bounds__(512, 2) k_col_fwd_b(const JobDesc* __restrict__ jobs,
+                                                      const uint2* __restrict__ twf) {
+    constexpr int NTILES = 1 << (SBG_ROW_LG - col_lgw(LGN1));
+    constexpr int PER_JOB = SBG_NP * 2 * NTILES;
+    const JobDesc& J = jobs[blockIdx.x / PER_JOB];
+    const int r = blockIdx.x % PER_JOB;
+    const int q = r / (2 * NTILES);
+    const int r2 = r % (2 * NTILES);
+    const int op = r2 / NTILES;
+    if (op && J.sq) return;
+    uint32_t* YB = J.ws + ((size_t)SBG_NP << (LGN1 + SBG_ROW_LG));
+    col_fwd_body<LGN1>(q, r2 % NTILES, op, J.a, J.an, J.b, J.bn, twf, J.ws, YB);
+}
+
 // K3: column DIT (reverse of K1), in place, natural row order out.
 template <int LGN1>
-__global__ void __launch_bounds__(512, 2) k_col_inv(uint32_t* __restrict__ YA,
-                                                 const uint2* __restrict__ twi) {
+__device__ __forceinline__ void col_inv_body(int q, int tile, uint32_t* __restrict__ YA,
+                                             const uint2* __restrict__ twi) {
     extern __shared__ uint32_t sm[];
     constexpr int NP = col_np(LGN1);
     constexpr int LGW = col_lgw(LGN1);
-    constexpr int NTILES = 1 << (SBG_ROW_LG - LGW);
-    const int q = blockIdx.x / NTILES;
-    const int tile = blockIdx.x - q * NTILES;
     uint32_t* Y = YA + ((size_t)q << (LGN1 + SBG_ROW_LG));
     const PrimeConst pc = c_pr[q];
     const uint2* tw = twi + (size_t)q * SBG_TW_N;
@@ -341,6 +380,23 @@ __global__ void __launch_bounds__(512, 2) k_col_inv(uint32_t* __restrict__ YA,
     col_pass_t<LGN1, 0, false>(sm, nullptr, 0, Y, c0, tw, pc);
 }
 
+template <int LGN1>
+__global__ void __launch_bounds__(512, 2) k_col_inv(uint32_t* __restrict__ YA,
+                                                    const uint2* __restrict__ twi) {
+    constexpr int NTILES = 1 << (SBG_ROW_LG - col_lgw(LGN1));
+    col_inv_body<LGN1>(blockIdx.x / NTILES, blockIdx.x % NTILES, YA, twi);
+}
+
+template <int LGN1>
+__global__ void __launch_bounds__(512, 2) k_col_inv_b(const JobDesc* __restrict__ jobs,
+                                                      const uint2* __restrict__ twi) {
+    constexpr int NTILES = 1 << (SBG_ROW_LG - col_lgw(LGN1));
+    constexpr int PER_JOB = SBG_NP * NTILES;
+    const JobDesc& J = jobs[blockIdx.x / PER_JOB];
+    const int r = blockIdx.x % PER_JOB;
+    col_inv_body<LGN1>(r / NTILES, r % NTILES, J.ws, twi);
+}
+
 // K2: one row of N2 = 2^12 points for one prime, 256 threads.
 //   P1  global -> four-step twiddle -> DIF levels 1-4 (A and B) -> smem
 //   P2  DIF levels 5-8 (A and B)
@@ -351,19 +407,16 @@ __global__ void __launch_bounds__(512, 2) k_col_inv(uint32_t* __restrict__ YA,
 // register group, so that stage never touches shared memory.
 #define ROW_LG 12
 #define ROW_N (1 << ROW_LG)
-__global__ void __launch_bounds__(256, 4) k_row12(uint32_t* __restrict__ YA,
-                                               const uint32_t* __restrict__ YB, int sq, int lgN1,
-                                               FsTables fsf, FsTables fsi, ScaleArg sc,
-                                               const uint2* __restrict__ twf,
-                                               const uint2* __restrict__ twi) {
+__device__ __forceinline__ void row_body(int q, int row, uint32_t* __restrict__ YA,
+                                         const uint32_t* __restrict__ YB, int sq, int lgN1,
+                                         const FsTables& fsf, const FsTables& fsi,
+                                         const ScaleArg& sc, const uint2* __restrict__ twf,
+                                         const uint2* __restrict__ twi) {
     __shared__ uint32_t smA[padded_len(ROW_N)];
     __shared__ uint32_t smB[padded_len(ROW_N)];
     __shared__ uint2 s_f[16];
     __shared__ uint2 s_i[16];
     const int tid = threadIdx.x;
-    const int N1 = 1 << lgN1;
-    const int q = blockIdx.x >> lgN1;
-    const int row = blockIdx.x & (N1 - 1);
     const PrimeConst pc = c_pr[q];
     const uint32_t p = pc.p;
     const uint32_t Lmask = (1u << (lgN1 + ROW_LG)) - 1u;
@@ -473,6 +526,27 @@ __global__ void __launch_bounds__(256, 4) k_row12(uint32_t* __restrict__ YA,
     }
 }
 
+__global__ void __launch_bounds__(256, 4) k_row12(uint32_t* __restrict__ YA,
+                                                  const uint32_t* __restrict__ YB, int sq,
+                                                  int lgN1, FsTables fsf, FsTables fsi, ScaleArg sc,
+                                                  const uint2* __restrict__ twf,
+                                                  const uint2* __restrict__ twi) {
+    row_body(blockIdx.x >> lgN1, blockIdx.x & ((1 << lgN1) - 1), YA, YB, sq, lgN1, fsf, fsi, sc,
+             twf, twi);
+}
+
+// batched: blocks (job, prime, row), job slowest
+__global__ void __launch_bounds__(256, 4) k_row12_b(const JobDesc* __restrict__ jobs, int lgN1,
+                                                    FsTables fsf, FsTables fsi, ScaleArg sc,
+                                                    const uint2* __restrict__ twf,
+                                                    const uint2* __restrict__ twi) {
+    const int per_job = SBG_NP << lgN1;
+    const JobDesc& J = jobs[blockIdx.x / per_job];
+    const int r = blockIdx.x % per_job;
+    uint32_t* YB = J.ws + ((size_t)SBG_NP << (lgN1 + ROW_LG));
+    row_body(r >> lgN1, r & ((1 << lgN1) - 1), J.ws, YB, J.sq, lgN1, fsf, fsi, sc, twf, twi);
+}
+
 // ------------------------------------------------------------------------
 // K4: Garner CRT + three-stream compose + carry resolution.
 //
@@ -557,17 +631,13 @@ __device__ __forceinline__ uint32_t gp_compose(uint32_t left, uint32_t right) {
     return (gr | (pr & gl)) | ((pr & pl) << 1);
 }
 
-__global__ void __launch_bounds__(CRT_T) k_crt_carry(const uint32_t* __restrict__ R, int lgL,
-                                                     int64_t cmin, int64_t cmax, int64_t off,
-                                                     uint64_t* __restrict__ out, int64_t nout,
-                                                     uint32_t* flags, uint32_t* err) {
-    __shared__ uint32_t s_bid;
+__device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restrict__ R, int lgL,
+                                         int64_t cmin, int64_t cmax, int64_t off,
+                                         uint64_t* __restrict__ out, int64_t nout,
+                                         uint32_t* flags, uint32_t* err) {
     __shared__ uint32_t s_warp[CRT_T / 32];
     __shared__ uint32_t s_cin;
     const int64_t L = (int64_t)1 << lgL;
-    if (threadIdx.x == 0) s_bid = atomicAdd(&flags[0], 1u);
-    __syncthreads();
-    const uint32_t bid = s_bid;
     const int64_t m0 = (int64_t)bid * CRT_BLK + (int64_t)threadIdx.x * CRT_PER;
     const int64_t j0 = m0 + off;
     // residues of coefficients j0-4 .. j0+15 arrive in 5 chunks of 4: one
@@ -745,6 +815,31 @@ __global__ void __launch_bounds__(CRT_T) k_crt_carry(const uint32_t* __restrict_
     if (has_v && ((zv | (uint64_t)tcin | (uint64_t)kv) != 0)) atomicOr(err, 2u);
 }
 
+// Block order comes from an atomic ticket (flags[0]), not blockIdx, so every
+// block's look-back predecessors were scheduled before it.
+__global__ void __launch_bounds__(CRT_T) k_crt_carry(const uint32_t* __restrict__ R, int lgL,
+                                                     int64_t cmin, int64_t cmax, int64_t off,
+                                                     uint64_t* __restrict__ out, int64_t nout,
+                                                     uint32_t* flags, uint32_t* err) {
+    __shared__ uint32_t s_bid;
+    if (threadIdx.x == 0) s_bid = atomicAdd(&flags[0], 1u);
+    __syncthreads();
+    crt_body(s_bid, R, lgL, cmin, cmax, off, out, nout, flags, err);
+}
+
+// batched: blocks_per_job CTAs per job (enough for the longest output of the
+// launch); each takes a ticket on its own job's counter, surplus ones exit.
+__global__ void __launch_bounds__(CRT_T) k_crt_carry_b(const JobDesc* __restrict__ jobs, int lgL,
+                                                       int blocks_per_job, uint32_t* err) {
+    __shared__ uint32_t s_bid;
+    const JobDesc& J = jobs[blockIdx.x / blocks_per_job];
+    if (threadIdx.x == 0) s_bid = atomicAdd(&J.flags[0], 1u);
+    __syncthreads();
+    const int64_t need = (J.nout + 1 + CRT_BLK - 1) / CRT_BLK;
+    if ((int64_t)s_bid >= need) return;
+    crt_body(s_bid, J.ws, lgL, J.cmin, J.cmax, J.off, J.out, J.nout, J.flags, err);
+}
+
 // ------------------------------------------------------------------------
 // launchers
 // ------------------------------------------------------------------------
@@ -755,6 +850,10 @@ static cudaError_t col_attr() {
     cudaError_t e = cudaFuncSetAttribute(k_col_fwd<LGN1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_col_inv<LGN1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_col_fwd_b<LGN1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_col_inv_b<LGN1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     return e;
 }
 
@@ -768,6 +867,8 @@ cudaError_t set_kernel_attributes() {
 #undef SBG_ATTR
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_small_b, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     return e;
 }
 
@@ -882,6 +983,54 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
         default: return cudaErrorInvalidValue;
     }
     KT_END(kt, KID_COL_INV, st);
+    return cudaGetLastError();
+}
+
+int64_t crt_blocks(int64_t nout) { return (nout + 1 + CRT_BLK - 1) / CRT_BLK; }
+
+cudaError_t launch_batch_class(const JobDesc* djobs, int njobs, int lgL, const LenPlan* lp,
+                               const uint2* tw_f, const uint2* tw_i, int64_t max_nout,
+                               uint32_t* flags, size_t flag_words, uint32_t* err,
+                               cudaStream_t st, KTimer* kt) {
+    if (njobs <= 0) return cudaSuccess;
+    ScaleArg sc;
+    for (int q = 0; q < SBG_NP; ++q) {
+        sc.w[q] = lp->scale[q].w;
+        sc.ws[q] = lp->scale[q].ws;
+    }
+    cudaError_t e = cudaMemsetAsync(flags, 0, flag_words * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    KT_BEGIN(kt, KID_BATCH, st);
+    if (lgL <= SBG_SMALL_MAX_LG) {
+        size_t smem = (size_t)2 * padded_len(1 << lgL) * 4;
+        k_small_b<<<njobs * SBG_NP, 256, smem, st>>>(djobs, lgL, tw_f, tw_i, sc);
+    } else {
+        const int lgN1 = lp->lgN1;
+        FsTables fsf{lp->fs_lo_f, lp->fs_hi_f, lp->hi_n};
+        FsTables fsi{lp->fs_lo_i, lp->fs_hi_i, lp->hi_n};
+        const int ntiles = 1 << (SBG_ROW_LG - col_lgw(lgN1));
+        const size_t col_smem = (size_t)col_smem_bytes(lgN1);
+        switch (lgN1) {
+#define SBG_LAUNCH_FB(n)                                                              \
+    case n:                                                                           \
+        k_col_fwd_b<n><<<njobs * SBG_NP * 2 * ntiles, 512, col_smem, st>>>(djobs, tw_f); \
+        break;
+            SBG_COL_CASES(SBG_LAUNCH_FB)
+#undef SBG_LAUNCH_FB
+            default: return cudaErrorInvalidValue;
+        }
+        k_row12_b<<<(njobs * SBG_NP) << lgN1, 256, 0, st>>>(djobs, lgN1, fsf, fsi, sc, tw_f, tw_i);
+        switch (lgN1) {
+#define SBG_LAUNCH_IB(n)                                                           \
+    case n: k_col_inv_b<n><<<njobs * SBG_NP * ntiles, 512, col_smem, st>>>(djobs, tw_i); break;
+            SBG_COL_CASES(SBG_LAUNCH_IB)
+#undef SBG_LAUNCH_IB
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    const int bpj = (int)crt_blocks(max_nout);
+    k_crt_carry_b<<<njobs * bpj, CRT_T, 0, st>>>(djobs, lgL, bpj, err);
+    KT_END(kt, KID_BATCH, st);
     return cudaGetLastError();
 }
 

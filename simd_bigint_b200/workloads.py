@@ -1,0 +1,44 @@
+"""Seeded synthetic workloads of the benchmark configurations (shapes and
+value distributions only; limbs are uniform random u64 with the top limb
+nonzero).  Used by bench.py and by the tests."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import JOB_MUL, JOB_SQR
+
+
+def mixed_batch_shapes(count: int = 4096, seed: int = 12345, lo: int = 64, hi: int = 65536,
+                       rmax: float = 8.0, sq_frac: float = 0.2) -> list[tuple[int, int, int]]:
+    """The batched mixed-size configuration: an log-uniform in [lo, hi],
+    bn = max(1, floor(an / r)) with r log-uniform in [1, rmax], a fraction
+    sq_frac of squarings.  Returns (kind, an, bn) triples."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        an = int(math.exp(rng.uniform(math.log(lo), math.log(hi))))
+        r = math.exp(rng.uniform(0.0, math.log(rmax)))
+        bn = max(1, int(an / r))
+        sq = rng.uniform() < sq_frac
+        out.append((JOB_SQR, an, an) if sq else (JOB_MUL, an, bn))
+    return out
+
+
+def division_shapes(count: int = 1024, seed: int = 4242, lo: int = 512,
+                    hi: int = 262144) -> list[int]:
+    """Divisor sizes n of the batched division configuration (numerator 2n
+    limbs, divisor n limbs, top bit set), n log-uniform in [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    return [int(math.exp(rng.uniform(math.log(lo), math.log(hi)))) for _ in range(count)]
+
+
+def fill_limbs(n: int, rng: np.random.Generator, top_bit: bool = False) -> np.ndarray:
+    x = rng.integers(0, 2**64, size=n, dtype=np.uint64)
+    if n:
+        if top_bit:
+            x[-1] |= np.uint64(1 << 63)
+        elif x[-1] == 0:
+            x[-1] = np.uint64(1)
+    return x
