@@ -123,6 +123,31 @@ void sbg_batch_destroy(sbg_batch *batch);
 /* create + run + destroy: returns when the products are written. */
 int sbg_mul_batch(sbg_ctx *ctx, const sbg_job *jobs, int64_t count);
 
+/* ---- Newton reciprocal and division ----------------------------------------
+ * All pointers are device memory; the calls wait for their result.
+ *
+ * sbg_recip: V = floor((2^(128 n) - 1) / D) - 2^(64 n), n limbs, for an n-limb
+ * normalised D (top bit set): the reciprocal the reference's Newton
+ * prototypes compute (bench/recip_mulmid_ref.c:51-116), here exact.
+ *
+ * sbg_divrem: Q = floor(N / D) (nn-dn+1 limbs), R = N mod D (dn limbs) for a
+ * normalised D and dn <= nn <= 2 dn, by the Newton reciprocal and GPU
+ * products; the results equal the reference's divrem_u64_dc
+ * (include/dc_div.h:154) bit for bit.  sbg_divrem_batch runs many such
+ * divisions with their recursion levels in lockstep (one batch of products
+ * per level). */
+int sbg_recip(sbg_ctx *ctx, uint64_t *ip, const uint64_t *dp, int64_t n);
+int sbg_divrem(sbg_ctx *ctx, uint64_t *qp, uint64_t *rp, const uint64_t *np, int64_t nn,
+               const uint64_t *dp, int64_t dn);
+typedef struct {
+    uint64_t *qp;          /* nn-dn+1 limbs */
+    uint64_t *rp;          /* dn limbs */
+    const uint64_t *np;
+    const uint64_t *dp;    /* top bit set */
+    int64_t nn, dn;        /* dn <= nn <= 2 dn */
+} sbg_div_job;
+int sbg_divrem_batch(sbg_ctx *ctx, const sbg_div_job *jobs, int64_t count);
+
 /* ---- reference-signature drop-ins ---------------------------------------- */
 
 /* int nt_mul(uint64_t *rp, const uint64_t *ap, ptrdiff_t an,
@@ -132,6 +157,17 @@ int sbg_nt_mul(uint64_t *rp, const uint64_t *ap, ptrdiff_t an, const uint64_t *b
 /* int nt_sqr(uint64_t *rp, const uint64_t *ap, ptrdiff_t an)
  *                                                  -- reference include/ntmul.h:77 */
 int sbg_nt_sqr(uint64_t *rp, const uint64_t *ap, ptrdiff_t an);
+
+/* void divrem_u64(uint64_t *qp, uint64_t *rp, const uint64_t *np, uint64_t nn64,
+ *                 const uint64_t *dp, uint64_t dn64, uint64_t *qn64_out,
+ *                 uint64_t *rn64_out)        -- reference include/divrem.h:218,
+ *                                               include/dc_div.h:154 (divrem_u64_dc)
+ * Same arguments: qp gets nn-dn+1 limbs, rp gets dn limbs, *qn/*rn the
+ * trimmed lengths (>= 1).  Any divisor with a nonzero top limb, any
+ * nn >= dn (normalised and split into 2dn/dn Newton steps).  Returns 1 on
+ * success, 0 on failure (the reference's version returns void). */
+int sbg_divrem_u64(uint64_t *qp, uint64_t *rp, const uint64_t *np, uint64_t nn64,
+                   const uint64_t *dp, uint64_t dn64, uint64_t *qn64_out, uint64_t *rn64_out);
 
 /* ---- allocation-free multiply -------------------------------------------------
  * No counterpart in the reference.  For callers that must not allocate device

@@ -96,6 +96,15 @@ def lib(build_if_missing: bool = False):
         L.sbg_batch_destroy.restype = None
         L.sbg_mul_batch.argtypes = [_vp, _vp, _i64]
         L.sbg_mul_batch.restype = C.c_int
+        L.sbg_recip.argtypes = [_vp, _vp, _vp, _i64]
+        L.sbg_recip.restype = C.c_int
+        L.sbg_divrem.argtypes = [_vp, _vp, _vp, _vp, _i64, _vp, _i64]
+        L.sbg_divrem.restype = C.c_int
+        L.sbg_divrem_batch.argtypes = [_vp, _vp, _i64]
+        L.sbg_divrem_batch.restype = C.c_int
+        L.sbg_divrem_u64.argtypes = [_vp, _vp, _vp, C.c_uint64, _vp, C.c_uint64,
+                                     C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.sbg_divrem_u64.restype = C.c_int
         _lib = L
     return _lib
 
@@ -186,6 +195,26 @@ class Context:
         an = a.numel() if an is None else an
         _check(self._L.sbg_sqr(self.handle, _dptr(r), _dptr(a), an), "sbg_sqr")
 
+    def recip(self, i, d, n: int | None = None):
+        """i[0..n) = floor((B^2n - 1) / D) - B^n for a normalised n-limb D."""
+        n = d.numel() if n is None else n
+        _check(self._L.sbg_recip(self.handle, _dptr(i), _dptr(d), n), "sbg_recip")
+
+    def divrem(self, q, r, n_, d, nn: int | None = None, dn: int | None = None):
+        """q = N // D (nn-dn+1 limbs), r = N % D (dn limbs); D normalised,
+        dn <= nn <= 2 dn."""
+        nn = n_.numel() if nn is None else nn
+        dn = d.numel() if dn is None else dn
+        _check(self._L.sbg_divrem(self.handle, _dptr(q), _dptr(r), _dptr(n_), nn, _dptr(d), dn),
+               "sbg_divrem")
+
+    def divrem_batch(self, jobs: list[tuple]):
+        """jobs: (q_ptr, r_ptr, n_ptr, d_ptr, nn, dn) raw device addresses."""
+        arr = (DivJob * max(1, len(jobs)))()
+        for i, (q, r, n_, d, nn, dn) in enumerate(jobs):
+            arr[i].qp, arr[i].rp, arr[i].np, arr[i].dp, arr[i].nn, arr[i].dn = q, r, n_, d, nn, dn
+        _check(self._L.sbg_divrem_batch(self.handle, C.cast(arr, _vp), len(jobs)), "sbg_divrem_batch")
+
     def mulmid(self, r, a, b, an: int | None = None, bn: int | None = None):
         an = a.numel() if an is None else an
         bn = b.numel() if bn is None else bn
@@ -193,6 +222,12 @@ class Context:
 
 
 JOB_MUL, JOB_SQR, JOB_MULMID = 0, 1, 2
+
+
+class DivJob(C.Structure):
+    """sbg_div_job (include/simd_bigint_b200.h)."""
+    _fields_ = [("qp", C.c_void_p), ("rp", C.c_void_p), ("np", C.c_void_p), ("dp", C.c_void_p),
+                ("nn", C.c_int64), ("dn", C.c_int64)]
 
 
 class Job(C.Structure):
@@ -282,6 +317,20 @@ def sqr(a: np.ndarray) -> np.ndarray:
     if not nt_sqr(r, a, len(a)):
         raise SbgError(2, "nt_sqr")
     return r
+
+
+def divrem_u64(n: np.ndarray, d: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Reference-signature division (include/divrem.h:218) on host arrays:
+    returns (Q, R) trimmed to their lengths as the reference reports them."""
+    n = _np_u64(n)
+    d = _np_u64(d)
+    q = np.zeros(len(n) - len(d) + 1, dtype=np.uint64)
+    r = np.zeros(len(d), dtype=np.uint64)
+    qn, rn = C.c_uint64(0), C.c_uint64(0)
+    if not lib().sbg_divrem_u64(q.ctypes.data, r.ctypes.data, n.ctypes.data, len(n), d.ctypes.data,
+                                len(d), C.byref(qn), C.byref(rn)):
+        raise SbgError(4, "sbg_divrem_u64")
+    return q[: qn.value], r[: rn.value]
 
 
 def probe_bfly_peak(device: int = 0) -> float:

@@ -577,6 +577,8 @@ static sbg_ctx* default_ctx() {
     return g_ctx[dev];
 }
 
+extern "C" sbg_ctx* sbg_default_ctx_internal(void) { return default_ctx(); }
+
 static bool is_device_ptr(const void* p) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {

@@ -1,0 +1,747 @@
+// sbg_div.cu -- Newton reciprocal and division on top of the GPU products.
+//
+// Reciprocal: the Newton iteration for an n-limb normalised divisor D
+// (B = 2^64, B^n/2 <= D < B^n), as the reference's division prototypes
+// specify it (bench/recip_mulmid_ref.c:51-116, bench/mpinv_mulmid_verify.c:
+// 27-45: X_h from the top h limbs, residual of D * X_h, correction
+// x_hi * residual / B^k, h -> n = 2h).  We follow the "approximate
+// reciprocal" formulation of Brent and Zimmermann (Modern Computer
+// Arithmetic, Algorithm 3.5): with l = floor((n-1)/2), h = n - l,
+//     X_h = R(top h limbs of D)
+//     T   = D * X_h;   while T >= B^(n+h): X_h -= 1, T -= D   (at most 4 times)
+//     T_m = floor((B^(n+h) - T) / B^l)
+//     U   = T_m * X_h
+//     X   = X_h * B^l + floor(U / B^(2h-l))
+// which keeps D X < B^2n <= D (X + 2) at every level.  The base case (at
+// most SBG_DIV_BASE limbs) is an exact long division, one thread per
+// divisor.  Every product runs on the batch engine, so all divisions of a
+// batch advance one recursion level per round.
+//
+// Division of a 2n-limb N by D: Q0 = N_hi + floor(N_hi * (X - B^n) / B^n)
+// (within 5 of floor(N / D)), R = N - Q0 D, then at most five (R -= D, Q += 1)
+// steps.  The linear steps (borrow/carry chains, compares) run one CTA per
+// division with a block-wide carry scan.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "../../include/simd_bigint_b200.h"
+#include "sbg_internal.h"
+
+namespace sbg {
+
+#define DIV_T 1024           // threads of the per-division linear kernels
+#define DIV_PER 4            // limbs per thread per tile
+#define DIV_TILE (DIV_T * DIV_PER)
+
+// ---------------------------------------------------------------------------
+// block-wide multi-limb add / sub with carry scan (one CTA, tiles of 4096)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t gp2(uint32_t left, uint32_t right) {
+    uint32_t gl = left & 1, pl = (left >> 1) & 1, gr = right & 1, pr = (right >> 1) & 1;
+    return (gr | (pr & gl)) | ((pr & pl) << 1);
+}
+
+// exclusive block scan of (G, P) pairs; returns this thread's prefix and
+// writes the block total to *total (all threads)
+__device__ __forceinline__ uint32_t block_scan_gp(uint32_t gp, uint32_t* total) {
+    __shared__ uint32_t s_w[DIV_T / 32];
+    __shared__ uint32_t s_tot;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t inc = gp;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t o = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc = gp2(o, inc);
+    }
+    if (lane == 31) s_w[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t v = s_w[lane];
+        uint32_t iv = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t o = __shfl_up_sync(0xffffffffu, iv, d);
+            if (lane >= d) iv = gp2(o, iv);
+        }
+        s_w[lane] = iv;
+        if (lane == 31) s_tot = iv;
+    }
+    __syncthreads();
+    uint32_t prev = __shfl_up_sync(0xffffffffu, inc, 1);
+    uint32_t wpre = wid > 0 ? s_w[wid - 1] : 2u;
+    uint32_t excl = lane > 0 ? gp2(wpre, prev) : wpre;
+    *total = s_tot;
+    __syncthreads();
+    return excl;
+}
+
+// z[0..len) = x +/- y (+ cin / - bin), x(i), y(i) limb accessors (0 beyond
+// their length); returns the carry / borrow out.  z may alias x or y limb
+// for limb.
+template <class FX, class FY>
+__device__ uint32_t block_addsub(uint64_t* z, int64_t len, FX x, FY y, bool sub, uint32_t cin) {
+    uint32_t carry = cin;
+    for (int64_t base = 0; base < len; base += DIV_TILE) {
+        const int64_t i0 = base + (int64_t)threadIdx.x * DIV_PER;
+        uint64_t s[DIV_PER];
+        uint32_t gmask = 0, pmask = 0;
+#pragma unroll
+        for (int k = 0; k < DIV_PER; ++k) {
+            const int64_t i = i0 + k;
+            uint64_t a = i < len ? x(i) : 0, b = i < len ? y(i) : 0;
+            if (sub) {
+                uint64_t d = a - b;
+                s[k] = d;
+                if (a < b) gmask |= 1u << k;          // borrow generated
+                if (d == 0 && i < len) pmask |= 1u << k;   // borrow propagates
+            } else {
+                uint64_t d = a + b;
+                s[k] = d;
+                if (d < a) gmask |= 1u << k;
+                if (d == ~0ull && i < len) pmask |= 1u << k;
+            }
+        }
+        // thread aggregate over its DIV_PER limbs (in order)
+        uint32_t G = 0, P = 1;
+#pragma unroll
+        for (int k = 0; k < DIV_PER; ++k) {
+            uint32_t g = (gmask >> k) & 1, p = (pmask >> k) & 1;
+            G = g | (p & G);
+            P = p & P;
+        }
+        uint32_t tot;
+        uint32_t excl = block_scan_gp(G | (P << 1), &tot);
+        uint32_t c = (excl & 1) | (((excl >> 1) & 1) & carry);
+#pragma unroll
+        for (int k = 0; k < DIV_PER; ++k) {
+            const int64_t i = i0 + k;
+            if (i < len) z[i] = sub ? s[k] - c : s[k] + c;
+            uint32_t g = (gmask >> k) & 1, p = (pmask >> k) & 1;
+            c = g | (p & c);
+        }
+        carry = (tot & 1) | (((tot >> 1) & 1) & carry);
+    }
+    return carry;
+}
+
+// sign of x - y over len limbs: -1, 0, 1 (block-uniform)
+template <class FX, class FY>
+__device__ int block_cmp(int64_t len, FX x, FY y) {
+    __shared__ long long s_hi;
+    if (threadIdx.x == 0) s_hi = -1;
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < len; i += DIV_T) {
+        if (x(i) != y(i)) atomicMax(&s_hi, (long long)i);
+    }
+    __syncthreads();
+    long long hi = s_hi;
+    __syncthreads();
+    if (hi < 0) return 0;
+    return x(hi) > y(hi) ? 1 : -1;
+}
+
+// ---------------------------------------------------------------------------
+// per-division descriptors
+// ---------------------------------------------------------------------------
+struct RecipStep {
+    const uint64_t* A;      // top n limbs of D
+    uint64_t* Xh;           // h+1 limbs (in/out: corrected in place)
+    uint64_t* T;            // n+h+1 limbs: D*Xh on entry
+    uint64_t* TM;           // out: h+1 limbs
+    const uint64_t* U;      // n/a in step 1; 2h+2 limbs in step 2
+    uint64_t* X;            // out of step 2: n+1 limbs
+    int64_t n, h;
+};
+
+struct DivFix {
+    const uint64_t* N;      // 2n limbs
+    const uint64_t* D;      // n limbs
+    const uint64_t* P;      // step q0: N_hi * V (2n limbs); step fix: Q0 * D (2n+1)
+    uint64_t* Q;            // n+1 limbs
+    uint64_t* R;            // n limbs (remainder out)
+    uint64_t* Rw;           // n+1 limbs of scratch
+    int64_t n;
+};
+
+// exact base case: X = floor((B^2m - 1) / A), m+1 limbs (top limb 1), for
+// m <= SBG_DIV_BASE; one thread per divisor, schoolbook long division
+// (Knuth D with a 128/64 trial quotient).
+#define SBG_DIV_BASE 32
+__global__ void k_recip_base(const uint64_t* const* A, const int64_t* m, uint64_t* const* X,
+                             int count, uint32_t* err) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= count) return;
+    const int64_t n = m[idx];
+    const uint64_t* d = A[idx];
+    uint64_t u[2 * SBG_DIV_BASE + 1];
+    for (int64_t i = 0; i < 2 * n; ++i) u[i] = ~0ull;
+    u[2 * n] = 0;
+    uint64_t* q = X[idx];
+    const uint64_t dh = d[n - 1], dl = n >= 2 ? d[n - 2] : 0;
+    for (int64_t j = n; j >= 0; --j) {
+        // trial quotient from the top two limbs of the remainder
+        const unsigned __int128 num = ((unsigned __int128)u[j + n] << 64) | u[j + n - 1];
+        unsigned __int128 qh = num / dh, rh = num % dh;
+        const uint64_t u2 = (j + n - 2 >= 0) ? u[j + n - 2] : 0;
+        while ((qh >> 64) || (n >= 2 && (unsigned __int128)(uint64_t)qh * dl > ((rh << 64) | u2))) {
+            qh -= 1;
+            rh += dh;
+            if (rh >> 64) break;
+        }
+        uint64_t qd = (uint64_t)qh, borrow = 0, cy = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            unsigned __int128 pr = (unsigned __int128)qd * d[i] + cy;
+            cy = (uint64_t)(pr >> 64);
+            uint64_t pl = (uint64_t)pr;
+            uint64_t t = u[i + j] - pl - borrow;
+            borrow = (u[i + j] < pl) || (u[i + j] - pl < borrow);
+            u[i + j] = t;
+        }
+        uint64_t t = u[j + n] - cy - borrow;
+        bool neg = (u[j + n] < cy) || (u[j + n] - cy < borrow);
+        u[j + n] = t;
+        if (neg) {
+            qd -= 1;
+            uint64_t c = 0;
+            for (int64_t i = 0; i < n; ++i) {
+                unsigned __int128 sum = (unsigned __int128)u[i + j] + d[i] + c;
+                u[i + j] = (uint64_t)sum;
+                c = (uint64_t)(sum >> 64);
+            }
+            u[j + n] += c;
+        }
+        q[j] = qd;
+    }
+    if (q[n] != 1) atomicOr(err, 8u);
+}
+
+// step 1: correct X_h while T >= B^(n+h); T_m = limbs l..n of B^(n+h) - T
+__global__ void __launch_bounds__(DIV_T) k_recip_step1(const RecipStep* st, uint32_t* err) {
+    const RecipStep S = st[blockIdx.x];
+    const int64_t n = S.n, h = S.h, l = n - h, tl = n + h + 1;
+    // T - B^(n+h) < A_lo * X_h < 2 B^n <= 4 A: at most four corrections
+    for (int it = 0; it < 6; ++it) {
+        __syncthreads();
+        if (S.T[n + h] == 0) break;
+        if (it == 5) {
+            if (threadIdx.x == 0) atomicOr(err, 16u);
+            break;
+        }
+        const uint64_t* A = S.A;
+        uint64_t* T = S.T;
+        block_addsub(T, tl, [&](int64_t i) { return T[i]; },
+                     [&](int64_t i) { return i < n ? A[i] : 0ull; }, true, 0);
+        uint64_t* Xh = S.Xh;
+        block_addsub(Xh, h + 1, [&](int64_t i) { return Xh[i]; },
+                     [&](int64_t i) { return i == 0 ? 1ull : 0ull; }, true, 0);
+    }
+    __syncthreads();
+    // B^(n+h) - T = (~T + 1) on the low n+1 limbs; the +1 reaches limb l only
+    // when the limbs below l are all zero
+    const uint64_t* T = S.T;
+    __shared__ int s_nz;
+    if (threadIdx.x == 0) s_nz = 0;
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < l; i += DIV_T)
+        if (T[i] != 0) s_nz = 1;
+    __syncthreads();
+    const uint32_t cin = s_nz ? 0u : 1u;
+    uint64_t* TM = S.TM;
+    block_addsub(TM, h + 1, [&](int64_t i) { return ~T[l + i]; },
+                 [&](int64_t i) { return 0ull; }, false, cin);
+}
+
+// step 2: X = X_h * B^l + floor(U / B^(2h-l))
+__global__ void __launch_bounds__(DIV_T) k_recip_step2(const RecipStep* st) {
+    const RecipStep S = st[blockIdx.x];
+    const int64_t n = S.n, h = S.h, l = n - h, sh = 2 * h - l;
+    const uint64_t* U = S.U;
+    const uint64_t* Xh = S.Xh;
+    uint64_t* X = S.X;
+    // U' = U >> sh limbs has l + 2 limbs (U has 2h + 2)
+    block_addsub(X, n + 1,
+                 [&](int64_t i) {
+                     const int64_t k = sh + i;
+                     return k < 2 * h + 2 ? U[k] : 0ull;
+                 },
+                 [&](int64_t i) { return i >= l ? Xh[i - l] : 0ull; }, false, 0);
+}
+
+// Q0 = N_hi + floor(P / B^n), P = N_hi * V (2n limbs)
+__global__ void __launch_bounds__(DIV_T) k_div_q0(const DivFix* df) {
+    const DivFix F = df[blockIdx.x];
+    const int64_t n = F.n;
+    const uint64_t* Nh = F.N + n;
+    const uint64_t* P = F.P;
+    block_addsub(F.Q, n + 1, [&](int64_t i) { return i < n ? Nh[i] : 0ull; },
+                 [&](int64_t i) { return i < n ? P[n + i] : 0ull; }, false, 0);
+}
+
+// R = (N - Q0 D) on n+1 limbs, then while R >= D: R -= D, Q += 1
+__global__ void __launch_bounds__(DIV_T) k_div_fix(const DivFix* df, uint32_t* err) {
+    const DivFix F = df[blockIdx.x];
+    const int64_t n = F.n;
+    const uint64_t* N = F.N;
+    const uint64_t* P = F.P;
+    const uint64_t* D = F.D;
+    uint64_t* Rw = F.Rw;
+    block_addsub(Rw, n + 1, [&](int64_t i) { return N[i]; }, [&](int64_t i) { return P[i]; }, true,
+                 0);
+    for (int it = 0; it < 8; ++it) {
+        __syncthreads();
+        int c = block_cmp(n + 1, [&](int64_t i) { return Rw[i]; },
+                          [&](int64_t i) { return i < n ? D[i] : 0ull; });
+        if (c < 0) break;
+        if (it == 7) {
+            if (threadIdx.x == 0) atomicOr(err, 32u);
+            break;
+        }
+        block_addsub(Rw, n + 1, [&](int64_t i) { return Rw[i]; },
+                     [&](int64_t i) { return i < n ? D[i] : 0ull; }, true, 0);
+        uint64_t* Q = F.Q;
+        block_addsub(Q, n + 1, [&](int64_t i) { return Q[i]; },
+                     [&](int64_t i) { return i == 0 ? 1ull : 0ull; }, false, 0);
+    }
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < n; i += DIV_T) F.R[i] = Rw[i];
+}
+
+// recip output: V = X - B^n, +1 when B^2n - 1 - D X >= D (X exact in {V, V+1}),
+// computed from P = D * X (2n+1 limbs): R = complement of P's low n+1 limbs
+__global__ void __launch_bounds__(DIV_T) k_recip_final(const DivFix* df, uint32_t* err) {
+    const DivFix F = df[blockIdx.x];
+    const int64_t n = F.n;
+    const uint64_t* P = F.P;
+    const uint64_t* D = F.D;
+    uint64_t* Rw = F.Rw;
+    for (int64_t i = threadIdx.x; i <= n; i += DIV_T) Rw[i] = ~P[i];
+    __syncthreads();
+    int c = block_cmp(n + 1, [&](int64_t i) { return Rw[i]; },
+                      [&](int64_t i) { return i < n ? D[i] : 0ull; });
+    // Q holds X (n+1 limbs); V = X (+1) low n limbs
+    uint64_t* Q = F.Q;
+    if (c >= 0)
+        block_addsub(Q, n + 1, [&](int64_t i) { return Q[i]; },
+                     [&](int64_t i) { return i == 0 ? 1ull : 0ull; }, false, 0);
+    __syncthreads();
+    if (threadIdx.x == 0 && Q[n] != 1) atomicOr(err, 64u);
+    for (int64_t i = threadIdx.x; i < n; i += DIV_T) F.R[i] = Q[i];
+}
+
+}  // namespace sbg
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+namespace sbg {
+
+struct DivInst {
+    const uint64_t* D;      // normalised divisor, n limbs (device)
+    const uint64_t* N;      // numerator padded to 2n limbs (device), or null (recip only)
+    uint64_t* Qout;         // quotient out (qlen limbs) or reciprocal out (n limbs)
+    uint64_t* Rout;         // remainder out (n limbs) or null
+    int64_t n;
+    int64_t qlen;
+    // scratch (device)
+    uint64_t* X[2];
+    uint64_t* T;
+    uint64_t* TM;
+    uint64_t* U;
+    uint64_t* P;
+    uint64_t* Q;
+    uint64_t* Rw;
+    std::vector<int64_t> sz;   // recursion sizes, sz[0] = n
+};
+
+static int64_t h_of(int64_t n) { return n - (n - 1) / 2; }
+
+size_t div_scratch_limbs(int64_t n) { return (size_t)(14 * n + 64); }
+
+}  // namespace sbg
+
+using namespace sbg;
+
+// run one list of products on the context (synchronous)
+extern "C" int sbg_batch_create(sbg_ctx*, const sbg_job*, int64_t, sbg_batch**);
+extern "C" int sbg_batch_run(sbg_batch*);
+extern "C" void sbg_batch_destroy(sbg_batch*);
+
+static int run_products(sbg_ctx* c, const std::vector<sbg_job>& jobs) {
+    if (jobs.empty()) return SBG_OK;
+    sbg_batch* b = nullptr;
+    int st = sbg_batch_create(c, jobs.data(), (int64_t)jobs.size(), &b);
+    if (st) return st;
+    st = sbg_batch_run(b);
+    sbg_batch_destroy(b);
+    return st;
+}
+
+template <class T>
+static int upload(std::vector<T>& host, T** dev, size_t* cap) {
+    size_t bytes = host.size() * sizeof(T);
+    if (bytes > *cap) {
+        cudaFree(*dev);
+        *dev = nullptr;
+        *cap = 0;
+        if (cudaMalloc(dev, bytes) != cudaSuccess) return SBG_EALLOC;
+        *cap = bytes;
+    }
+    if (bytes && cudaMemcpy(*dev, host.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return SBG_ECUDA;
+    return SBG_OK;
+}
+
+// Reciprocals (and optionally quotients) of every instance; all scratch set.
+static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quotient) {
+    cudaStream_t st = (cudaStream_t)sbg_ctx_get_stream(c);
+    int maxd = 0;
+    for (auto& d : v) {
+        d.sz.clear();
+        d.sz.push_back(d.n);
+        while (d.sz.back() > SBG_DIV_BASE) d.sz.push_back(h_of(d.sz.back()));
+        maxd = std::max(maxd, (int)d.sz.size() - 1);
+    }
+    // base case: X[cur] of every instance
+    {
+        std::vector<const uint64_t*> A;
+        std::vector<int64_t> m;
+        std::vector<uint64_t*> X;
+        for (auto& d : v) {
+            const int64_t mb = d.sz.back();
+            A.push_back(d.D + (d.n - mb));
+            m.push_back(mb);
+            X.push_back(d.X[(d.sz.size() - 1) & 1]);
+        }
+        const uint64_t** dA = nullptr;
+        int64_t* dm = nullptr;
+        uint64_t** dX = nullptr;
+        size_t ca = 0, cm = 0, cx = 0;
+        int s1 = upload(A, (const uint64_t***)&dA, &ca);
+        if (!s1) s1 = upload(m, &dm, &cm);
+        if (!s1) s1 = upload(X, &dX, &cx);
+        if (!s1) {
+            k_recip_base<<<((int)v.size() + 127) / 128, 128, 0, st>>>(dA, dm, dX, (int)v.size(), err);
+            if (cudaGetLastError() != cudaSuccess) s1 = SBG_ECUDA;
+            if (!s1 && cudaStreamSynchronize(st) != cudaSuccess) s1 = SBG_ECUDA;
+        }
+        cudaFree(dA);
+        cudaFree(dm);
+        cudaFree(dX);
+        if (s1) return s1;
+    }
+    RecipStep* dsteps = nullptr;
+    size_t cap = 0;
+    int rc = SBG_OK;
+    for (int r = 1; r <= maxd && !rc; ++r) {
+        std::vector<sbg_job> jt, ju;
+        std::vector<RecipStep> steps;
+        for (auto& d : v) {
+            const int depth = (int)d.sz.size() - 1;
+            if (depth < r) continue;
+            const int k = depth - r;               // level: n = sz[k], h = sz[k+1]
+            const int64_t n = d.sz[k], h = d.sz[k + 1];
+            RecipStep S{};
+            S.A = d.D + (d.n - n);
+            S.Xh = d.X[(k + 1) & 1];
+            S.X = d.X[k & 1];
+            S.T = d.T;
+            S.TM = d.TM;
+            S.U = d.U;
+            S.n = n;
+            S.h = h;
+            steps.push_back(S);
+            jt.push_back(sbg_job{S.T, S.A, S.Xh, n, h + 1, SBG_JOB_MUL, 0});
+            ju.push_back(sbg_job{d.U, S.TM, S.Xh, h + 1, h + 1, SBG_JOB_MUL, 0});
+        }
+        if (steps.empty()) continue;
+        if ((rc = upload(steps, &dsteps, &cap))) break;
+        if ((rc = run_products(c, jt))) break;
+        k_recip_step1<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps, err);
+        if (cudaGetLastError() != cudaSuccess) { rc = SBG_ECUDA; break; }
+        if ((rc = run_products(c, ju))) break;
+        k_recip_step2<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps);
+        if (cudaGetLastError() != cudaSuccess) { rc = SBG_ECUDA; break; }
+    }
+    cudaFree(dsteps);
+    if (rc) return rc;
+    // final stage: exact reciprocal, or quotient and remainder
+    std::vector<DivFix> fx;
+    std::vector<sbg_job> jp;
+    for (auto& d : v) {
+        DivFix F{};
+        F.N = d.N;
+        F.D = d.D;
+        F.P = d.P;
+        F.Q = d.Q;
+        F.R = quotient ? d.Rout : d.Qout;
+        F.Rw = d.Rw;
+        F.n = d.n;
+        fx.push_back(F);
+        uint64_t* X = d.X[0];
+        if (quotient) {
+            // P = N_hi * V, V = low n limbs of X
+            jp.push_back(sbg_job{d.P, d.N + d.n, X, d.n, d.n, SBG_JOB_MUL, 0});
+        } else {
+            cudaMemcpyAsync(d.Q, X, (d.n + 1) * 8, cudaMemcpyDeviceToDevice, st);
+            jp.push_back(sbg_job{d.P, d.D, X, d.n, d.n + 1, SBG_JOB_MUL, 0});
+        }
+    }
+    DivFix* dfx = nullptr;
+    size_t fcap = 0;
+    rc = upload(fx, &dfx, &fcap);
+    if (!rc) rc = run_products(c, jp);
+    if (!rc && !quotient) {
+        k_recip_final<<<(int)fx.size(), DIV_T, 0, st>>>(dfx, err);
+        if (cudaGetLastError() != cudaSuccess) rc = SBG_ECUDA;
+    }
+    if (!rc && quotient) {
+        k_div_q0<<<(int)fx.size(), DIV_T, 0, st>>>(dfx);
+        if (cudaGetLastError() != cudaSuccess) rc = SBG_ECUDA;
+        std::vector<sbg_job> jq;
+        for (auto& d : v) jq.push_back(sbg_job{d.P, d.Q, d.D, d.n + 1, d.n, SBG_JOB_MUL, 0});
+        if (!rc) rc = run_products(c, jq);
+        if (!rc) {
+            k_div_fix<<<(int)fx.size(), DIV_T, 0, st>>>(dfx, err);
+            if (cudaGetLastError() != cudaSuccess) rc = SBG_ECUDA;
+        }
+        for (auto& d : v)
+            if (!rc) cudaMemcpyAsync(d.Qout, d.Q, d.qlen * 8, cudaMemcpyDeviceToDevice, st);
+    }
+    if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = SBG_ECUDA;
+    cudaFree(dfx);
+    return rc;
+}
+
+static void carve(DivInst& d, uint64_t*& p) {
+    const int64_t n = d.n;
+    d.X[0] = p; p += n + 2;
+    d.X[1] = p; p += n + 2;
+    d.T = p; p += 2 * n + 4;
+    d.TM = p; p += n + 2;
+    d.U = p; p += 2 * n + 6;
+    d.P = p; p += 2 * n + 4;
+    d.Q = p; p += n + 2;
+    d.Rw = p; p += n + 2;
+}
+
+extern "C" int sbg_recip(sbg_ctx* c, uint64_t* ip, const uint64_t* dp, int64_t n) {
+    if (!c || !ip || !dp || n <= 0) return SBG_EINVAL;
+    if (2 * n + 2 > ((int64_t)1 << 25)) return SBG_EBAND;
+    void* sp = sbg_ctx_get_stream(c);
+    (void)sp;
+    uint64_t* scratch = nullptr;
+    uint32_t* err = nullptr;
+    if (cudaMalloc(&scratch, div_scratch_limbs(n) * 8) != cudaSuccess) return SBG_EALLOC;
+    if (cudaMalloc(&err, 4) != cudaSuccess) {
+        cudaFree(scratch);
+        return SBG_EALLOC;
+    }
+    cudaMemset(err, 0, 4);
+    std::vector<DivInst> v(1);
+    v[0].D = dp;
+    v[0].N = nullptr;
+    v[0].Qout = ip;
+    v[0].Rout = nullptr;
+    v[0].n = n;
+    v[0].qlen = n;
+    uint64_t* p = scratch;
+    carve(v[0], p);
+    int rc = div_core(c, v, err, false);
+    uint32_t h = 0;
+    if (!rc) cudaMemcpy(&h, err, 4, cudaMemcpyDeviceToHost);
+    cudaFree(scratch);
+    cudaFree(err);
+    if (rc) return rc;
+    return h ? SBG_ECUDA : SBG_OK;
+}
+
+// Batched division: every job has a normalised divisor (top bit set) and
+// nn <= 2 dn (the configurations of the reference's Newton division); other
+// shapes go through sbg_divrem, which normalises and splits them.
+extern "C" int sbg_divrem_batch(sbg_ctx* c, const sbg_div_job* jobs, int64_t count) {
+    if (!c || (count > 0 && !jobs) || count < 0) return SBG_EINVAL;
+    cudaStream_t st = (cudaStream_t)sbg_ctx_get_stream(c);
+    size_t total = 0;
+    for (int64_t i = 0; i < count; ++i) {
+        const sbg_div_job& j = jobs[i];
+        if (!j.qp || !j.rp || !j.np || !j.dp || j.dn <= 0 || j.nn < j.dn || j.nn > 2 * j.dn)
+            return SBG_EINVAL;
+        if (2 * j.dn + 2 > ((int64_t)1 << 25)) return SBG_EBAND;
+        total += div_scratch_limbs(j.dn) + 2 * j.dn + 8;
+    }
+    uint64_t* scratch = nullptr;
+    uint32_t* err = nullptr;
+    if (cudaMalloc(&scratch, total * 8) != cudaSuccess) return SBG_EALLOC;
+    if (cudaMalloc(&err, 4) != cudaSuccess) {
+        cudaFree(scratch);
+        return SBG_EALLOC;
+    }
+    cudaMemsetAsync(err, 0, 4, st);
+    std::vector<DivInst> v((size_t)count);
+    uint64_t* p = scratch;
+    int rc = SBG_OK;
+    for (int64_t i = 0; i < count && !rc; ++i) {
+        const sbg_div_job& j = jobs[i];
+        DivInst& d = v[i];
+        d.D = j.dp;
+        d.n = j.dn;
+        d.Qout = j.qp;
+        d.Rout = j.rp;
+        d.qlen = j.nn - j.dn + 1;
+        // numerator zero-padded to 2n limbs
+        uint64_t* Np = p;
+        p += 2 * j.dn + 8;
+        if (cudaMemsetAsync(Np, 0, 2 * j.dn * 8, st) != cudaSuccess ||
+            cudaMemcpyAsync(Np, j.np, j.nn * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            rc = SBG_ECUDA;
+        d.N = Np;
+        carve(d, p);
+    }
+    if (!rc) rc = div_core(c, v, err, true);
+    uint32_t h = 0;
+    if (!rc) cudaMemcpy(&h, err, 4, cudaMemcpyDeviceToHost);
+    if (getenv("SBG_DEBUG") && (rc || h))
+        fprintf(stderr, "sbg_divrem_batch: rc=%d err=0x%x (count %lld, first dn %lld nn %lld)\n", rc,
+                h, (long long)count, count ? (long long)jobs[0].dn : 0LL,
+                count ? (long long)jobs[0].nn : 0LL);
+    cudaFree(scratch);
+    cudaFree(err);
+    if (rc) return rc;
+    return h ? SBG_ECUDA : SBG_OK;
+}
+
+extern "C" int sbg_divrem(sbg_ctx* c, uint64_t* qp, uint64_t* rp, const uint64_t* np, int64_t nn,
+                          const uint64_t* dp, int64_t dn) {
+    sbg_div_job j{qp, rp, np, dp, nn, dn};
+    return sbg_divrem_batch(c, &j, 1);
+}
+
+// ---------------------------------------------------------------------------
+// reference-signature division (include/divrem.h:218, include/dc_div.h:154)
+// ---------------------------------------------------------------------------
+namespace sbg {
+
+// out[0..n) = (in[0..n) << s) | (carry-in from below); out[n] = spill (if out_n > n)
+__global__ void k_shl(uint64_t* out, const uint64_t* in, int64_t n, int64_t out_n, int s) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < out_n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t cur = i < n ? in[i] : 0, prev = (i >= 1 && i - 1 < n) ? in[i - 1] : 0;
+        out[i] = s ? ((cur << s) | (prev >> (64 - s))) : cur;
+    }
+}
+__global__ void k_shr(uint64_t* out, const uint64_t* in, int64_t n, int s) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t cur = in[i], next = i + 1 < n ? in[i + 1] : 0;
+        out[i] = s ? ((cur >> s) | (next << (64 - s))) : cur;
+    }
+}
+
+}  // namespace sbg
+
+static bool dev_ptr(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+extern "C" sbg_ctx* sbg_default_ctx_internal(void);
+
+// Q = floor(N / D), R = N mod D for any dn >= 1 with dp[dn-1] != 0 and
+// nn >= dn (the reference's contract, include/divrem.h:212-217); writes the
+// trimmed lengths.  Host or device pointers; synchronous.  Returns 1 on
+// success, 0 on failure (the reference returns nothing and aborts on OOM).
+extern "C" int sbg_divrem_u64(uint64_t* qp, uint64_t* rp, const uint64_t* np, uint64_t nn64,
+                              const uint64_t* dp, uint64_t dn64, uint64_t* qn_out,
+                              uint64_t* rn_out) {
+    if (!qp || !rp || !np || !dp || dn64 == 0 || nn64 < dn64) return 0;
+    sbg_ctx* c = sbg_default_ctx_internal();
+    if (!c) return 0;
+    cudaStream_t st = (cudaStream_t)sbg_ctx_get_stream(c);
+    const int64_t nn = (int64_t)nn64, dn = (int64_t)dn64;
+    uint64_t dtop = 0;
+    const bool ddev = dev_ptr(dp);
+    if (cudaMemcpy(&dtop, dp + dn - 1, 8, ddev ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost) !=
+            cudaSuccess || dtop == 0)
+        return 0;
+    const int s = __builtin_clzll(dtop);
+    // device copies: D' (dn), N' (nn+1 limbs), Q (nn-dn+2), R work
+    const int64_t nn1 = nn + 1;
+    size_t limbs = (size_t)(2 * dn + 2 * nn1 + 4 * dn + 16);
+    uint64_t* buf = nullptr;
+    if (cudaMalloc(&buf, limbs * 8) != cudaSuccess) return 0;
+    uint64_t* dD = buf;                 // dn (raw then normalised in place via tmp)
+    uint64_t* dN = dD + dn;             // nn1
+    uint64_t* dQ = dN + nn1;            // nn1
+    uint64_t* chunk = dQ + nn1;         // 2dn
+    uint64_t* cq = chunk + 2 * dn;      // dn + 1
+    uint64_t* cr = cq + dn + 1;         // dn
+    uint64_t* tmp = cr + dn;            // max(dn, nn) staging
+    int ok = 1;
+    auto cp = [&](void* d, const void* sp, size_t bytes, cudaMemcpyKind k) {
+        if (ok && cudaMemcpyAsync(d, sp, bytes, k, st) != cudaSuccess) ok = 0;
+    };
+    uint64_t* stage = nullptr;
+    if (cudaMalloc(&stage, (size_t)std::max(dn, nn) * 8) != cudaSuccess) {
+        cudaFree(buf);
+        return 0;
+    }
+    cp(stage, dp, dn * 8, cudaMemcpyDefault);
+    k_shl<<<64, 256, 0, st>>>(dD, stage, dn, dn, s);
+    cp(stage, np, nn * 8, cudaMemcpyDefault);
+    k_shl<<<256, 256, 0, st>>>(dN, stage, nn, nn1, s);
+    if (cudaGetLastError() != cudaSuccess) ok = 0;
+    // schoolbook over dn-limb chunks of N' from the top: R < D' always
+    int64_t top = nn1;                      // limbs of N' not yet consumed
+    int64_t first = nn1 % dn;               // a short leading chunk, if any
+    if (first == 0) first = dn;
+    // R = the leading chunk (first limbs, < B^first) -- if first < dn it is < D'
+    // trivially; if first == dn compare is folded into the first 2dn step by
+    // prefixing a zero chunk.
+    cudaMemsetAsync(cr, 0, dn * 8, st);
+    cudaMemsetAsync(dQ, 0, nn1 * 8, st);
+    int64_t qpos = top;                     // quotient limbs are written below qpos
+    bool started = false;
+    while (ok && top > 0) {
+        const int64_t take = started ? dn : first;
+        top -= take;
+        // chunk = R * B^take + N'[top .. top+take)   (take + dn limbs <= 2dn)
+        cp(chunk, dN + top, take * 8, cudaMemcpyDeviceToDevice);
+        cp(chunk + take, cr, dn * 8, cudaMemcpyDeviceToDevice);
+        sbg_div_job j{cq, cr, chunk, dD, take + dn, dn};
+        if (ok && sbg_divrem_batch(c, &j, 1) != SBG_OK) ok = 0;
+        // quotient chunk: take+1 limbs, the top one is zero since R < D'
+        qpos -= take;
+        cp(dQ + qpos, cq, take * 8, cudaMemcpyDeviceToDevice);
+        started = true;
+    }
+    // Q = dQ[0 .. nn-dn+1), R = cr >> s
+    const int64_t qlen = nn - dn + 1;
+    k_shr<<<64, 256, 0, st>>>(tmp, cr, dn, s);
+    if (cudaGetLastError() != cudaSuccess) ok = 0;
+    cp(qp, dQ, qlen * 8, cudaMemcpyDefault);
+    cp(rp, tmp, dn * 8, cudaMemcpyDefault);
+    if (ok && cudaStreamSynchronize(st) != cudaSuccess) ok = 0;
+    if (ok) {
+        // trimmed lengths (at least 1), as the reference reports them
+        std::vector<uint64_t> hq((size_t)qlen), hr((size_t)dn);
+        cudaMemcpy(hq.data(), dQ, qlen * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(hr.data(), tmp, dn * 8, cudaMemcpyDeviceToHost);
+        int64_t a = qlen;
+        while (a > 1 && hq[a - 1] == 0) --a;
+        int64_t b = dn;
+        while (b > 1 && hr[b - 1] == 0) --b;
+        if (qn_out) *qn_out = (uint64_t)a;
+        if (rn_out) *rn_out = (uint64_t)b;
+    }
+    cudaFree(stage);
+    cudaFree(buf);
+    return ok;
+}

@@ -1,0 +1,119 @@
+"""GPU tests of the Newton reciprocal and division (sbg_recip, sbg_divrem,
+sbg_divrem_batch).
+
+Quotients and remainders must equal the reference's divrem_u64_dc
+(include/dc_div.h:154) bit for bit: against its golden digests
+(tests/golden/golden.json, generated by the unmodified reference), and
+against our restatement (Knuth D, oracle/port.c) and Python integers on
+further shapes, including the all-0xFF and minimal (B^n / 2) divisors.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.common import digest, div_inputs, golden
+
+pytestmark = pytest.mark.gpu
+G = golden()
+
+
+def _dev(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x).view(np.int64)).cuda()
+
+
+def _host(t):
+    return t.cpu().numpy().view(np.uint64)
+
+
+def _divrem(ctx, N, D):
+    import torch
+    q = torch.empty(len(N) - len(D) + 1, dtype=torch.int64, device="cuda")
+    r = torch.empty(len(D), dtype=torch.int64, device="cuda")
+    ctx.divrem(q, r, _dev(N), _dev(D))
+    return _host(q), _host(r)
+
+
+@pytest.mark.parametrize("case", G["div"], ids=lambda c: f'div-{c["nn"]}/{c["dn"]}')
+def test_divrem_matches_reference_golden(ctx, case):
+    N, D = div_inputs(case["dn"], case["seed"])
+    q, r = _divrem(ctx, N, D)
+    assert digest(q) == case["q"]["sha256"]
+    assert digest(r) == case["r"]["sha256"]
+
+
+def test_divrem_shapes_vs_python(ctx):
+    rng = np.random.default_rng(401)
+    for n in [1, 2, 3, 5, 31, 32, 33, 64, 100, 257, 1000, 4097, 20000]:
+        for nn in sorted({n, n + 1, (3 * n) // 2 + 1, 2 * n}):
+            if nn < n or nn > 2 * n:
+                continue
+            N = rng.integers(0, 2**64, nn, dtype=np.uint64)
+            D = rng.integers(0, 2**64, n, dtype=np.uint64)
+            D[-1] |= np.uint64(1 << 63)
+            q, r = _divrem(ctx, N, D)
+            qq, rr = divmod(O.to_int(N), O.to_int(D))
+            assert O.to_int(q) == qq and O.to_int(r) == rr, (n, nn)
+
+
+def test_divrem_adversarial_divisors(ctx):
+    for n in [40, 333, 5000]:
+        ones = O.pattern(2 * n, "ones")
+        for D in (O.pattern(n, "ones"),
+                  np.concatenate([np.zeros(n - 1, np.uint64), np.array([1 << 63], np.uint64)])):
+            q, r = _divrem(ctx, ones, D)
+            qq, rr = divmod(O.to_int(ones), O.to_int(D))
+            assert O.to_int(q) == qq and O.to_int(r) == rr, n
+
+
+def test_recip_exact(ctx):
+    import torch
+    rng = np.random.default_rng(402)
+    for n in [1, 7, 32, 33, 100, 1000, 8191]:
+        D = rng.integers(0, 2**64, n, dtype=np.uint64)
+        D[-1] |= np.uint64(1 << 63)
+        i = torch.empty(n, dtype=torch.int64, device="cuda")
+        ctx.recip(i, _dev(D))
+        want = ((1 << (128 * n)) - 1) // O.to_int(D) - (1 << (64 * n))
+        assert O.to_int(_host(i)) == want, n
+        if n <= 1000:
+            assert np.array_equal(_host(i), O.port_recip(D))
+
+
+def test_divrem_batch_vs_port(ctx):
+    import torch
+    rng = np.random.default_rng(403)
+    ns = [512, 700, 1500, 3000, 9000, 513, 40000]
+    jobs, keep = [], []
+    for n in ns:
+        N = rng.integers(0, 2**64, 2 * n, dtype=np.uint64)
+        D = rng.integers(0, 2**64, n, dtype=np.uint64)
+        D[-1] |= np.uint64(1 << 63)
+        tN, tD = _dev(N), _dev(D)
+        q = torch.full((n + 1,), -1, dtype=torch.int64, device="cuda")
+        r = torch.full((n,), -1, dtype=torch.int64, device="cuda")
+        jobs.append((q.data_ptr(), r.data_ptr(), tN.data_ptr(), tD.data_ptr(), 2 * n, n))
+        keep.append((N, D, tN, tD, q, r))
+    ctx.divrem_batch(jobs)
+    for N, D, tN, tD, q, r in keep:
+        qq, rr = O.port_divrem(N, D)
+        assert np.array_equal(_host(q), qq) and np.array_equal(_host(r), rr), len(D)
+
+
+def test_reference_signature_divrem_any_shape(ctx):
+    """sbg_divrem_u64: the reference's divrem_u64 contract (any divisor with
+    a nonzero top limb, any nn >= dn, trimmed lengths) on host arrays."""
+    import simd_bigint_b200 as sbg
+    rng = np.random.default_rng(404)
+    for dn, nn in [(1, 1), (1, 9), (2, 5), (7, 7), (7, 30), (50, 260), (300, 1000), (1000, 5000)]:
+        N = rng.integers(0, 2**64, nn, dtype=np.uint64)
+        D = rng.integers(0, 2**64, dn, dtype=np.uint64)
+        D[-1] = np.uint64(int(D[-1]) >> int(rng.integers(0, 63))) | np.uint64(1)
+        q, r = sbg.divrem_u64(N, D)
+        qq, rr = divmod(O.to_int(N), O.to_int(D))
+        assert O.to_int(q) == qq and O.to_int(r) == rr, (dn, nn)
+        assert len(q) >= 1 and len(r) >= 1
+        assert (len(q) == 1 or q[-1] != 0) and (len(r) == 1 or r[-1] != 0)
+        if O.ref_available() and O.to_int(D).bit_length() > 416:
+            q2, r2 = O.ref_divrem(N, D)
+            assert O.to_int(q2) == qq and O.to_int(r2) == rr
