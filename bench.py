@@ -39,6 +39,7 @@ WORKLOADS = {
     "mul2p24x2p20": ("mul", 1 << 24, 1 << 20),
     "mul16k": ("mul", 16384, 16384),
     "batch4096": ("batch", 4096, 0),     # the batched mixed-size configuration
+    "div1024": ("div", 1024, 0),         # the batched Newton division configuration
 }
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
@@ -466,6 +467,138 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
     return res
 
 
+# ------------------------------------------------------- division workload --
+def _div_worker(ns, seed, steps, warmup, barrier, queue):
+    """One baseline process: its share of the divisions through the
+    reference's divrem_u64_dc (the port's Knuth D where the reference cannot run)."""
+    try:
+        from oracle import oracle as O
+        from simd_bigint_b200.workloads import fill_limbs
+        rng = np.random.default_rng(seed)
+        ops = []
+        for n in ns:
+            ops.append((fill_limbs(2 * n, rng), fill_limbs(n, rng, top_bit=True)))
+        use_ref = O.ref_available()
+
+        def one():
+            for N, D in ops:
+                (O.ref_divrem(N, D) if use_ref else O.port_divrem(N, D))
+        for _ in range(max(1, warmup)):
+            one()
+        times = []
+        for _ in range(steps):
+            barrier.wait(timeout=3600)
+            t = time.perf_counter()
+            one()
+            times.append(time.perf_counter() - t)
+        queue.put(("ok", 0.0, times))
+    except Exception as e:
+        try:
+            barrier.abort()
+        except Exception:
+            pass
+        queue.put(("err", repr(e), []))
+
+
+def cpu_run_div(ns, procs: int, steps: int, warmup: int) -> dict:
+    import multiprocessing as mp
+    from oracle import oracle as O
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs)
+    queue = ctx.Queue()
+    order = sorted(range(len(ns)), key=lambda i: -ns[i])
+    parts = [[ns[i] for i in order[k::procs]] for k in range(procs)]
+    ps = [ctx.Process(target=_div_worker, args=(parts[k], 200 + k, steps, warmup, barrier, queue))
+          for k in range(procs)]
+    for p in ps:
+        p.start()
+    res = [queue.get(timeout=7200) for _ in ps]
+    for p in ps:
+        p.join(timeout=60)
+    errs = [r[1] for r in res if r[0] != "ok"]
+    if errs:
+        raise RuntimeError("CPU division baseline failed: " + errs[0])
+    step = statistics.median([max(r[2][k] for r in res) for k in range(steps)])
+    total = sum(2 * n for n in ns)
+    cpu = O.host_cpu()
+    return {"value": total / step / 1e6, "unit": "Mlimb/s", "cores": procs,
+            "kind": "reference" if O.ref_available() else "port", "step_s": step,
+            "sample": f"the {len(ns)} divisions dealt over {procs} single-threaded processes "
+                      f"(reference divrem_u64_dc), median of {steps} steps",
+            "cpu_model": cpu["model"], "host_cores": cpu["cores"],
+            "isa": [f for f in O.REF_ISA if f in cpu["flags"]]}
+
+
+def run_div(args, ws, rank, local, pg) -> dict | None:
+    import torch
+
+    import simd_bigint_b200 as sbg
+    from oracle import oracle as O
+    from simd_bigint_b200.workloads import division_shapes, fill_limbs
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ns = division_shapes(1024, seed=4242)
+    rng = np.random.default_rng(991 + rank)
+    hostN = [fill_limbs(2 * n, rng) for n in ns]
+    hostD = [fill_limbs(n, rng, top_bit=True) for n in ns]
+    tN = [torch.from_numpy(x.view(np.int64)).to(dev) for x in hostN]
+    tD = [torch.from_numpy(x.view(np.int64)).to(dev) for x in hostD]
+    tQ = [torch.empty(n + 1, dtype=torch.int64, device=dev) for n in ns]
+    tR = [torch.empty(n, dtype=torch.int64, device=dev) for n in ns]
+    jobs = [(q.data_ptr(), r.data_ptr(), a.data_ptr(), d.data_ptr(), 2 * n, n)
+            for q, r, a, d, n in zip(tQ, tR, tN, tD, ns)]
+    ctx = sbg.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream)
+    clocks = ClockSampler(local)
+    if rank == 0:
+        clocks.start()
+    warm = max(1, min(args.warmup, 2))
+    for _ in range(warm):
+        ctx.divrem_batch(jobs)
+    # Q D + R == N and R < D for every division (modular check with two
+    # 61-bit primes plus an exact compare)
+    qs = (2305843009213693951, 2305843009213693921)
+    exact = True
+    for N, D, q, r in zip(hostN, hostD, tQ, tR):
+        Q = q.cpu().numpy().view(np.uint64)
+        R = r.cpu().numpy().view(np.uint64)
+        for p in qs:
+            if (O.mod_u64(Q, p) * O.mod_u64(D, p) + O.mod_u64(R, p)) % p != O.mod_u64(N, p):
+                exact = False
+        hi = np.nonzero(R != D)[0]
+        if len(hi) == 0 or R[hi[-1]] > D[hi[-1]]:
+            exact = False
+    steps = max(1, min(args.steps, 5))
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ctx.divrem_batch(jobs)
+    torch.cuda.synchronize()
+    dt = barrier_max(pg, time.perf_counter() - t0, dev) / steps
+    clk = clocks.stop() if rank == 0 else None
+    total = sum(2 * n for n in ns)
+    if rank != 0:
+        ctx.close()
+        return None
+    res = {
+        "metric": "numerator Mlimb/s (batched Newton divrem)", "value": round(total * ws / dt / 1e6, 2),
+        "unit": "Mlimb/s", "n_gpus": ws, "steps": steps, "warmup": warm, "ms_per_step": round(dt * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic: seeded uniform u64 limbs, divisor top bit set",
+        "config": {"workload": "1024 divisions of 2n by n limbs, n log-uniform [512, 262144] (seed 4242); "
+                               "Newton reciprocal + quotient, all divisions in lockstep",
+                   "numerator_limbs": total, "parallelism": f"replicas x{ws}"},
+        "divisions_per_s": round(len(ns) * ws / dt, 1),
+        "bit_exact": bool(exact),
+        "e2e": None, "gpu_launches": None, "roofline": None, "clocks": clk,
+    }
+    ctx.close()
+    return res
+
+
 # ------------------------------------------------------------- our arm -----
 def run_ours(args, ws, rank, local, pg) -> dict | None:
     import torch
@@ -630,6 +763,10 @@ def main():
             from simd_bigint_b200.workloads import mixed_batch_shapes
             r = cpu_run_batch(mixed_batch_shapes(4096, seed=12345), threads, steps, 1)
             an, bn = 4096, 0
+        elif op == "div":
+            from simd_bigint_b200.workloads import division_shapes
+            r = cpu_run_div(division_shapes(1024, seed=4242), threads, steps, 0)
+            an, bn = 1024, 0
         else:
             r = cpu_run(op, an, bn, threads, steps=steps, warmup=1)
         out = {"metric": "product Mlimb/s", "value": round(r["value"], 3), "unit": "Mlimb/s",
@@ -648,6 +785,8 @@ def main():
     ws, rank, local, pg = dist_init()
     if op == "batch":
         res = run_batch(args, ws, rank, local, pg)
+    elif op == "div":
+        res = run_div(args, ws, rank, local, pg)
     else:
         res = run_ours(args, ws, rank, local, pg)
     if pg is not None:
@@ -661,6 +800,10 @@ def main():
                 from simd_bigint_b200.workloads import mixed_batch_shapes
                 res["cpu_baseline"] = cpu_run_batch(mixed_batch_shapes(4096, seed=12345),
                                                     cpu_threads_for(1 << 16, 1 << 16, cap=32), 2, 1)
+            elif op == "div":
+                from simd_bigint_b200.workloads import division_shapes
+                res["cpu_baseline"] = cpu_run_div(division_shapes(1024, seed=4242),
+                                                  cpu_threads_for(1 << 18, 1 << 18, cap=32), 1, 0)
             else:
                 res["cpu_baseline"] = cpu_bounded(op, an, bn)
         except Exception as e:  # recorded, not fatal

@@ -458,6 +458,9 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
             ju.push_back(sbg_job{d.U, S.TM, S.Xh, h + 1, h + 1, SBG_JOB_MUL, 0});
         }
         if (steps.empty()) continue;
+        // the previous round's kernels still read dsteps: the (synchronous,
+        // default-stream) upload must not overtake them on our non-blocking stream
+        if (cudaStreamSynchronize(st) != cudaSuccess) { rc = SBG_ECUDA; break; }
         if ((rc = upload(steps, &dsteps, &cap))) break;
         if ((rc = run_products(c, jt))) break;
         k_recip_step1<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps, err);
@@ -466,6 +469,7 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
         k_recip_step2<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps);
         if (cudaGetLastError() != cudaSuccess) { rc = SBG_ECUDA; break; }
     }
+    if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = SBG_ECUDA;
     cudaFree(dsteps);
     if (rc) return rc;
     // final stage: exact reciprocal, or quotient and remainder
@@ -492,6 +496,7 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
     }
     DivFix* dfx = nullptr;
     size_t fcap = 0;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return SBG_ECUDA;
     rc = upload(fx, &dfx, &fcap);
     if (!rc) rc = run_products(c, jp);
     if (!rc && !quotient) {

@@ -117,3 +117,28 @@ def test_reference_signature_divrem_any_shape(ctx):
         if O.ref_available() and O.to_int(D).bit_length() > 416:
             q2, r2 = O.ref_divrem(N, D)
             assert O.to_int(q2) == qq and O.to_int(r2) == rr
+
+
+def test_divrem_many_in_flight(ctx):
+    """A wide batch (many divisions, many recursion rounds in flight): every
+    quotient and remainder satisfies Q D + R = N (mod two 61-bit primes) with
+    0 <= R < D.  Guards the per-round descriptor reuse across rounds."""
+    import torch
+
+    from simd_bigint_b200.workloads import division_shapes, fill_limbs
+    ns = division_shapes(160, seed=77, lo=512, hi=40000)
+    rng = np.random.default_rng(405)
+    hostN = [fill_limbs(2 * n, rng) for n in ns]
+    hostD = [fill_limbs(n, rng, top_bit=True) for n in ns]
+    tN = [_dev(x) for x in hostN]
+    tD = [_dev(x) for x in hostD]
+    tQ = [torch.zeros(n + 1, dtype=torch.int64, device="cuda") for n in ns]
+    tR = [torch.zeros(n, dtype=torch.int64, device="cuda") for n in ns]
+    ctx.divrem_batch([(q.data_ptr(), r.data_ptr(), a.data_ptr(), d.data_ptr(), 2 * n, n)
+                      for q, r, a, d, n in zip(tQ, tR, tN, tD, ns)])
+    for N, D, q, r in zip(hostN, hostD, tQ, tR):
+        Q, R = _host(q), _host(r)
+        for p in (2305843009213693951, 2305843009213693921):
+            assert (O.mod_u64(Q, p) * O.mod_u64(D, p) + O.mod_u64(R, p)) % p == O.mod_u64(N, p)
+        hi = np.nonzero(R != D)[0]
+        assert len(hi) and R[hi[-1]] < D[hi[-1]]
