@@ -148,6 +148,51 @@ typedef struct {
 } sbg_div_job;
 int sbg_divrem_batch(sbg_ctx *ctx, const sbg_div_job *jobs, int64_t count);
 
+/* ---- serving loop -------------------------------------------------------------
+ * Continuous batching of independent requests with admission by HBM
+ * footprint; no counterpart in the reference.  Requests name DEVICE operands
+ * (which must stay valid until the request completes); results are written
+ * into the server's HBM arena and stay there until sbg_server_release.
+ * A scheduler thread forms batches from the head of the request FIFO while
+ * their footprint (workspace + result) fits the arena, and runs up to
+ * `slots` batches concurrently on their own streams; reciprocal requests are
+ * batched by a second thread.  Latency is measured from sbg_server_submit to
+ * the moment the server observes the result on the device. */
+enum { SBG_REQ_MUL = 0, SBG_REQ_SQR = 1, SBG_REQ_RECIP = 2 };
+typedef struct {
+    int32_t kind;          /* SBG_REQ_*; RECIP: ap = normalised divisor (an limbs) */
+    int32_t reserved;
+    const uint64_t *ap;
+    int64_t an;
+    const uint64_t *bp;    /* MUL only */
+    int64_t bn;
+} sbg_request;
+typedef struct {
+    uint64_t ticket;
+    int32_t status;        /* SBG_OK or an error code */
+    int32_t reserved;
+    uint64_t *rp;          /* device result: an+bn (mul), 2an (sqr), an (recip) limbs */
+    int64_t rn;
+    double latency_s;
+} sbg_completion;
+typedef struct {
+    size_t arena_bytes;    /* HBM budget for workspaces and results (default 8 GiB) */
+    int32_t slots;         /* batches in flight (default 4) */
+    int32_t max_batch;     /* requests per batch (default 512) */
+} sbg_server_config;
+typedef struct sbg_server sbg_server;
+int sbg_server_create(sbg_ctx *ctx, const sbg_server_config *cfg, sbg_server **out);
+/* Thread-safe, non-blocking.  SBG_EADMIT: the request can never fit the arena. */
+int sbg_server_submit(sbg_server *srv, const sbg_request *req, uint64_t *ticket);
+/* Up to max completions; waits up to wait_ms for the first. */
+int sbg_server_poll(sbg_server *srv, sbg_completion *out, int max, int *n, int wait_ms);
+/* Frees a completed request's result buffer. */
+int sbg_server_release(sbg_server *srv, uint64_t ticket);
+int sbg_server_stats(sbg_server *srv, int64_t *pending, int64_t *completed, int64_t *batches,
+                     size_t *arena_used);
+/* Stops the scheduler (queued requests are dropped) and frees the arena. */
+void sbg_server_destroy(sbg_server *srv);
+
 /* ---- reference-signature drop-ins ---------------------------------------- */
 
 /* int nt_mul(uint64_t *rp, const uint64_t *ap, ptrdiff_t an,

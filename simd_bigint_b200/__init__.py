@@ -105,6 +105,19 @@ def lib(build_if_missing: bool = False):
         L.sbg_divrem_u64.argtypes = [_vp, _vp, _vp, C.c_uint64, _vp, C.c_uint64,
                                      C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.sbg_divrem_u64.restype = C.c_int
+        L.sbg_server_create.argtypes = [_vp, _vp, C.POINTER(_vp)]
+        L.sbg_server_create.restype = C.c_int
+        L.sbg_server_submit.argtypes = [_vp, _vp, C.POINTER(C.c_uint64)]
+        L.sbg_server_submit.restype = C.c_int
+        L.sbg_server_poll.argtypes = [_vp, _vp, C.c_int, C.POINTER(C.c_int), C.c_int]
+        L.sbg_server_poll.restype = C.c_int
+        L.sbg_server_release.argtypes = [_vp, C.c_uint64]
+        L.sbg_server_release.restype = C.c_int
+        L.sbg_server_stats.argtypes = [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                       C.POINTER(C.c_int64), C.POINTER(C.c_size_t)]
+        L.sbg_server_stats.restype = C.c_int
+        L.sbg_server_destroy.argtypes = [_vp]
+        L.sbg_server_destroy.restype = None
         _lib = L
     return _lib
 
@@ -275,6 +288,97 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+REQ_MUL, REQ_SQR, REQ_RECIP = 0, 1, 2
+
+
+class Request(C.Structure):
+    """sbg_request."""
+    _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("ap", C.c_void_p), ("an", C.c_int64),
+                ("bp", C.c_void_p), ("bn", C.c_int64)]
+
+
+class Completion(C.Structure):
+    """sbg_completion."""
+    _fields_ = [("ticket", C.c_uint64), ("status", C.c_int32), ("reserved", C.c_int32),
+                ("rp", C.c_void_p), ("rn", C.c_int64), ("latency_s", C.c_double)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("arena_bytes", C.c_size_t), ("slots", C.c_int32), ("max_batch", C.c_int32)]
+
+
+class Server:
+    """The serving loop (sbg_server_*): submit device-operand requests from
+    any thread, poll completions (device result pointer + latency), release."""
+
+    def __init__(self, ctx: Context, arena_bytes: int = 8 << 30, slots: int = 4, max_batch: int = 512):
+        self._L = lib()
+        self.ctx = ctx
+        cfg = ServerConfig(arena_bytes, slots, max_batch)
+        h = _vp()
+        _check(self._L.sbg_server_create(ctx.handle, C.byref(cfg), C.byref(h)), "sbg_server_create")
+        self.handle = h
+        self._buf = (Completion * 4096)()
+
+    def submit(self, kind: int, ap: int, an: int, bp: int = 0, bn: int = 0) -> int:
+        req = Request(kind, 0, ap, an, bp, bn)
+        t = C.c_uint64(0)
+        _check(self._L.sbg_server_submit(self.handle, C.byref(req), C.byref(t)), "sbg_server_submit")
+        return t.value
+
+    def try_submit(self, kind: int, ap: int, an: int, bp: int = 0, bn: int = 0) -> tuple[int, int]:
+        req = Request(kind, 0, ap, an, bp, bn)
+        t = C.c_uint64(0)
+        st = self._L.sbg_server_submit(self.handle, C.byref(req), C.byref(t))
+        return st, t.value
+
+    def poll(self, wait_ms: int = 0) -> list[tuple[int, int, int, int, float]]:
+        """[(ticket, status, result device pointer, result limbs, latency_s)]"""
+        n = C.c_int(0)
+        _check(self._L.sbg_server_poll(self.handle, C.cast(self._buf, _vp), 4096, C.byref(n), wait_ms),
+               "sbg_server_poll")
+        return [(c.ticket, c.status, c.rp or 0, c.rn, c.latency_s) for c in self._buf[: n.value]]
+
+    def result(self, rp: int, rn: int):
+        """torch.int64 view of a completed result in the server's arena; valid
+        until the ticket is released."""
+        return device_limbs(rp, rn)
+
+    def release(self, ticket: int):
+        _check(self._L.sbg_server_release(self.handle, ticket), "sbg_server_release")
+
+    def stats(self) -> dict:
+        p, c, b, u = C.c_int64(0), C.c_int64(0), C.c_int64(0), C.c_size_t(0)
+        _check(self._L.sbg_server_stats(self.handle, C.byref(p), C.byref(c), C.byref(b), C.byref(u)),
+               "sbg_server_stats")
+        return {"pending": p.value, "completed": c.value, "batches": b.value, "arena_used": u.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._L.sbg_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _DevArray:
+    """Minimal __cuda_array_interface__ holder for a raw device pointer."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i8", "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def device_limbs(ptr: int, n: int):
+    """torch.int64 CUDA tensor viewing n limbs at device address ptr (no copy)."""
+    import torch
+    return torch.as_tensor(_DevArray(ptr, n), device="cuda")
 
 
 def _np_u64(x) -> np.ndarray:

@@ -13,80 +13,8 @@
 
 using namespace sbg;
 
-// Per-launch CUDA event pairs, summed per kernel id by sbg_ctx_kernel_times.
-struct EventTimer : KTimer {
-    struct Rec {
-        int kid;
-        cudaEvent_t a, b;
-    };
-    std::vector<Rec> recs;
-    std::vector<cudaEvent_t> pool;
-    cudaEvent_t take() {
-        if (!pool.empty()) {
-            cudaEvent_t e = pool.back();
-            pool.pop_back();
-            return e;
-        }
-        cudaEvent_t e = nullptr;
-        cudaEventCreate(&e);
-        return e;
-    }
-    void begin(int kid, cudaStream_t st) override {
-        Rec r{kid, take(), nullptr};
-        cudaEventRecord(r.a, st);
-        recs.push_back(r);
-    }
-    void end(int kid, cudaStream_t st) override {
-        for (size_t i = recs.size(); i-- > 0;)
-            if (recs[i].kid == kid && recs[i].b == nullptr) {
-                recs[i].b = take();
-                cudaEventRecord(recs[i].b, st);
-                return;
-            }
-    }
-    void collect(double* ms, int64_t* cnt) {
-        for (auto& r : recs) {
-            if (r.b) {
-                float t = 0.f;
-                if (cudaEventSynchronize(r.b) == cudaSuccess &&
-                    cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
-                    ms[r.kid] += t;
-                    cnt[r.kid] += 1;
-                }
-                pool.push_back(r.b);
-            }
-            pool.push_back(r.a);
-        }
-        recs.clear();
-    }
-    ~EventTimer() override {
-        for (auto& r : recs) {
-            cudaEventDestroy(r.a);
-            if (r.b) cudaEventDestroy(r.b);
-        }
-        for (auto e : pool) cudaEventDestroy(e);
-    }
-};
-
-struct sbg_ctx {
-    int device = 0;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    uint2* tw_f = nullptr;          // master tables [q][2^12]
-    uint2* tw_i = nullptr;
-    LenPlan plans[SBG_MAX_LG + 1];
-    uint32_t* ws = nullptr;         // transform workspace (u32 words)
-    size_t ws_cap = 0;
-    uint32_t* flags = nullptr;      // carry look-back flags
-    size_t flags_cap = 0;
-    uint32_t* err = nullptr;        // sticky device error bits
-    // staging for the host-pointer drop-ins
-    uint64_t* d_stage = nullptr;
-    size_t stage_cap = 0;
-    EventTimer* timer = nullptr;    // non-null while kernel timing is on
-};
-
-static int cuda_fail(cudaError_t e, const char* where) {
+namespace sbg {
+int cuda_fail(cudaError_t e, const char* where) {
     if (e == cudaSuccess) return SBG_OK;
     if (getenv("SBG_DEBUG")) fprintf(stderr, "sbg: %s: %s\n", where, cudaGetErrorString(e));
     if (e == cudaErrorMemoryAllocation) return SBG_EALLOC;
@@ -99,19 +27,19 @@ static int cuda_fail(cudaError_t e, const char* where) {
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
 
-static int lg_ceil(int64_t n) {
+int lg_ceil(int64_t n) {
     int l = 0;
     while (((int64_t)1 << l) < n) ++l;
     return l;
 }
 
 // Transform length for a convolution whose wanted coefficients need L >= need.
-static int conv_lg(int64_t need) {
+int conv_lg(int64_t need) {
     int l = lg_ceil(need);
     return l < 4 ? 4 : l;
 }
 
-static int ensure_plan(sbg_ctx* c, int lgL) {
+int ensure_plan(sbg_ctx* c, int lgL) {
     LenPlan* lp = &c->plans[lgL];
     if (lp->lgL == lgL) return SBG_OK;
     LenPlan np;
@@ -135,6 +63,8 @@ static int ensure_plan(sbg_ctx* c, int lgL) {
     *lp = np;
     return SBG_OK;
 }
+
+}  // namespace sbg
 
 static int ensure_ws(sbg_ctx* c, size_t words, size_t flag_words) {
     if (words > c->ws_cap) {

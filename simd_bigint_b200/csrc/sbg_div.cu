@@ -533,28 +533,34 @@ static void carve(DivInst& d, uint64_t*& p) {
     d.Rw = p; p += n + 2;
 }
 
-extern "C" int sbg_recip(sbg_ctx* c, uint64_t* ip, const uint64_t* dp, int64_t n) {
-    if (!c || !ip || !dp || n <= 0) return SBG_EINVAL;
-    if (2 * n + 2 > ((int64_t)1 << 25)) return SBG_EBAND;
-    void* sp = sbg_ctx_get_stream(c);
-    (void)sp;
+int sbg::recip_batch(sbg_ctx* c, const uint64_t* const* D, uint64_t* const* V, const int64_t* n,
+                     int count) {
+    if (count <= 0) return SBG_OK;
+    size_t total = 0;
+    for (int i = 0; i < count; ++i) {
+        if (!D[i] || !V[i] || n[i] <= 0) return SBG_EINVAL;
+        if (2 * n[i] + 2 > ((int64_t)1 << 25)) return SBG_EBAND;
+        total += div_scratch_limbs(n[i]);
+    }
     uint64_t* scratch = nullptr;
     uint32_t* err = nullptr;
-    if (cudaMalloc(&scratch, div_scratch_limbs(n) * 8) != cudaSuccess) return SBG_EALLOC;
+    if (cudaMalloc(&scratch, total * 8) != cudaSuccess) return SBG_EALLOC;
     if (cudaMalloc(&err, 4) != cudaSuccess) {
         cudaFree(scratch);
         return SBG_EALLOC;
     }
-    cudaMemset(err, 0, 4);
-    std::vector<DivInst> v(1);
-    v[0].D = dp;
-    v[0].N = nullptr;
-    v[0].Qout = ip;
-    v[0].Rout = nullptr;
-    v[0].n = n;
-    v[0].qlen = n;
+    cudaMemsetAsync(err, 0, 4, (cudaStream_t)sbg_ctx_get_stream(c));
+    std::vector<DivInst> v((size_t)count);
     uint64_t* p = scratch;
-    carve(v[0], p);
+    for (int i = 0; i < count; ++i) {
+        v[i].D = D[i];
+        v[i].N = nullptr;
+        v[i].Qout = V[i];
+        v[i].Rout = nullptr;
+        v[i].n = n[i];
+        v[i].qlen = n[i];
+        carve(v[i], p);
+    }
     int rc = div_core(c, v, err, false);
     uint32_t h = 0;
     if (!rc) cudaMemcpy(&h, err, 4, cudaMemcpyDeviceToHost);
@@ -562,6 +568,11 @@ extern "C" int sbg_recip(sbg_ctx* c, uint64_t* ip, const uint64_t* dp, int64_t n
     cudaFree(err);
     if (rc) return rc;
     return h ? SBG_ECUDA : SBG_OK;
+}
+
+extern "C" int sbg_recip(sbg_ctx* c, uint64_t* ip, const uint64_t* dp, int64_t n) {
+    if (!c || !ip || !dp || n <= 0) return SBG_EINVAL;
+    return sbg::recip_batch(c, &dp, &ip, &n, 1);
 }
 
 // Batched division: every job has a normalised divisor (top bit set) and

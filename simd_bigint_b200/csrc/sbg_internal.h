@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cstddef>
 
+#include <vector>
+
 #include "sbg_arith.cuh"
 
 namespace sbg {
@@ -128,4 +130,92 @@ cudaError_t launch_batch_class(const JobDesc* djobs, int njobs, int lgL, const L
                                uint32_t* flags, size_t flag_words, uint32_t* err,
                                cudaStream_t st, KTimer* kt = nullptr);
 
+
+// ---- the context (C ABI opaque type), shared by the library's TUs ----
+// Per-launch CUDA event pairs, summed per kernel id by sbg_ctx_kernel_times.
+struct EventTimer : KTimer {
+    struct Rec {
+        int kid;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t take() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(int kid, cudaStream_t st) override {
+        Rec r{kid, take(), nullptr};
+        cudaEventRecord(r.a, st);
+        recs.push_back(r);
+    }
+    void end(int kid, cudaStream_t st) override {
+        for (size_t i = recs.size(); i-- > 0;)
+            if (recs[i].kid == kid && recs[i].b == nullptr) {
+                recs[i].b = take();
+                cudaEventRecord(recs[i].b, st);
+                return;
+            }
+    }
+    void collect(double* ms, int64_t* cnt) {
+        for (auto& r : recs) {
+            if (r.b) {
+                float t = 0.f;
+                if (cudaEventSynchronize(r.b) == cudaSuccess &&
+                    cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
+                    ms[r.kid] += t;
+                    cnt[r.kid] += 1;
+                }
+                pool.push_back(r.b);
+            }
+            pool.push_back(r.a);
+        }
+        recs.clear();
+    }
+    ~EventTimer() override {
+        for (auto& r : recs) {
+            cudaEventDestroy(r.a);
+            if (r.b) cudaEventDestroy(r.b);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
 }  // namespace sbg
+
+struct sbg_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    uint2* tw_f = nullptr;          // master tables [q][2^12]
+    uint2* tw_i = nullptr;
+    sbg::LenPlan plans[SBG_MAX_LG + 1];
+    uint32_t* ws = nullptr;         // transform workspace (u32 words)
+    size_t ws_cap = 0;
+    uint32_t* flags = nullptr;      // carry look-back flags
+    size_t flags_cap = 0;
+    uint32_t* err = nullptr;        // sticky device error bits
+    // staging for the host-pointer drop-ins
+    uint64_t* d_stage = nullptr;
+    size_t stage_cap = 0;
+    sbg::EventTimer* timer = nullptr;    // non-null while kernel timing is on
+};
+
+namespace sbg {
+int cuda_fail(cudaError_t e, const char* where);
+int lg_ceil(int64_t n);
+int conv_lg(int64_t need);
+int ensure_plan(sbg_ctx* c, int lgL);
+// Newton reciprocals of `count` normalised divisors (device pointers), all
+// recursion levels in lockstep; synchronous on the context stream.
+int recip_batch(sbg_ctx* c, const uint64_t* const* D, uint64_t* const* V, const int64_t* n,
+                int count);
+size_t div_scratch_limbs(int64_t n);
+}  // namespace sbg
+

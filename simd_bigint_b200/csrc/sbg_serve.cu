@@ -1,0 +1,483 @@
+// sbg_serve.cu -- the serving loop: continuous batching of mul / sqr /
+// reciprocal requests with admission by HBM footprint.
+//
+// Requests arrive through sbg_server_submit (any host thread) and wait in a
+// FIFO.  A scheduler thread owns S "slots" (CUDA streams).  Whenever a slot is
+// free it takes the pending multiply requests from the head of the FIFO while
+// their footprint -- transform workspace, carry flags, job descriptor and the
+// result buffer -- fits in the server's HBM arena (first-fit allocator over
+// one device allocation), groups them by transform length and launches the
+// batch engine's stages on the slot's stream.  Requests that arrive while
+// other batches run join the next batch of a free slot, so batches from
+// different arrivals overlap on the device; finished batches are retired as
+// soon as their completion event fires, which frees their workspace for the
+// next admissions.  Reciprocal requests are batched the same way by a second
+// thread running the Newton reciprocal (all divisors of a batch in lockstep)
+// on its own context and stream.  A request is complete when its result is
+// in device memory; its latency is measured from submission to the moment the
+// server observes the completion.  Results stay in the arena until the client
+// releases them.  There is no counterpart in the reference, which has no
+// serving layer; each result is the one sbg_mul / sbg_sqr / sbg_recip
+// compute for the same request alone.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/simd_bigint_b200.h"
+#include "sbg_internal.h"
+
+namespace sbg {
+
+static double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+// first-fit allocator over [0, size) in 256-byte units, coalescing on free
+class Arena {
+   public:
+    void init(size_t size) {
+        free_.clear();
+        size_ = size & ~(size_t)255;
+        free_[0] = size_;
+        used_ = 0;
+    }
+    bool alloc(size_t bytes, size_t* off) {
+        bytes = (bytes + 255) & ~(size_t)255;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= bytes) {
+                *off = it->first;
+                size_t rest = it->second - bytes;
+                size_t noff = it->first + bytes;
+                free_.erase(it);
+                if (rest) free_[noff] = rest;
+                used_ += bytes;
+                return true;
+            }
+        }
+        return false;
+    }
+    void release(size_t off, size_t bytes) {
+        bytes = (bytes + 255) & ~(size_t)255;
+        used_ -= bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    size_t size() const { return size_; }
+    size_t used() const { return used_; }
+
+   private:
+    std::map<size_t, size_t> free_;
+    size_t size_ = 0, used_ = 0;
+};
+
+struct SReq {
+    uint64_t ticket = 0;
+    sbg_request r{};
+    double t_arrive = 0.0;
+    // shape
+    int lgL = 0, sq = 0;
+    int64_t cmin = 0, cmax = 0, off = 0, nout = 0;
+    // arena blocks
+    size_t ws_off = 0, ws_bytes = 0;     // workspace (+ flags) or Newton scratch charge
+    size_t out_off = 0, out_bytes = 0;   // result
+};
+
+struct Slot {
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    bool busy = false;
+    std::vector<SReq> reqs;
+    size_t meta_off = 0, meta_bytes = 0;
+    JobDesc* staging = nullptr;          // pinned host copy of the descriptors (max_batch)
+    uint32_t* herr = nullptr;            // pinned copy of the batch's device error word
+};
+
+// device error bits (bit 0 look-back timeout, bit 1 carry spill) -> status
+static int err_status(uint32_t h) {
+    if (!h) return SBG_OK;
+    if (h & 1u) return SBG_ETIMEOUT;
+    if (h & 2u) return SBG_ESPILL;
+    return SBG_ECUDA;
+}
+
+}  // namespace sbg
+
+using namespace sbg;
+
+struct sbg_server {
+    sbg_ctx* ctx = nullptr;              // multiplies
+    sbg_ctx* rctx = nullptr;             // reciprocals (own stream and workspace)
+    sbg_server_config cfg{};
+    uint8_t* arena_base = nullptr;
+    Arena arena;
+    std::mutex mu;                       // guards queues, arena, completions
+    std::condition_variable cv_work, cv_done;
+    std::deque<SReq> pending_mul, pending_recip;
+    std::vector<Slot> slots;
+    std::deque<sbg_completion> done;
+    std::unordered_map<uint64_t, std::pair<size_t, size_t>> results;   // ticket -> out block
+    std::atomic<bool> stop{false};
+    std::thread sched, recip;
+    uint64_t next_ticket = 1;
+    int64_t n_done = 0, n_batches = 0;
+};
+
+static size_t flag_words_of(const SReq& q) { return (size_t)(crt_blocks(q.nout) + 1 + 3) / 4 * 4; }
+static size_t mul_ws_bytes(const SReq& q) { return ws_words(q.lgL, q.sq) * 4; }
+
+static void complete(sbg_server* s, const SReq& q, int status, double t) {
+    sbg_completion c{};
+    c.ticket = q.ticket;
+    c.status = status;
+    c.rp = status == SBG_OK ? (uint64_t*)(s->arena_base + q.out_off) : nullptr;
+    c.rn = q.nout;
+    c.latency_s = t - q.t_arrive;
+    if (status == SBG_OK)
+        s->results[q.ticket] = {q.out_off, q.out_bytes};
+    else
+        s->arena.release(q.out_off, q.out_bytes);
+    s->done.push_back(c);
+    s->n_done++;
+}
+
+// one batch of multiplies on a free slot (called with s->mu held)
+static int launch_slot(sbg_server* s, Slot& sl) {
+    sbg_ctx* c = s->ctx;
+    std::vector<SReq> take;
+    const size_t batch_cap = s->arena.size() / (size_t)std::max(1, s->cfg.slots);
+    size_t batch_bytes = 0;
+    while (!s->pending_mul.empty() && (int)take.size() < s->cfg.max_batch) {
+        SReq& q = s->pending_mul.front();
+        const size_t need = mul_ws_bytes(q) + q.out_bytes;
+        if (!take.empty() && batch_bytes + need > batch_cap) break;   // leave room for other slots
+        size_t wo, oo;
+        if (!s->arena.alloc(mul_ws_bytes(q), &wo)) break;             // FIFO: wait for memory
+        if (!s->arena.alloc(q.out_bytes, &oo)) {
+            s->arena.release(wo, mul_ws_bytes(q));
+            break;
+        }
+        q.ws_off = wo;
+        q.ws_bytes = mul_ws_bytes(q);
+        q.out_off = oo;
+        take.push_back(q);
+        batch_bytes += need;
+        s->pending_mul.pop_front();
+    }
+    if (take.empty()) return 0;
+    // descriptors grouped by length; the batch's carry flags follow them
+    std::stable_sort(take.begin(), take.end(), [](const SReq& a, const SReq& b) { return a.lgL < b.lgL; });
+    size_t nflags = 0;
+    for (auto& q : take) nflags += flag_words_of(q);
+    nflags += 4;                                     // the batch's error word (last)
+    const size_t meta = take.size() * sizeof(JobDesc) + 256 + nflags * 4;
+    size_t mo;
+    if (!s->arena.alloc(meta, &mo)) {
+        for (auto& q : take) {                       // give everything back, retry later
+            s->arena.release(q.ws_off, q.ws_bytes);
+            s->arena.release(q.out_off, q.out_bytes);
+        }
+        for (auto it = take.rbegin(); it != take.rend(); ++it) s->pending_mul.push_front(*it);
+        return 0;
+    }
+    // a failed enqueue fails the whole batch: wait for what was enqueued, free its memory
+    auto fail_batch = [&]() {
+        cudaStreamSynchronize(sl.st);
+        const double t = now_s();
+        for (auto& q : take) {
+            s->arena.release(q.ws_off, q.ws_bytes);
+            complete(s, q, SBG_ECUDA, t);
+        }
+        s->arena.release(mo, meta);
+        return -1;
+    };
+    uint32_t* flags = (uint32_t*)(s->arena_base + mo + ((take.size() * sizeof(JobDesc) + 255) & ~(size_t)255));
+    uint32_t* derr = flags + nflags - 4;
+    uint32_t* fcur = flags;
+    for (size_t i = 0; i < take.size(); ++i) {
+        const SReq& q = take[i];
+        JobDesc d{};
+        d.a = q.r.ap;
+        d.b = q.sq ? q.r.ap : q.r.bp;
+        d.out = (uint64_t*)(s->arena_base + q.out_off);
+        d.an = q.r.an;
+        d.bn = q.sq ? q.r.an : q.r.bn;
+        d.cmin = q.cmin;
+        d.cmax = q.cmax;
+        d.off = q.off;
+        d.nout = q.nout;
+        d.ws = (uint32_t*)(s->arena_base + q.ws_off);
+        d.flags = fcur;
+        fcur += flag_words_of(q);
+        d.sq = q.sq;
+        sl.staging[i] = d;
+    }
+    JobDesc* dd = (JobDesc*)(s->arena_base + mo);
+    if (cudaMemcpyAsync(dd, sl.staging, take.size() * sizeof(JobDesc), cudaMemcpyHostToDevice,
+                        sl.st) != cudaSuccess ||
+        cudaMemsetAsync(flags, 0, nflags * 4, sl.st) != cudaSuccess)
+        return fail_batch();
+    // one launch sequence per length class (flags already zeroed above)
+    size_t i = 0;
+    while (i < take.size()) {
+        size_t j = i;
+        int64_t max_nout = 0;
+        while (j < take.size() && take[j].lgL == take[i].lgL) {
+            max_nout = std::max(max_nout, take[j].nout);
+            ++j;
+        }
+        if (launch_batch_class(dd + i, (int)(j - i), take[i].lgL, &c->plans[take[i].lgL], c->tw_f,
+                               c->tw_i, max_nout, sl.staging[i].flags, 0, derr, sl.st) !=
+            cudaSuccess)
+            return fail_batch();
+        i = j;
+    }
+    if (cudaMemcpyAsync(sl.herr, derr, 4, cudaMemcpyDeviceToHost, sl.st) != cudaSuccess ||
+        cudaEventRecord(sl.done, sl.st) != cudaSuccess)
+        return fail_batch();
+    sl.reqs = std::move(take);
+    sl.meta_off = mo;
+    sl.meta_bytes = meta;
+    sl.busy = true;
+    s->n_batches++;
+    return 1;
+}
+
+static void sched_loop(sbg_server* s) {
+    cudaSetDevice(s->ctx->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (!s->stop) {
+        bool progress = false;
+        for (auto& sl : s->slots) {
+            if (!sl.busy) continue;
+            cudaError_t q = cudaEventQuery(sl.done);
+            if (q == cudaErrorNotReady) continue;
+            const double t = now_s();
+            const int status = q == cudaSuccess ? err_status(*sl.herr) : SBG_ECUDA;
+            for (auto& r : sl.reqs) {
+                s->arena.release(r.ws_off, r.ws_bytes);
+                complete(s, r, status, t);
+            }
+            s->arena.release(sl.meta_off, sl.meta_bytes);
+            sl.reqs.clear();
+            sl.busy = false;
+            progress = true;
+        }
+        if (progress) s->cv_done.notify_all();
+        for (auto& sl : s->slots) {
+            if (sl.busy || s->pending_mul.empty()) continue;
+            if (launch_slot(s, sl) != 0) progress = true;
+        }
+        bool any_busy = false;
+        for (auto& sl : s->slots) any_busy |= sl.busy;
+        if (!progress) {
+            if (any_busy)
+                s->cv_work.wait_for(lk, std::chrono::microseconds(20));
+            else
+                s->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+        }
+    }
+}
+
+static void recip_loop(sbg_server* s) {
+    cudaSetDevice(s->rctx->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (!s->stop) {
+        if (s->pending_recip.empty()) {
+            s->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+            continue;
+        }
+        std::vector<SReq> take;
+        while (!s->pending_recip.empty() && (int)take.size() < s->cfg.max_batch) {
+            SReq& q = s->pending_recip.front();
+            size_t wo, oo;
+            if (!s->arena.alloc(q.ws_bytes, &wo)) break;
+            if (!s->arena.alloc(q.out_bytes, &oo)) {
+                s->arena.release(wo, q.ws_bytes);
+                break;
+            }
+            q.ws_off = wo;
+            q.out_off = oo;
+            take.push_back(q);
+            s->pending_recip.pop_front();
+        }
+        if (take.empty()) {
+            s->cv_work.wait_for(lk, std::chrono::milliseconds(1));
+            continue;
+        }
+        std::vector<const uint64_t*> D;
+        std::vector<uint64_t*> V;
+        std::vector<int64_t> n;
+        for (auto& q : take) {
+            D.push_back(q.r.ap);
+            V.push_back((uint64_t*)(s->arena_base + q.out_off));
+            n.push_back(q.r.an);
+        }
+        lk.unlock();
+        int st = recip_batch(s->rctx, D.data(), V.data(), n.data(), (int)take.size());
+        lk.lock();
+        const double t = now_s();
+        for (auto& q : take) {
+            s->arena.release(q.ws_off, q.ws_bytes);
+            complete(s, q, st, t);
+        }
+        s->n_batches++;
+        s->cv_done.notify_all();
+    }
+}
+
+extern "C" int sbg_server_create(sbg_ctx* ctx, const sbg_server_config* cfg, sbg_server** out) {
+    if (!ctx || !out) return SBG_EINVAL;
+    *out = nullptr;
+    sbg_server* s = new sbg_server();
+    s->ctx = ctx;
+    s->cfg.arena_bytes = cfg && cfg->arena_bytes ? cfg->arena_bytes : ((size_t)8 << 30);
+    s->cfg.slots = cfg && cfg->slots > 0 ? cfg->slots : 4;
+    s->cfg.max_batch = cfg && cfg->max_batch > 0 ? cfg->max_batch : 512;
+    int st = SBG_OK;
+    do {
+        if ((st = cuda_fail(cudaSetDevice(ctx->device), "device"))) break;
+        for (int l = 4; l <= 22 && !st; ++l) st = ensure_plan(ctx, l);   // tables to 2^22 points
+        if (st) break;
+        if ((st = sbg_ctx_create(ctx->device, &s->rctx))) break;
+        if ((st = cuda_fail(cudaMalloc(&s->arena_base, s->cfg.arena_bytes), "arena"))) break;
+        s->arena.init(s->cfg.arena_bytes);
+        s->slots.resize((size_t)s->cfg.slots);
+        for (auto& sl : s->slots) {
+            if ((st = cuda_fail(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking), "slot")))
+                break;
+            if ((st = cuda_fail(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "ev")))
+                break;
+            if ((st = cuda_fail(cudaHostAlloc(&sl.herr, 4, 0), "herr"))) break;
+            if ((st = cuda_fail(cudaHostAlloc(&sl.staging, (size_t)s->cfg.max_batch * sizeof(JobDesc), 0),
+                                "staging")))
+                break;
+            *sl.herr = 0;
+        }
+    } while (0);
+    if (st) {
+        sbg_server_destroy(s);
+        return st;
+    }
+    s->sched = std::thread(sched_loop, s);
+    s->recip = std::thread(recip_loop, s);
+    *out = s;
+    return SBG_OK;
+}
+
+extern "C" void sbg_server_destroy(sbg_server* s) {
+    if (!s) return;
+    s->stop = true;
+    s->cv_work.notify_all();
+    if (s->sched.joinable()) s->sched.join();
+    if (s->recip.joinable()) s->recip.join();
+    if (s->ctx) cudaSetDevice(s->ctx->device);
+    for (auto& sl : s->slots) {
+        if (sl.st) cudaStreamSynchronize(sl.st);
+        if (sl.st) cudaStreamDestroy(sl.st);
+        if (sl.done) cudaEventDestroy(sl.done);
+        cudaFreeHost(sl.staging);
+        cudaFreeHost(sl.herr);
+    }
+    cudaFree(s->arena_base);
+    if (s->rctx) sbg_ctx_destroy(s->rctx);
+    delete s;
+}
+
+extern "C" int sbg_server_submit(sbg_server* s, const sbg_request* req, uint64_t* ticket) {
+    if (!s || !req || !req->ap || req->an <= 0) return SBG_EINVAL;
+    SReq q;
+    q.r = *req;
+    q.t_arrive = now_s();
+    if (req->kind == SBG_REQ_RECIP) {
+        q.nout = req->an;
+        q.ws_bytes = div_scratch_limbs(req->an) * 8;
+        q.out_bytes = (size_t)req->an * 8;
+        if (2 * req->an + 2 > ((int64_t)1 << 25)) return SBG_EBAND;
+    } else {
+        if (req->kind != SBG_REQ_MUL && req->kind != SBG_REQ_SQR) return SBG_EINVAL;
+        if (req->kind == SBG_REQ_MUL && (!req->bp || req->bn <= 0)) return SBG_EINVAL;
+        int64_t need = req->kind == SBG_REQ_SQR ? 2 * req->an - 1 : req->an + req->bn - 1;
+        if (need > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
+        q.lgL = conv_lg(need);
+        q.sq = req->kind == SBG_REQ_SQR;
+        q.cmin = 0;
+        q.cmax = need - 1;
+        q.off = 0;
+        q.nout = need + 1;
+        q.out_bytes = (size_t)q.nout * 8;
+        q.ws_bytes = mul_ws_bytes(q);
+    }
+    if (q.ws_bytes + q.out_bytes + 4096 > s->arena.size()) return SBG_EADMIT;   // can never fit
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        if (q.lgL > 0 && s->ctx->plans[q.lgL].lgL != q.lgL) {
+            int st = ensure_plan(s->ctx, q.lgL);
+            if (st) return st;
+        }
+        q.ticket = s->next_ticket++;
+        if (req->kind == SBG_REQ_RECIP)
+            s->pending_recip.push_back(q);
+        else
+            s->pending_mul.push_back(q);
+    }
+    s->cv_work.notify_all();
+    if (ticket) *ticket = q.ticket;
+    return SBG_OK;
+}
+
+extern "C" int sbg_server_poll(sbg_server* s, sbg_completion* out, int max, int* n, int wait_ms) {
+    if (!s || !out || !n || max <= 0) return SBG_EINVAL;
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->done.empty() && wait_ms > 0)
+        s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return !s->done.empty(); });
+    int k = 0;
+    while (k < max && !s->done.empty()) {
+        out[k++] = s->done.front();
+        s->done.pop_front();
+    }
+    *n = k;
+    return SBG_OK;
+}
+
+extern "C" int sbg_server_release(sbg_server* s, uint64_t ticket) {
+    if (!s) return SBG_EINVAL;
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->results.find(ticket);
+    if (it == s->results.end()) return SBG_EINVAL;
+    s->arena.release(it->second.first, it->second.second);
+    s->results.erase(it);
+    s->cv_work.notify_all();
+    return SBG_OK;
+}
+
+extern "C" int sbg_server_stats(sbg_server* s, int64_t* pending, int64_t* completed,
+                                int64_t* batches, size_t* arena_used) {
+    if (!s) return SBG_EINVAL;
+    std::lock_guard<std::mutex> g(s->mu);
+    if (pending) *pending = (int64_t)(s->pending_mul.size() + s->pending_recip.size());
+    if (completed) *completed = s->n_done;
+    if (batches) *batches = s->n_batches;
+    if (arena_used) *arena_used = s->arena.used();
+    return SBG_OK;
+}

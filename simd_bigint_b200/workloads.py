@@ -42,3 +42,31 @@ def fill_limbs(n: int, rng: np.random.Generator, top_bit: bool = False) -> np.nd
         elif x[-1] == 0:
             x[-1] = np.uint64(1)
     return x
+
+
+def serving_requests(count: int, seed: int = 2025, lo: int = 32, hi: int = 1 << 20,
+                     balanced: float = 0.7, rmax: float = 16.0,
+                     mix: tuple[float, float, float] = (0.5, 0.3, 0.2)) -> list[tuple[int, int, int]]:
+    """The serving configuration's request stream: (kind, an, bn) with an
+    log-uniform in [lo, hi], 70% balanced (bn = an) and 30% unbalanced
+    (bn = an / r, r log-uniform in (1, rmax]); kind 0 mul, 1 sqr, 2 reciprocal
+    of an an-limb divisor, drawn with probabilities `mix`."""
+    rng = np.random.default_rng(seed)
+    out = []
+    cdf = np.cumsum(mix)
+    for _ in range(count):
+        an = int(math.exp(rng.uniform(math.log(lo), math.log(hi))))
+        u = rng.uniform()
+        kind = 0 if u < cdf[0] else (1 if u < cdf[1] else 2)
+        if kind == 0:
+            bn = an if rng.uniform() < balanced else max(1, int(an / math.exp(rng.uniform(0, math.log(rmax)))))
+        else:
+            bn = an
+        out.append((kind, an, bn))
+    return out
+
+
+def poisson_arrivals(count: int, rate: float, seed: int = 7) -> np.ndarray:
+    """Arrival times (seconds from 0) of a Poisson stream of `rate` per second."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=count))
