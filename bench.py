@@ -2,17 +2,23 @@
 """Benchmark of the large-operand multiply path (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mul2p24|sqr2p24|mul2p22|mul2p24x2p20|mul16k]
+                    [--workload mul2p24|sqr2p24|mul2p22|mul2p24x2p20|mul16k|batch4096|div1024|serve]
 
-A step is one product of the workload on one GPU (replicas across ranks: the
-path shards by instance, with no collective).  `value` is product limbs
-(an + bn) per second over all ranks with operands resident in HBM, timed with
-CUDA events on the library's stream; `e2e` is the same through the
-reference-signature C entry (sbg_nt_mul) on pinned HOST buffers, copies in
-and out inside the timed region.  The roofline names the dominant kernel,
-its algorithmic bytes and butterflies per launch divided by its average
-CUDA-event duration.  `cpu_baseline` times the reference's own nt_mul
-(compiled from its sources into oracle/_ref) on the host cores.
+Default (mul2p24): a step is one 2^24 x 2^24-limb product on one GPU
+(replicas across ranks: the path shards by instance, with no collective).
+`value` is product limbs (an + bn) per second over all ranks with operands
+resident in HBM, timed with CUDA events on the library's stream; `e2e` is the
+same through the reference-signature C entry (sbg_nt_mul) on pinned HOST
+buffers, copies in and out inside the timed region.  The roofline names the
+dominant kernel, its algorithmic bytes and butterflies per launch divided by
+its average CUDA-event duration.  `cpu_baseline` times the reference's own
+nt_mul (compiled from its sources into oracle/_ref) on the host cores.
+
+Other workloads: batch4096 (4096 mixed-size products as one captured batch),
+div1024 (1024 batched Newton divisions), serve (the serving loop: a 200k
+request stream at saturation, then a Poisson arrival-rate sweep with p50/p99
+latency).  Every timed result is spot-checked (products modulo 2^61-1 and
+2^64-1; divisions as Q D + R = N with R < D; small reciprocals exactly).
 """
 from __future__ import annotations
 
@@ -40,6 +46,7 @@ WORKLOADS = {
     "mul16k": ("mul", 16384, 16384),
     "batch4096": ("batch", 4096, 0),     # the batched mixed-size configuration
     "div1024": ("div", 1024, 0),         # the batched Newton division configuration
+    "serve": ("serve", 0, 0),            # the serving-loop configuration
 }
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
@@ -158,6 +165,36 @@ def barrier_max(pg, value: float, device) -> float:
     t = torch.tensor([value], dtype=torch.float64, device=device)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+M61 = (1 << 61) - 1
+M64 = (1 << 64) - 1
+
+
+def residues(a: np.ndarray) -> tuple[int, int]:
+    """(A mod 2^61-1, A mod 2^64-1) of a little-endian u64 limb array, in
+    numpy: 2^64 = 8 (mod 2^61-1), so limb i weighs 2^(3i mod 61), a 61-bit
+    rotation; 2^64 = 1 (mod 2^64-1), so A is the plain limb sum there.  Used
+    to spot-check timed products (A B = R in both rings)."""
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    if a.size == 0:
+        return 0, 0
+    m = np.uint64(M61)
+    x = (a & m) + (a >> np.uint64(61))
+    x = np.where(x >= m, x - m, x)
+    k = ((np.arange(a.size, dtype=np.uint64) * np.uint64(3)) % np.uint64(61))
+    rot = ((x << k) & m) | (x >> (np.uint64(61) - k))
+    lo32 = np.uint64(0xFFFFFFFF)
+    r61 = (int(np.sum(rot & lo32, dtype=np.uint64)) + (int(np.sum(rot >> np.uint64(32), dtype=np.uint64)) << 32)) % M61
+    r64 = (int(np.sum(a & lo32, dtype=np.uint64)) + (int(np.sum(a >> np.uint64(32), dtype=np.uint64)) << 32)) % M64
+    return r61, r64
+
+
+def product_ok(a: np.ndarray, b: np.ndarray, r: np.ndarray) -> bool:
+    """A B == R modulo 2^61-1 and 2^64-1, and in the lowest limb."""
+    (a1, a2), (b1, b2), (r1, r2) = residues(a), residues(b), residues(r)
+    low = (int(a[0]) * int(b[0])) & M64 == int(r[0]) if len(a) and len(b) and len(r) else True
+    return (a1 * b1) % M61 == r1 and (a2 * b2) % M64 == r2 and low
 
 
 def make_inputs(an: int, bn: int, seed: int):
@@ -377,14 +414,12 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
         batch.run()
     ctx.sync()
     # bit-exactness of the timed products: every job through the modular spot check
-    from oracle import oracle as O
     got = d_out.cpu().numpy().view(np.uint64)
-    q = 2305843009213693951
     exact = True
     for (kind, an, bn), ao, bo, ro in zip(shapes, a_off, b_off, r_off):
         a = host_in[ao:ao + an]
         b = a if kind == sbg.JOB_SQR else host_in[bo:bo + bn]
-        if (O.mod_u64(a, q) * O.mod_u64(b, q)) % q != O.mod_u64(got[ro:ro + an + bn], q):
+        if not product_ok(a, b, got[ro:ro + an + bn]):
             exact = False
             break
     if pg is not None:
@@ -533,7 +568,6 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
     import torch
 
     import simd_bigint_b200 as sbg
-    from oracle import oracle as O
     from simd_bigint_b200.workloads import division_shapes, fill_limbs
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -556,16 +590,14 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
     warm = max(1, min(args.warmup, 2))
     for _ in range(warm):
         ctx.divrem_batch(jobs)
-    # Q D + R == N and R < D for every division (modular check with two
-    # 61-bit primes plus an exact compare)
-    qs = (2305843009213693951, 2305843009213693921)
+    # Q D + R == N (modulo 2^61-1 and 2^64-1) and R < D for every division
     exact = True
     for N, D, q, r in zip(hostN, hostD, tQ, tR):
         Q = q.cpu().numpy().view(np.uint64)
         R = r.cpu().numpy().view(np.uint64)
-        for p in qs:
-            if (O.mod_u64(Q, p) * O.mod_u64(D, p) + O.mod_u64(R, p)) % p != O.mod_u64(N, p):
-                exact = False
+        (q1, q2), (d1, d2), (r1, r2), (n1, n2) = residues(Q), residues(D), residues(R), residues(N)
+        if (q1 * d1 + r1) % M61 != n1 or (q2 * d2 + r2) % M64 != n2:
+            exact = False
         hi = np.nonzero(R != D)[0]
         if len(hi) == 0 or R[hi[-1]] > D[hi[-1]]:
             exact = False
@@ -599,6 +631,276 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
     return res
 
 
+# ------------------------------------------------------- serving workload --
+SERVE_POOL = 1 << 25          # operand pool resident on the device: 2^25 random limbs (256 MB)
+SERVE_FRACS = (0.3, 0.6, 0.8, 0.95)
+
+
+def serve_out_limbs(kind: int, an: int, bn: int) -> int:
+    return an + bn if kind == 0 else (2 * an if kind == 1 else an)
+
+
+def serve_operands(reqs, pool: np.ndarray, seed: int) -> list[tuple[int, int, int, int, int]]:
+    """(kind, a_off, an, b_off, bn) into the pool for each request; a
+    reciprocal's divisor ends on a limb whose top bit is set (normalised)."""
+    rng = np.random.default_rng(seed)
+    P = len(pool)
+    top = np.nonzero(pool >> np.uint64(63))[0]
+    out = []
+    for kind, an, bn in reqs:
+        if kind == 2:
+            lo = int(np.searchsorted(top, an - 1))
+            ao = int(top[int(rng.integers(lo, len(top)))]) - an + 1
+        else:
+            ao = int(rng.integers(0, P - an + 1))
+        bo = int(rng.integers(0, P - bn + 1))
+        out.append((kind, ao, an, bo, bn))
+    return out
+
+
+def serve_drive(srv, ops, base: int, arrivals, check_every: int, limit_s: float = 900.0) -> dict:
+    """Open-loop client: submits ops at their arrival times (all at once when
+    arrivals is None) from a thread, polls and releases completions on this
+    one, copies every check_every-th result to the host for verification."""
+    import threading
+    n = len(ops)
+    idx = {}
+    lock = threading.Lock()
+    sub_t = [0.0, 0.0]
+    failed = []
+
+    def submitter():
+        try:
+            t0 = time.perf_counter()
+            sub_t[0] = t0
+            for i, (kind, ao, an, bo, bn) in enumerate(ops):
+                if arrivals is not None:
+                    d = t0 + arrivals[i] - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                t = srv.submit(kind, base + 8 * ao, an, base + 8 * bo, bn)
+                with lock:
+                    idx[t] = i
+            sub_t[1] = time.perf_counter()
+        except Exception as e:  # reported by the poller
+            failed.append(repr(e))
+
+    lat = np.zeros(n)
+    samples = []
+    got = 0
+    th = threading.Thread(target=submitter)
+    t_start = time.perf_counter()
+    th.start()
+    while got < n:
+        if failed:
+            raise RuntimeError("submit failed: " + failed[0])
+        if time.perf_counter() - t_start > limit_s:
+            raise RuntimeError(f"serving run exceeded {limit_s:.0f}s ({got}/{n} done)")
+        for ticket, status, rp, rn, l in srv.poll(wait_ms=20):
+            if status:
+                raise RuntimeError(f"request failed with status {status}")
+            while True:
+                with lock:
+                    i = idx.get(ticket)
+                if i is not None:
+                    break
+                time.sleep(0.0001)
+            lat[i] = l
+            if check_every and i % check_every == 0:
+                samples.append((i, srv.result(rp, rn).cpu().numpy().view(np.uint64).copy()))
+            srv.release(ticket)
+            got += 1
+    t_end = time.perf_counter()
+    th.join()
+    return {"lat": lat, "samples": samples, "wall_s": t_end - t_start,
+            "submit_s": sub_t[1] - sub_t[0]}
+
+
+def serve_check(samples, ops, pool: np.ndarray) -> tuple[bool, int, int]:
+    """Products by the residue check; reciprocals up to 4096 limbs exactly
+    (D (B^n + I) <= B^2n - 1 < D (B^n + I + 1))."""
+    ok, checked, skipped = True, 0, 0
+    for i, r in samples:
+        kind, ao, an, bo, bn = ops[i]
+        a = pool[ao:ao + an]
+        if kind == 2:
+            if an > 4096:
+                skipped += 1
+                continue
+            D = int.from_bytes(a.tobytes(), "little")
+            X = (1 << (64 * an)) + int.from_bytes(r.tobytes(), "little")
+            ok &= D * X <= (1 << (128 * an)) - 1 < D * (X + 1)
+        else:
+            ok &= product_ok(a, a if kind == 1 else pool[bo:bo + bn], r)
+        checked += 1
+    return bool(ok), checked, skipped
+
+
+def _pct(x, q):
+    return round(float(np.percentile(x, q)) * 1e3, 3) if len(x) else None
+
+
+def run_serve(args, ws, rank, local, pg) -> dict | None:
+    import torch
+
+    import simd_bigint_b200 as sbg
+    from simd_bigint_b200.workloads import poisson_arrivals, serving_requests
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n_main = args.requests
+    n_sweep = args.sweep_requests
+    pool = np.random.default_rng(55 + rank).integers(0, 2**64, SERVE_POOL, dtype=np.uint64)
+    dpool = torch.from_numpy(pool.view(np.int64)).to(dev)
+    base = dpool.data_ptr()
+    reqs = serving_requests(n_main, seed=2025)
+    ops = serve_operands(reqs, pool, seed=77 + rank)
+    limbs = sum(serve_out_limbs(k, an, bn) for k, an, bn in reqs)
+    ctx = sbg.Context(local)
+    srv = sbg.Server(ctx, arena_bytes=args.arena_gb << 30, slots=4, max_batch=256)
+    clocks = ClockSampler(local)
+    if rank == 0:
+        clocks.start()
+    # warm-up: every length class and the reciprocal path once
+    warm = serving_requests(max(64, args.warmup * 32), seed=9)
+    serve_drive(srv, serve_operands(warm, pool, seed=5), base, None, 0)
+    if pg is not None:
+        pg.barrier()
+    l0 = srv.launches()
+    clocks.mark("timed")
+    sat = serve_drive(srv, ops, base, None, 997)
+    launches = srv.launches() - l0
+    wall = barrier_max(pg, sat["wall_s"], dev)
+    capacity = n_main / sat["wall_s"]
+    exact, checked, skipped = serve_check(sat["samples"], ops, pool)
+    kinds = np.array([k for k, _, _ in reqs])
+    sweep = []
+    sreqs = serving_requests(n_sweep, seed=2026)
+    sops = serve_operands(sreqs, pool, seed=78 + rank)
+    slimbs = sum(serve_out_limbs(k, an, bn) for k, an, bn in sreqs)
+    skinds = np.array([k for k, _, _ in sreqs])
+    for j, f in enumerate(SERVE_FRACS if n_sweep else ()):
+        # offered load: fraction f of the measured capacity, in requests of this stream
+        rate = f * capacity * (limbs / n_main) / (slimbs / n_sweep)
+        arr = poisson_arrivals(n_sweep, rate, seed=300 + j)
+        r = serve_drive(srv, sops, base, arr, 499)
+        e2, c2, s2 = serve_check(r["samples"], sops, pool)
+        exact &= e2
+        checked += c2
+        skipped += s2
+        lat = r["lat"]
+        sweep.append({"offered_req_s": round(rate, 1), "achieved_req_s": round(n_sweep / r["wall_s"], 1),
+                      "submit_req_s": round(n_sweep / max(r["submit_s"], 1e-9), 1),
+                      "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99),
+                      "by_kind": {nm: {"p50_ms": _pct(lat[skinds == k], 50), "p99_ms": _pct(lat[skinds == k], 99)}
+                                  for k, nm in ((0, "mul"), (1, "sqr"), (2, "recip"))}})
+    clk = clocks.stop() if rank == 0 else None
+    st = srv.stats()
+    srv.close()
+    ctx.close()
+    if rank != 0:
+        return None
+    lat = sat["lat"]
+    return {
+        "metric": "served requests/s", "value": round(capacity * ws, 1), "unit": "req/s", "n_gpus": ws,
+        "steps": 1, "warmup": 1, "ms_per_step": round(wall * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic: seeded uniform u64 limbs from a 2^25-limb device pool, divisors top bit set",
+        "config": {"workload": f"serving: {n_main} mul/sqr/reciprocal requests (50/30/20%), sizes log-uniform "
+                               "[32, 2^20] limbs, 70% balanced / 30% unbalanced (ratio up to 16), seed 2025; "
+                               "all submitted at once (saturation), then a Poisson arrival-rate sweep of "
+                               f"{n_sweep} requests at {list(SERVE_FRACS)} of that capacity",
+                   "requests": n_main, "parallelism": f"replicas x{ws}",
+                   "server": {"arena_gb": args.arena_gb, "slots": 4, "max_batch": 256},
+                   "l2": "operand pool and results exceed L2; no flush"},
+        "bit_exact": exact, "checked_results": checked, "recip_unchecked_large": skipped,
+        "served_mlimb_s": round(limbs * ws / wall / 1e6, 1),
+        "saturation": {"wall_s": round(wall, 3), "submit_s": round(sat["submit_s"], 3),
+                       "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99),
+                       "by_kind": {nm: {"p50_ms": _pct(lat[kinds == k], 50), "p99_ms": _pct(lat[kinds == k], 99)}
+                                   for k, nm in ((0, "mul"), (1, "sqr"), (2, "recip"))}},
+        "sweep": sweep, "server_stats": st,
+        "e2e": None, "gpu_launches": int(launches), "roofline": None, "clocks": clk,
+    }
+
+
+def _serve_worker(reqs, seed, steps, warmup, barrier, queue):
+    """One baseline process: its share of the request stream through the
+    reference (mul/sqr by its size router, reciprocals as divrem_u64_dc of
+    B^2n - 1 by D)."""
+    try:
+        from oracle import oracle as O
+        use_ref = O.ref_available()
+        rng = np.random.default_rng(seed)
+        jobs = []
+        for kind, an, bn in reqs:
+            a = rng.integers(0, 2**64, an, dtype=np.uint64)
+            if kind == 2:
+                a[-1] |= np.uint64(1 << 63)
+                jobs.append((kind, a, np.full(2 * an, 2**64 - 1, dtype=np.uint64), None))
+            else:
+                b = rng.integers(0, 2**64, bn, dtype=np.uint64) if kind == 0 else a
+                jobs.append((kind, a, b, np.zeros(an + bn + 2, dtype=np.uint64)))
+
+        def run():
+            for kind, a, b, r in jobs:
+                if kind == 2:
+                    if use_ref:
+                        O.ref_divrem(b, a)
+                    else:
+                        O.port_recip(a)
+                elif use_ref:
+                    O.ref().sbref_mul_router(kind, O._ptr(r), O._ptr(a), len(a), O._ptr(b), len(b))
+                else:
+                    O.port_sqr(a) if kind == 1 else O.port_mul(a, b)
+
+        for _ in range(max(1, warmup)):
+            run()
+        times = []
+        for _ in range(steps):
+            barrier.wait(timeout=3600)
+            t = time.perf_counter()
+            run()
+            times.append(time.perf_counter() - t)
+        queue.put(("ok", 0.0, times))
+    except Exception as e:
+        try:
+            barrier.abort()
+        except Exception:
+            pass
+        queue.put(("err", repr(e), []))
+
+
+def cpu_run_serve(count: int, procs: int, steps: int = 1, warmup: int = 1) -> dict:
+    """The first `count` requests of the serving stream, dealt round-robin to
+    `procs` spawned single-threaded processes; requests/s = count / slowest."""
+    import multiprocessing as mp
+
+    from oracle import oracle as O
+    from simd_bigint_b200.workloads import serving_requests
+    reqs = serving_requests(count, seed=2025)
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs)
+    queue = ctx.Queue()
+    ps = [ctx.Process(target=_serve_worker, args=(reqs[i::procs], 31 + i, steps, warmup, barrier, queue))
+          for i in range(procs)]
+    for p in ps:
+        p.start()
+    res = [queue.get(timeout=7200) for _ in ps]
+    for p in ps:
+        p.join(timeout=60)
+    errs = [r[1] for r in res if r[0] != "ok"]
+    if errs:
+        raise RuntimeError("CPU baseline failed: " + errs[0])
+    step = statistics.median([max(r[2][k] for r in res) for k in range(steps)])
+    cpu = O.host_cpu()
+    return {"value": count / step, "unit": "req/s", "cores": procs,
+            "kind": "reference" if O.ref_available() else "port", "step_s": step,
+            "sample": f"first {count} requests of the serving stream (seed 2025) on {procs} single-threaded "
+                      f"processes, round-robin; {warmup} untimed pass first; no queueing (throughput only)",
+            "cpu_model": cpu["model"], "host_cores": cpu["cores"],
+            "isa": [f for f in O.REF_ISA if f in cpu["flags"]]}
+
+
 # ------------------------------------------------------------- our arm -----
 def run_ours(args, ws, rank, local, pg) -> dict | None:
     import torch
@@ -629,11 +931,8 @@ def run_ours(args, ws, rank, local, pg) -> dict | None:
         step()
     ctx.sync()
     # bit-exactness of what is timed: spot check of the warm-up product
-    from oracle import oracle as O
     got = tr.cpu().numpy().view(np.uint64)
-    qs = [2305843009213693951, 2305843009213693921]
-    bb = a if op == "sqr" else b
-    exact = all((O.mod_u64(a, q) * O.mod_u64(bb, q)) % q == O.mod_u64(got, q) for q in qs)
+    exact = product_ok(a, a if op == "sqr" else b, got)
 
     # ---- device-timed region (operands resident in HBM) ----
     if pg is not None:
@@ -739,6 +1038,43 @@ def run_ours(args, ws, rank, local, pg) -> dict | None:
     return result
 
 
+def reference_line(args, op: str, an: int, bn: int) -> dict:
+    """The reference arm: the reference's own CPU code on a bounded sample of
+    the same workload, reported in the same metric, unit and config as ours."""
+    steps = max(1, min(args.steps, 3))
+    if op == "batch":
+        from simd_bigint_b200.workloads import mixed_batch_shapes
+        r = cpu_run_batch(mixed_batch_shapes(4096, seed=12345), cpu_threads_for(1 << 16, 1 << 16), steps, 1)
+        metric, unit = "product Mlimb/s (batched)", "Mlimb/s"
+        cfg = {"workload": "4096 independent products, an log-uniform [64, 65536], bn = an/r, "
+                           "r log-uniform [1, 8], 20% squarings (seed 12345); one captured batch per step"}
+    elif op == "div":
+        from simd_bigint_b200.workloads import division_shapes
+        steps = 1
+        r = cpu_run_div(division_shapes(1024, seed=4242), cpu_threads_for(1 << 18, 1 << 18), steps, 0)
+        metric, unit = "numerator Mlimb/s (batched Newton divrem)", "Mlimb/s"
+        cfg = {"workload": "1024 divisions of 2n by n limbs, n log-uniform [512, 262144] (seed 4242); "
+                           "Newton reciprocal + quotient, all divisions in lockstep"}
+    elif op == "serve":
+        steps = 1
+        r = cpu_run_serve(args.cpu_requests, cpu_threads_for(1 << 20, 1 << 20), steps)
+        metric, unit = "served requests/s", "req/s"
+        cfg = {"workload": "serving stream (seed 2025): mul/sqr/reciprocal 50/30/20%, sizes log-uniform "
+                           "[32, 2^20] limbs; CPU throughput on a bounded prefix"}
+    else:
+        r = cpu_run(op, an, bn, cpu_threads_for(an, bn), steps=steps, warmup=1)
+        metric, unit = "product Mlimb/s", "Mlimb/s"
+        cfg = {"workload": f"{op} {an} x {bn} limbs, one product per step per GPU", "an": an, "bn": bn}
+    cfg["parallelism"] = f"{r['cores']} host processes"
+    return {"metric": metric, "value": round(r["value"], 3), "unit": unit,
+            "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": round(r["step_s"] * 1e3, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: seeded uniform u64 limbs", "config": cfg, "impl": "reference",
+            "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample", "cpu_model", "isa")},
+            "e2e": {"value": round(r["value"], 3), "unit": unit, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -747,6 +1083,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="mul2p24")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--requests", type=int, default=200000, help="serve: requests at saturation")
+    ap.add_argument("--sweep-requests", type=int, default=20000, help="serve: requests per sweep point")
+    ap.add_argument("--arena-gb", type=int, default=16, help="serve: server arena (GiB)")
+    ap.add_argument("--cpu-requests", type=int, default=640, help="serve: CPU baseline sample")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local, pg = (1, 0, 0, None)
@@ -756,30 +1096,7 @@ def main():
         # the reference is CPU code: rank 0 alone runs it, on all host threads
         if int(os.environ.get("RANK", "0")) != 0:
             return
-        threads = cpu_threads_for(an, bn) if op != "batch" else cpu_threads_for(1 << 16, 1 << 16)
-        # bounded sample: one product per thread per step, few steps
-        steps = max(1, min(args.steps, 3))
-        if op == "batch":
-            from simd_bigint_b200.workloads import mixed_batch_shapes
-            r = cpu_run_batch(mixed_batch_shapes(4096, seed=12345), threads, steps, 1)
-            an, bn = 4096, 0
-        elif op == "div":
-            from simd_bigint_b200.workloads import division_shapes
-            r = cpu_run_div(division_shapes(1024, seed=4242), threads, steps, 0)
-            an, bn = 1024, 0
-        else:
-            r = cpu_run(op, an, bn, threads, steps=steps, warmup=1)
-        out = {"metric": "product Mlimb/s", "value": round(r["value"], 3), "unit": "Mlimb/s",
-               "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": round(r["step_s"] * 1e3, 1),
-               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
-               "data": "synthetic: seeded uniform u64 limbs, top limb nonzero",
-               "config": {"workload": f"{op} {an} x {bn} limbs, one product per step per thread",
-                          "an": an, "bn": bn, "parallelism": f"{threads} host threads"},
-               "impl": "reference",
-               "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample", "cpu_model", "isa")},
-               "e2e": {"value": round(r["value"], 3), "unit": "Mlimb/s", "h2d_bytes_per_step": 0,
-                       "d2h_bytes_per_step": 0}}
-        print(json.dumps(out), flush=True)
+        print(json.dumps(reference_line(args, op, an, bn)), flush=True)
         return
 
     ws, rank, local, pg = dist_init()
@@ -787,6 +1104,8 @@ def main():
         res = run_batch(args, ws, rank, local, pg)
     elif op == "div":
         res = run_div(args, ws, rank, local, pg)
+    elif op == "serve":
+        res = run_serve(args, ws, rank, local, pg)
     else:
         res = run_ours(args, ws, rank, local, pg)
     if pg is not None:
@@ -804,6 +1123,8 @@ def main():
                 from simd_bigint_b200.workloads import division_shapes
                 res["cpu_baseline"] = cpu_run_div(division_shapes(1024, seed=4242),
                                                   cpu_threads_for(1 << 18, 1 << 18, cap=32), 1, 0)
+            elif op == "serve":
+                res["cpu_baseline"] = cpu_run_serve(args.cpu_requests, cpu_threads_for(1 << 20, 1 << 20, cap=32))
             else:
                 res["cpu_baseline"] = cpu_bounded(op, an, bn)
         except Exception as e:  # recorded, not fatal

@@ -73,6 +73,8 @@ const char *sbg_strerror(int status);
  * forward+pointwise+inverse, 3 column inverse, 4 CRT+carry, 5 batch,
  * 6 division helpers), waiting for them; n must be >= 8. */
 int sbg_ctx_set_timing(sbg_ctx *ctx, int on);
+/* Number of kernel launches this context has queued so far (diagnostics). */
+int64_t sbg_ctx_launches(sbg_ctx *ctx);
 int sbg_ctx_kernel_times(sbg_ctx *ctx, double *ms, int64_t *counts, int n);
 /* Largest an + bn accepted by one product (2^25 + 1). */
 int64_t sbg_max_total_limbs(void);
@@ -120,7 +122,8 @@ int sbg_batch_capture(sbg_batch *batch);
 int sbg_batch_run(sbg_batch *batch);
 /* Waits for queued runs, then frees. */
 void sbg_batch_destroy(sbg_batch *batch);
-/* create + run + destroy: returns when the products are written. */
+/* One-shot batch through the context's reusable product arena (no per-call
+ * allocation once it has grown): returns when the products are written. */
 int sbg_mul_batch(sbg_ctx *ctx, const sbg_job *jobs, int64_t count);
 
 /* ---- Newton reciprocal and division ----------------------------------------
@@ -190,6 +193,8 @@ int sbg_server_poll(sbg_server *srv, sbg_completion *out, int max, int *n, int w
 int sbg_server_release(sbg_server *srv, uint64_t ticket);
 int sbg_server_stats(sbg_server *srv, int64_t *pending, int64_t *completed, int64_t *batches,
                      size_t *arena_used);
+/* Kernel launches queued by the server so far (multiply batches and reciprocals). */
+int64_t sbg_server_launches(sbg_server *srv);
 /* Stops the scheduler (queued requests are dropped) and frees the arena. */
 void sbg_server_destroy(sbg_server *srv);
 

@@ -116,6 +116,10 @@ def lib(build_if_missing: bool = False):
         L.sbg_server_stats.argtypes = [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                        C.POINTER(C.c_int64), C.POINTER(C.c_size_t)]
         L.sbg_server_stats.restype = C.c_int
+        L.sbg_server_launches.argtypes = [_vp]
+        L.sbg_server_launches.restype = _i64
+        L.sbg_ctx_launches.argtypes = [_vp]
+        L.sbg_ctx_launches.restype = _i64
         L.sbg_server_destroy.argtypes = [_vp]
         L.sbg_server_destroy.restype = None
         _lib = L
@@ -207,6 +211,10 @@ class Context:
     def sqr(self, r, a, an: int | None = None):
         an = a.numel() if an is None else an
         _check(self._L.sbg_sqr(self.handle, _dptr(r), _dptr(a), an), "sbg_sqr")
+
+    def launches(self) -> int:
+        """Kernel launches this context has queued so far."""
+        return int(self._L.sbg_ctx_launches(self.handle))
 
     def recip(self, i, d, n: int | None = None):
         """i[0..n) = floor((B^2n - 1) / D) - B^n for a normalised n-limb D."""
@@ -348,6 +356,10 @@ class Server:
 
     def release(self, ticket: int):
         _check(self._L.sbg_server_release(self.handle, ticket), "sbg_server_release")
+
+    def launches(self) -> int:
+        """Kernel launches the server has queued so far."""
+        return int(self._L.sbg_server_launches(self.handle))
 
     def stats(self) -> dict:
         p, c, b, u = C.c_int64(0), C.c_int64(0), C.c_int64(0), C.c_size_t(0)

@@ -101,6 +101,7 @@ static int run_conv(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, co
     CK(launch_conv(ap, an, bp, bn, sq, lgL, lp, c->tw_f, c->tw_i, c->ws, c->stream, c->timer));
     CK(launch_crt_carry(c->ws, lgL, lp, cmin, cmax, off, rp, nout, c->flags, c->err, c->stream,
                         c->timer));
+    c->launches += class_launches(lgL);
     return SBG_OK;
 }
 
@@ -174,6 +175,134 @@ static int batch_launch(sbg_batch* b, KTimer* kt) {
     return SBG_OK;
 }
 
+namespace sbg {
+
+int UploadRing::push(const void* src, size_t bytes, cudaStream_t st, void** dev) {
+    const size_t need = (bytes + 255) & ~(size_t)255;
+    if (need > cap || head + need > cap) {
+        // the bytes about to be reused may still feed a copy or a kernel
+        if (last && last != st && cudaStreamSynchronize(last) != cudaSuccess) return SBG_ECUDA;
+        if (cudaStreamSynchronize(st) != cudaSuccess) return SBG_ECUDA;
+        head = 0;
+        if (need > cap) {
+            release();
+            const size_t nc = std::max(need * 4, (size_t)8 << 20);
+            if (cudaHostAlloc(&h, nc, 0) != cudaSuccess) return SBG_EALLOC;
+            if (cudaMalloc(&d, nc) != cudaSuccess) {
+                cudaFreeHost(h);
+                h = nullptr;
+                return SBG_EALLOC;
+            }
+            cap = nc;
+        }
+    }
+    std::memcpy(h + head, src, bytes);
+    if (bytes && cudaMemcpyAsync(d + head, h + head, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return SBG_ECUDA;
+    *dev = d + head;
+    head += need;
+    last = st;
+    return SBG_OK;
+}
+
+void UploadRing::release() {
+    if (h) cudaFreeHost(h);
+    if (d) cudaFree(d);
+    h = nullptr;
+    d = nullptr;
+    cap = head = 0;
+}
+
+int enqueue_products(sbg_ctx* c, const sbg_job* jobs, int64_t count, uint32_t* err) {
+    if (count <= 0) return SBG_OK;
+    std::vector<JobDesc> by_lg[SBG_MAX_LG + 1];
+    int64_t max_nout[SBG_MAX_LG + 1] = {};
+    for (int64_t i = 0; i < count; ++i) {
+        int lgL, sq;
+        int64_t cmin, cmax, off, nout;
+        int st = job_shape(jobs[i], &lgL, &cmin, &cmax, &off, &nout, &sq);
+        if (st) return st;
+        JobDesc d{};
+        d.a = jobs[i].ap;
+        d.b = sq ? jobs[i].ap : jobs[i].bp;
+        d.out = jobs[i].rp;
+        d.an = jobs[i].an;
+        d.bn = sq ? jobs[i].an : jobs[i].bn;
+        d.cmin = cmin; d.cmax = cmax; d.off = off; d.nout = nout;
+        d.sq = sq;
+        by_lg[lgL].push_back(d);
+        max_nout[lgL] = std::max(max_nout[lgL], nout);
+    }
+    size_t ws_total = 0, flag_total = 0;
+    for (int l = 0; l <= SBG_MAX_LG; ++l) {
+        if (by_lg[l].empty()) continue;
+        int st = ensure_plan(c, l);
+        if (st) return st;
+        for (auto& d : by_lg[l]) ws_total += ws_words(l, d.sq);
+        flag_total += by_lg[l].size() * ((size_t)crt_blocks(max_nout[l]) + 1 + 3) / 4 * 4;
+    }
+    const size_t bytes = (ws_total + flag_total) * 4;
+    if (bytes > c->pw_cap) {
+        // earlier lists on this stream may still use the arena
+        CK(cudaStreamSynchronize(c->stream));
+        cudaFree(c->pw);
+        c->pw = nullptr;
+        c->pw_cap = 0;
+        const size_t nb = bytes + bytes / 4;
+        CK(cudaMalloc(&c->pw, nb));
+        c->pw_cap = nb;
+    }
+    if (!c->fork) {
+        for (int k = 0; k < SBG_AUX_STREAMS; ++k) {
+            CK(cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&c->join[k], cudaEventDisableTiming));
+        }
+        CK(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    }
+    uint32_t* ws = (uint32_t*)c->pw;
+    uint32_t* fl = ws + ws_total;
+    struct Cls {
+        int lgL, njobs;
+        size_t first, flag_words;
+        uint32_t* flags;
+    };
+    std::vector<Cls> cls;
+    std::vector<JobDesc> all;
+    all.reserve((size_t)count);
+    for (int l = SBG_MAX_LG; l >= 0; --l) {           // longest transforms first
+        if (by_lg[l].empty()) continue;
+        const size_t fpj = ((size_t)crt_blocks(max_nout[l]) + 1 + 3) / 4 * 4;
+        cls.push_back(Cls{l, (int)by_lg[l].size(), all.size(), fpj * by_lg[l].size(), fl});
+        for (auto& d : by_lg[l]) {
+            d.ws = ws;
+            ws += ws_words(l, d.sq);
+            d.flags = fl;
+            fl += fpj;
+            all.push_back(d);
+        }
+    }
+    void* dd = nullptr;
+    int st = c->ring.push(all.data(), all.size() * sizeof(JobDesc), c->stream, &dd);
+    if (st) return st;
+    CK(cudaEventRecord(c->fork, c->stream));
+    const int nst = std::min<int>(SBG_AUX_STREAMS, (int)cls.size());
+    for (int k = 0; k < nst; ++k) CK(cudaStreamWaitEvent(c->aux[k], c->fork, 0));
+    for (size_t i = 0; i < cls.size(); ++i) {
+        const Cls& k = cls[i];
+        CK(launch_batch_class((const JobDesc*)dd + k.first, k.njobs, k.lgL, &c->plans[k.lgL], c->tw_f,
+                              c->tw_i, max_nout[k.lgL], k.flags, k.flag_words, err ? err : c->err,
+                              c->aux[i % SBG_AUX_STREAMS], c->timer));
+        c->launches += class_launches(k.lgL);
+    }
+    for (int k = 0; k < nst; ++k) {
+        CK(cudaEventRecord(c->join[k], c->aux[k]));
+        CK(cudaStreamWaitEvent(c->stream, c->join[k], 0));
+    }
+    return SBG_OK;
+}
+
+}  // namespace sbg
+
 extern "C" {
 
 const char* sbg_strerror(int status) {
@@ -245,6 +374,15 @@ void sbg_ctx_destroy(sbg_ctx* c) {
     cudaFree(c->flags);
     cudaFree(c->err);
     cudaFree(c->d_stage);
+    cudaFree(c->pw);
+    cudaFree(c->dscr);
+    cudaFree(c->derr);
+    c->ring.release();
+    for (int k = 0; k < SBG_AUX_STREAMS; ++k) {
+        if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
+        if (c->join[k]) cudaEventDestroy(c->join[k]);
+    }
+    if (c->fork) cudaEventDestroy(c->fork);
     delete c->timer;
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
@@ -464,6 +602,7 @@ int sbg_batch_run(sbg_batch* b) {
     if (!b) return SBG_EINVAL;
     sbg_ctx* c = b->ctx;
     CK(cudaSetDevice(c->device));
+    for (const auto& cl : b->classes) c->launches += class_launches(cl.lgL);
     if (b->exec) {
         CK(cudaGraphLaunch(b->exec, c->stream));
         return SBG_OK;
@@ -471,13 +610,14 @@ int sbg_batch_run(sbg_batch* b) {
     return batch_launch(b, c->timer);
 }
 
+int64_t sbg_ctx_launches(sbg_ctx* c) { return c ? c->launches.load() : 0; }
+
 int sbg_mul_batch(sbg_ctx* c, const sbg_job* jobs, int64_t count) {
-    sbg_batch* b = nullptr;
-    int st = sbg_batch_create(c, jobs, count, &b);
+    if (!c || (count > 0 && !jobs) || count < 0) return SBG_EINVAL;
+    CK(cudaSetDevice(c->device));
+    int st = enqueue_products(c, jobs, count);
     if (st) return st;
-    st = sbg_batch_run(b);
-    sbg_batch_destroy(b);      // waits for the batch
-    return st;
+    return sbg_ctx_sync(c);
 }
 
 int sbg_mulmid(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, const uint64_t* bp,

@@ -365,39 +365,20 @@ size_t div_scratch_limbs(int64_t n) { return (size_t)(14 * n + 64); }
 
 using namespace sbg;
 
-// run one list of products on the context (synchronous)
-extern "C" int sbg_batch_create(sbg_ctx*, const sbg_job*, int64_t, sbg_batch**);
-extern "C" int sbg_batch_run(sbg_batch*);
-extern "C" void sbg_batch_destroy(sbg_batch*);
-
-static int run_products(sbg_ctx* c, const std::vector<sbg_job>& jobs) {
-    if (jobs.empty()) return SBG_OK;
-    sbg_batch* b = nullptr;
-    int st = sbg_batch_create(c, jobs.data(), (int64_t)jobs.size(), &b);
-    if (st) return st;
-    st = sbg_batch_run(b);
-    sbg_batch_destroy(b);
-    return st;
-}
-
+// Every transfer below is stream-ordered on the context stream: descriptor
+// arrays go through the context's upload ring, products through its product
+// queue; the only synchronisation is the one at the end of a call.
 template <class T>
-static int upload(std::vector<T>& host, T** dev, size_t* cap) {
-    size_t bytes = host.size() * sizeof(T);
-    if (bytes > *cap) {
-        cudaFree(*dev);
-        *dev = nullptr;
-        *cap = 0;
-        if (cudaMalloc(dev, bytes) != cudaSuccess) return SBG_EALLOC;
-        *cap = bytes;
-    }
-    if (bytes && cudaMemcpy(*dev, host.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-        return SBG_ECUDA;
-    return SBG_OK;
+static int upload(sbg_ctx* c, const std::vector<T>& host, T** dev) {
+    void* d = nullptr;
+    int st = c->ring.push(host.data(), host.size() * sizeof(T), c->stream, &d);
+    *dev = (T*)d;
+    return st;
 }
 
 // Reciprocals (and optionally quotients) of every instance; all scratch set.
 static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quotient) {
-    cudaStream_t st = (cudaStream_t)sbg_ctx_get_stream(c);
+    cudaStream_t st = c->stream;
     int maxd = 0;
     for (auto& d : v) {
         d.sz.clear();
@@ -405,6 +386,7 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
         while (d.sz.back() > SBG_DIV_BASE) d.sz.push_back(h_of(d.sz.back()));
         maxd = std::max(maxd, (int)d.sz.size() - 1);
     }
+    int rc = SBG_OK;
     // base case: X[cur] of every instance
     {
         std::vector<const uint64_t*> A;
@@ -419,23 +401,11 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
         const uint64_t** dA = nullptr;
         int64_t* dm = nullptr;
         uint64_t** dX = nullptr;
-        size_t ca = 0, cm = 0, cx = 0;
-        int s1 = upload(A, (const uint64_t***)&dA, &ca);
-        if (!s1) s1 = upload(m, &dm, &cm);
-        if (!s1) s1 = upload(X, &dX, &cx);
-        if (!s1) {
-            k_recip_base<<<((int)v.size() + 127) / 128, 128, 0, st>>>(dA, dm, dX, (int)v.size(), err);
-            if (cudaGetLastError() != cudaSuccess) s1 = SBG_ECUDA;
-            if (!s1 && cudaStreamSynchronize(st) != cudaSuccess) s1 = SBG_ECUDA;
-        }
-        cudaFree(dA);
-        cudaFree(dm);
-        cudaFree(dX);
-        if (s1) return s1;
+        if ((rc = upload(c, A, &dA)) || (rc = upload(c, m, &dm)) || (rc = upload(c, X, &dX))) return rc;
+        k_recip_base<<<((int)v.size() + 127) / 128, 128, 0, st>>>(dA, dm, dX, (int)v.size(), err);
+        c->launches += 1;
+        if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
     }
-    RecipStep* dsteps = nullptr;
-    size_t cap = 0;
-    int rc = SBG_OK;
     for (int r = 1; r <= maxd && !rc; ++r) {
         std::vector<sbg_job> jt, ju;
         std::vector<RecipStep> steps;
@@ -458,19 +428,16 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
             ju.push_back(sbg_job{d.U, S.TM, S.Xh, h + 1, h + 1, SBG_JOB_MUL, 0});
         }
         if (steps.empty()) continue;
-        // the previous round's kernels still read dsteps: the (synchronous,
-        // default-stream) upload must not overtake them on our non-blocking stream
-        if (cudaStreamSynchronize(st) != cudaSuccess) { rc = SBG_ECUDA; break; }
-        if ((rc = upload(steps, &dsteps, &cap))) break;
-        if ((rc = run_products(c, jt))) break;
+        RecipStep* dsteps = nullptr;
+        if ((rc = upload(c, steps, &dsteps))) break;
+        if ((rc = enqueue_products(c, jt.data(), (int64_t)jt.size(), err))) break;
         k_recip_step1<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps, err);
+        c->launches += 2;                      // step1 and step2
         if (cudaGetLastError() != cudaSuccess) { rc = SBG_ECUDA; break; }
-        if ((rc = run_products(c, ju))) break;
+        if ((rc = enqueue_products(c, ju.data(), (int64_t)ju.size(), err))) break;
         k_recip_step2<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps);
         if (cudaGetLastError() != cudaSuccess) { rc = SBG_ECUDA; break; }
     }
-    if (cudaStreamSynchronize(st) != cudaSuccess && !rc) rc = SBG_ECUDA;
-    cudaFree(dsteps);
     if (rc) return rc;
     // final stage: exact reciprocal, or quotient and remainder
     std::vector<DivFix> fx;
@@ -490,34 +457,57 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
             // P = N_hi * V, V = low n limbs of X
             jp.push_back(sbg_job{d.P, d.N + d.n, X, d.n, d.n, SBG_JOB_MUL, 0});
         } else {
-            cudaMemcpyAsync(d.Q, X, (d.n + 1) * 8, cudaMemcpyDeviceToDevice, st);
+            if (cudaMemcpyAsync(d.Q, X, (d.n + 1) * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+                return SBG_ECUDA;
             jp.push_back(sbg_job{d.P, d.D, X, d.n, d.n + 1, SBG_JOB_MUL, 0});
         }
     }
     DivFix* dfx = nullptr;
-    size_t fcap = 0;
-    if (cudaStreamSynchronize(st) != cudaSuccess) return SBG_ECUDA;
-    rc = upload(fx, &dfx, &fcap);
-    if (!rc) rc = run_products(c, jp);
-    if (!rc && !quotient) {
+    if ((rc = upload(c, fx, &dfx))) return rc;
+    if ((rc = enqueue_products(c, jp.data(), (int64_t)jp.size(), err))) return rc;
+    if (!quotient) {
         k_recip_final<<<(int)fx.size(), DIV_T, 0, st>>>(dfx, err);
-        if (cudaGetLastError() != cudaSuccess) rc = SBG_ECUDA;
-    }
-    if (!rc && quotient) {
+        c->launches += 1;
+        if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
+    } else {
         k_div_q0<<<(int)fx.size(), DIV_T, 0, st>>>(dfx);
-        if (cudaGetLastError() != cudaSuccess) rc = SBG_ECUDA;
+        c->launches += 2;                      // q0 and fix
+        if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
         std::vector<sbg_job> jq;
         for (auto& d : v) jq.push_back(sbg_job{d.P, d.Q, d.D, d.n + 1, d.n, SBG_JOB_MUL, 0});
-        if (!rc) rc = run_products(c, jq);
-        if (!rc) {
-            k_div_fix<<<(int)fx.size(), DIV_T, 0, st>>>(dfx, err);
-            if (cudaGetLastError() != cudaSuccess) rc = SBG_ECUDA;
-        }
+        if ((rc = enqueue_products(c, jq.data(), (int64_t)jq.size(), err))) return rc;
+        k_div_fix<<<(int)fx.size(), DIV_T, 0, st>>>(dfx, err);
+        if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
         for (auto& d : v)
-            if (!rc) cudaMemcpyAsync(d.Qout, d.Q, d.qlen * 8, cudaMemcpyDeviceToDevice, st);
+            if (cudaMemcpyAsync(d.Qout, d.Q, d.qlen * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+                return SBG_ECUDA;
     }
-    if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = SBG_ECUDA;
-    cudaFree(dfx);
+    return SBG_OK;
+}
+
+// grow-only division scratch of the context (and its error word, cleared)
+static int div_scratch(sbg_ctx* c, size_t limbs, uint64_t** scratch) {
+    if (limbs > c->dscr_cap) {
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) return SBG_ECUDA;
+        cudaFree(c->dscr);
+        c->dscr = nullptr;
+        c->dscr_cap = 0;
+        const size_t nl = limbs + limbs / 4;
+        if (cudaMalloc(&c->dscr, nl * 8) != cudaSuccess) return SBG_EALLOC;
+        c->dscr_cap = nl;
+    }
+    if (!c->derr && cudaMalloc(&c->derr, 4) != cudaSuccess) return SBG_EALLOC;
+    if (cudaMemsetAsync(c->derr, 0, 4, c->stream) != cudaSuccess) return SBG_ECUDA;
+    *scratch = c->dscr;
+    return SBG_OK;
+}
+
+// wait for the call's work and turn its error word into a status
+static int div_finish(sbg_ctx* c, int rc) {
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess && !rc) rc = SBG_ECUDA;
+    uint32_t h = 0;
+    if (!rc && cudaMemcpy(&h, c->derr, 4, cudaMemcpyDeviceToHost) != cudaSuccess) rc = SBG_ECUDA;
+    if (!rc && h) rc = (h & 1u) ? SBG_ETIMEOUT : ((h & 2u) ? SBG_ESPILL : SBG_ECUDA);
     return rc;
 }
 
@@ -542,14 +532,10 @@ int sbg::recip_batch(sbg_ctx* c, const uint64_t* const* D, uint64_t* const* V, c
         if (2 * n[i] + 2 > ((int64_t)1 << 25)) return SBG_EBAND;
         total += div_scratch_limbs(n[i]);
     }
+    if (cudaSetDevice(c->device) != cudaSuccess) return SBG_ECUDA;
     uint64_t* scratch = nullptr;
-    uint32_t* err = nullptr;
-    if (cudaMalloc(&scratch, total * 8) != cudaSuccess) return SBG_EALLOC;
-    if (cudaMalloc(&err, 4) != cudaSuccess) {
-        cudaFree(scratch);
-        return SBG_EALLOC;
-    }
-    cudaMemsetAsync(err, 0, 4, (cudaStream_t)sbg_ctx_get_stream(c));
+    int rc = div_scratch(c, total, &scratch);
+    if (rc) return rc;
     std::vector<DivInst> v((size_t)count);
     uint64_t* p = scratch;
     for (int i = 0; i < count; ++i) {
@@ -561,13 +547,7 @@ int sbg::recip_batch(sbg_ctx* c, const uint64_t* const* D, uint64_t* const* V, c
         v[i].qlen = n[i];
         carve(v[i], p);
     }
-    int rc = div_core(c, v, err, false);
-    uint32_t h = 0;
-    if (!rc) cudaMemcpy(&h, err, 4, cudaMemcpyDeviceToHost);
-    cudaFree(scratch);
-    cudaFree(err);
-    if (rc) return rc;
-    return h ? SBG_ECUDA : SBG_OK;
+    return div_finish(c, div_core(c, v, c->derr, false));
 }
 
 extern "C" int sbg_recip(sbg_ctx* c, uint64_t* ip, const uint64_t* dp, int64_t n) {
@@ -589,17 +569,12 @@ extern "C" int sbg_divrem_batch(sbg_ctx* c, const sbg_div_job* jobs, int64_t cou
         if (2 * j.dn + 2 > ((int64_t)1 << 25)) return SBG_EBAND;
         total += div_scratch_limbs(j.dn) + 2 * j.dn + 8;
     }
+    if (cudaSetDevice(c->device) != cudaSuccess) return SBG_ECUDA;
     uint64_t* scratch = nullptr;
-    uint32_t* err = nullptr;
-    if (cudaMalloc(&scratch, total * 8) != cudaSuccess) return SBG_EALLOC;
-    if (cudaMalloc(&err, 4) != cudaSuccess) {
-        cudaFree(scratch);
-        return SBG_EALLOC;
-    }
-    cudaMemsetAsync(err, 0, 4, st);
+    int rc = div_scratch(c, total, &scratch);
+    if (rc) return rc;
     std::vector<DivInst> v((size_t)count);
     uint64_t* p = scratch;
-    int rc = SBG_OK;
     for (int64_t i = 0; i < count && !rc; ++i) {
         const sbg_div_job& j = jobs[i];
         DivInst& d = v[i];
@@ -617,17 +592,13 @@ extern "C" int sbg_divrem_batch(sbg_ctx* c, const sbg_div_job* jobs, int64_t cou
         d.N = Np;
         carve(d, p);
     }
-    if (!rc) rc = div_core(c, v, err, true);
-    uint32_t h = 0;
-    if (!rc) cudaMemcpy(&h, err, 4, cudaMemcpyDeviceToHost);
-    if (getenv("SBG_DEBUG") && (rc || h))
-        fprintf(stderr, "sbg_divrem_batch: rc=%d err=0x%x (count %lld, first dn %lld nn %lld)\n", rc,
-                h, (long long)count, count ? (long long)jobs[0].dn : 0LL,
+    if (!rc) rc = div_core(c, v, c->derr, true);
+    rc = div_finish(c, rc);
+    if (getenv("SBG_DEBUG") && rc)
+        fprintf(stderr, "sbg_divrem_batch: status %d (count %lld, first dn %lld nn %lld)\n", rc,
+                (long long)count, count ? (long long)jobs[0].dn : 0LL,
                 count ? (long long)jobs[0].nn : 0LL);
-    cudaFree(scratch);
-    cudaFree(err);
-    if (rc) return rc;
-    return h ? SBG_ECUDA : SBG_OK;
+    return rc;
 }
 
 extern "C" int sbg_divrem(sbg_ctx* c, uint64_t* qp, uint64_t* rp, const uint64_t* np, int64_t nn,

@@ -5,8 +5,10 @@
 #include <cstdint>
 #include <cstddef>
 
+#include <atomic>
 #include <vector>
 
+#include "../../include/simd_bigint_b200.h"
 #include "sbg_arith.cuh"
 
 namespace sbg {
@@ -187,6 +189,29 @@ struct EventTimer : KTimer {
     }
 };
 
+// Stream-ordered upload of small descriptor arrays without allocation or
+// synchronisation in steady state: bytes are copied into a pinned host ring
+// and an asynchronous copy into the matching device ring is enqueued on the
+// caller's stream.  Reusing ring bytes (wrap-around) or growing the ring
+// first synchronises the streams of earlier pushes, so no copy or kernel
+// still reading the reused bytes is in flight.  One host thread at a time.
+struct UploadRing {
+    uint8_t* h = nullptr;
+    uint8_t* d = nullptr;
+    size_t cap = 0, head = 0;
+    cudaStream_t last = nullptr;
+    int push(const void* src, size_t bytes, cudaStream_t st, void** dev);
+    void release();
+};
+
+#define SBG_AUX_STREAMS 4
+// transforms up to 2^12 points run in one CTA per prime (k_small)
+#define SBG_SMALL_MAX_LG 12
+
+// kernel launches of one product (or one length class of a batch): the
+// fused single-CTA transform or the three four-step transforms, then CRT+carry
+inline int class_launches(int lgL) { return lgL <= SBG_SMALL_MAX_LG ? 2 : 4; }
+
 }  // namespace sbg
 
 struct sbg_ctx {
@@ -205,6 +230,19 @@ struct sbg_ctx {
     uint64_t* d_stage = nullptr;
     size_t stage_cap = 0;
     sbg::EventTimer* timer = nullptr;    // non-null while kernel timing is on
+    // queued product lists (Newton division): grow-only arena for the
+    // transforms and carry flags, descriptor ring, forked streams
+    uint8_t* pw = nullptr;
+    size_t pw_cap = 0;
+    sbg::UploadRing ring;
+    cudaStream_t aux[SBG_AUX_STREAMS] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[SBG_AUX_STREAMS] = {};
+    // division scratch (grow-only) and its error word
+    uint64_t* dscr = nullptr;
+    size_t dscr_cap = 0;
+    uint32_t* derr = nullptr;
+    std::atomic<int64_t> launches{0};   // kernels queued by this context (diagnostics)
 };
 
 namespace sbg {
@@ -217,5 +255,11 @@ int ensure_plan(sbg_ctx* c, int lgL);
 int recip_batch(sbg_ctx* c, const uint64_t* const* D, uint64_t* const* V, const int64_t* n,
                 int count);
 size_t div_scratch_limbs(int64_t n);
+// Enqueue a list of products (sbg_job) on the context stream: one launch
+// sequence per transform-length class on forked streams, joined back.  No
+// allocation or synchronisation once the context's arena and ring have grown
+// to the largest list seen.  Device error bits go to `err` (null: the
+// context's own word).
+int enqueue_products(sbg_ctx* c, const sbg_job* jobs, int64_t count, uint32_t* err = nullptr);
 }  // namespace sbg
 

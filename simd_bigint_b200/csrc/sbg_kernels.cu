@@ -18,7 +18,6 @@ namespace sbg {
 __constant__ PrimeConst c_pr[SBG_NP];
 __constant__ CrtConst c_crt;
 
-#define SBG_SMALL_MAX_LG 12
 #define SBG_ROW_LG 12
 #define SBG_FS_LO_LG 13
 #define SBG_FS_LO_N (1 << SBG_FS_LO_LG)

@@ -141,6 +141,7 @@ struct sbg_server {
     std::thread sched, recip;
     uint64_t next_ticket = 1;
     int64_t n_done = 0, n_batches = 0;
+    int64_t mul_launches = 0;            // kernels of multiply batches
 };
 
 static size_t flag_words_of(const SReq& q) { return (size_t)(crt_blocks(q.nout) + 1 + 3) / 4 * 4; }
@@ -250,6 +251,7 @@ static int launch_slot(sbg_server* s, Slot& sl) {
                                c->tw_i, max_nout, sl.staging[i].flags, 0, derr, sl.st) !=
             cudaSuccess)
             return fail_batch();
+        s->mul_launches += class_launches(take[i].lgL);
         i = j;
     }
     if (cudaMemcpyAsync(sl.herr, derr, 4, cudaMemcpyDeviceToHost, sl.st) != cudaSuccess ||
@@ -469,6 +471,12 @@ extern "C" int sbg_server_release(sbg_server* s, uint64_t ticket) {
     s->results.erase(it);
     s->cv_work.notify_all();
     return SBG_OK;
+}
+
+extern "C" int64_t sbg_server_launches(sbg_server* s) {
+    if (!s) return 0;
+    std::lock_guard<std::mutex> g(s->mu);
+    return s->mul_launches + (s->rctx ? s->rctx->launches.load() : 0);
 }
 
 extern "C" int sbg_server_stats(sbg_server* s, int64_t* pending, int64_t* completed,
