@@ -33,7 +33,10 @@ def sources() -> list[Path]:
 
 
 def lib_path() -> Path:
-    return LIBDIR / LIBNAME
+    """The in-tree library, or the file named by SBG_LIBRARY (a build made
+    elsewhere, e.g. with other -D settings)."""
+    env = os.environ.get("SBG_LIBRARY")
+    return Path(env) if env else LIBDIR / LIBNAME
 
 
 def needs_build() -> bool:

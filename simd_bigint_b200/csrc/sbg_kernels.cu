@@ -10,8 +10,12 @@
 // (include/p30.h:1847-1938: input -> forward -> fused pointwise+inverse ->
 // scale -> Garner/carry), laid out as a four-step NTT over HBM: every pass
 // reads and writes each spectrum once, all levels inside a pass stay on chip.
+#include <cooperative_groups.h>
+
 #include "sbg_internal.h"
 #include "sbg_ntt.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace sbg {
 
@@ -118,21 +122,52 @@ __device__ __forceinline__ uint32_t fs_value(const FsTables& fs, int q, uint32_t
     return mul_shoup(a.x, b.x, b.y, p);
 }
 
-// Column tiles.  A CTA owns w adjacent columns (all N1 rows) of one operand
-// and one prime: 2^14 points (fewer when N1 * N2 is smaller).  Each thread
-// owns a PAIR of adjacent columns of one group per pass, so one twiddle load
-// serves two columns and the global accesses are 16-byte (two limbs) or
-// 8-byte (two residues) per row.  Columns live in shared memory as separate
-// planes (padded one word per 16, plane stride COL_LD), and every stride is a
-// compile-time constant of the column length.
-__host__ __device__ constexpr int col_lgw(int lgN1) {
-    return (14 - lgN1) > 12 ? 12 : ((14 - lgN1) < 1 ? 1 : (14 - lgN1));
+// Column tiles.  A CTA owns W adjacent columns of one operand and one prime
+// over a slab of M rows (M * W = 2^13 points, fewer when the whole transform
+// is smaller).  Two thread mappings:
+//  * lane per column (columns of at most 2^8 rows, W >= 32): a warp covers 32
+//    adjacent columns of one group, so every global access of a warp is one
+//    128-byte row piece (256 for limbs), each level's twiddle is one
+//    broadcast load, and the columns live in shared memory as planes of M + 1
+//    words (odd stride: the 32 lanes hit 32 distinct banks);
+//  * column pairs (longer columns, M up to 2^10, W = 2^13 / M): a thread owns
+//    two adjacent columns of one group, so one twiddle load serves two
+//    butterflies and the global accesses are 16-byte (two limbs) or 8-byte
+//    (two residues) row pieces; planes padded one word per 16.
+// Columns of more than 2^10 rows (transform lengths 2^23..2^25) are split
+// over a thread-block cluster of C = N1 / 2^10 CTAs, one slab of 2^10 rows
+// each, exchanging through distributed shared memory: the top lg C DIF levels
+// pair rows r + 2^10 t across the slabs.  Forward: each CTA reads the C rows
+// of its share of those groups from global memory, runs the lg C levels in
+// registers and stores each result into the shared memory of the CTA that
+// owns its slab; after a cluster barrier every CTA transforms its slab (an
+// independent 2^10-point DIF per column) and writes it out.  The inverse runs
+// the same network backwards.  The in-place result is the one a single CTA
+// holding the whole column would produce.  (Measured on B200 at 2^25 points:
+// 256-thread CTAs, four per SM, beat 512-thread ones; slabs of 2^8 or 2^9
+// rows need clusters of 16 whose shared-memory exchange costs more than the
+// wider rows save; lane-per-column wins where no exchange is needed.)
+#define SBG_COL_SLAB_LG 10
+#define SBG_COL_LANE_MAX_LG 8
+#define COL_THREADS 256
+#define COL_MINB 4
+__host__ __device__ constexpr bool col_lanes(int lgN1) { return lgN1 <= SBG_COL_LANE_MAX_LG; }
+__host__ __device__ constexpr int col_lgc(int lgN1) {
+    return lgN1 > SBG_COL_SLAB_LG ? lgN1 - SBG_COL_SLAB_LG : 0;
 }
-__host__ __device__ constexpr int col_ld(int lgN1) { return padded_len(1 << lgN1) + 1; }
+__host__ __device__ constexpr int col_lgs(int lgN1) { return lgN1 - col_lgc(lgN1); }
+__host__ __device__ constexpr int col_lgw_of(bool lanes, int lgs) {
+    return (13 - lgs) > 12 ? 12 : ((lanes && 13 - lgs < 5) ? 5 : 13 - lgs);
+}
+__host__ __device__ constexpr int col_lgw(int lgN1) { return col_lgw_of(col_lanes(lgN1), col_lgs(lgN1)); }
+__host__ __device__ constexpr int col_ld_of(bool lanes, int lgs) {
+    return lanes ? (1 << lgs) + 1 : padded_len(1 << lgs) + 1;
+}
+__host__ __device__ constexpr int col_ld(int lgN1) { return col_ld_of(col_lanes(lgN1), col_lgs(lgN1)); }
 // Column radix schedule: passes of 16 from the top, the remainder (1..3
-// levels) last.  (Measured alternatives on B200 at 2^25 points: a radix-32
-// last pass spills under the 64-register cap, and the remainder first costs
-// an extra shared-memory round trip in the forward kernel; both were slower.)
+// levels) last.  (A radix-32 last pass spills under the 64-register cap, and
+// the remainder first costs an extra shared-memory round trip; both were
+// slower on B200.)
 __host__ __device__ constexpr int col_np(int lg) { return num_passes(lg); }
 __host__ __device__ constexpr int prl(int lg, int k) { return k < (lg >> 2) ? 4 : (lg & 3); }
 __host__ __device__ constexpr int lgm_of(int lg, int k) {
@@ -141,10 +176,11 @@ __host__ __device__ constexpr int lgm_of(int lg, int k) {
     return m;
 }
 __host__ __device__ constexpr int col_smem_bytes(int lgN1) {
-    return col_np(lgN1) > 1 ? (1 << col_lgw(lgN1)) * col_ld(lgN1) * 4 : 0;
+    return (col_np(col_lgs(lgN1)) > 1 || col_lgc(lgN1) > 0)
+               ? (1 << col_lgw(lgN1)) * col_ld(lgN1) * 4
+               : 0;
 }
-
-#define COL_THREADS 512
+__host__ __device__ constexpr int col_ntiles(int lgN1) { return 1 << (SBG_ROW_LG - col_lgw(lgN1)); }
 
 template <int LGST>
 __device__ __forceinline__ int padded_at(int i0, int t) {
@@ -156,64 +192,36 @@ __device__ __forceinline__ int padded_at(int i0, int t) {
     }
 }
 
-// Pass K (0-based, forward numbering) of the column transform.
-template <int LGN1, int K, bool FWD>
-__device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restrict__ X,
-                                           int64_t xn, uint32_t* __restrict__ Y, int c0,
+// two limbs of row n (columns c, c+1) -> residues; zero beyond xn
+__device__ __forceinline__ void load_limb_pair(const uint64_t* __restrict__ X, int64_t xn, int64_t n,
+                                               bool al16, const PrimeConst& pc, uint32_t& x,
+                                               uint32_t& y) {
+    if (al16 && n + 1 < xn) {
+        ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(X + n));
+        x = limb_residue(v.x, pc);
+        y = limb_residue(v.y, pc);
+    } else {
+        x = n < xn ? limb_residue(__ldg(&X[n]), pc) : 0u;
+        y = n + 1 < xn ? limb_residue(__ldg(&X[n + 1]), pc) : 0u;
+    }
+}
+
+// Pass K (0-based, forward numbering) of the DIF/DIT of length 2^LGS on the
+// slab whose first row is row0.  SRC_G: read from global (limbs when FWD,
+// residues otherwise); DST_G: write residues to global; else shared memory.
+template <int LGS, int K, bool FWD, bool SRC_G, bool DST_G>
+__device__ __forceinline__ void col_pass_pair(uint32_t* sm, const uint64_t* __restrict__ X,
+                                           int64_t xn, uint32_t* __restrict__ Y, int c0, int row0,
                                            const uint2* __restrict__ tw, const PrimeConst& pc) {
-    constexpr int NP = col_np(LGN1);
-    constexpr int r = prl(LGN1, K);
+    constexpr int r = prl(LGS, K);
     constexpr int R = 1 << r;
-    constexpr int LGM = lgm_of(LGN1, K);
+    constexpr int LGM = lgm_of(LGS, K);
     constexpr int LGST = LGM - r;
     constexpr int ST = 1 << LGST;
-    constexpr int LGW = col_lgw(LGN1);
-    constexpr int LD = col_ld(LGN1);
-    constexpr int TOTAL = (1 << (LGW - 1)) << (LGN1 - r);
-    constexpr bool SRC_G = FWD ? (K == 0) : (K == NP - 1);
-    constexpr bool DST_G = FWD ? (K == NP - 1) : (K == 0);
+    constexpr int LGW = col_lgw_of(false, LGS);
+    constexpr int LD = col_ld_of(false, LGS);
+    constexpr int TOTAL = (1 << (LGW - 1)) << (LGS - r);
     const uint32_t p = pc.p;
-    if constexpr (R == 32) {
-        // single-column groups, column index fastest across lanes
-        constexpr int TOT1 = 1 << (LGW + LGN1 - 5);
-#pragma unroll 1
-        for (int gid = threadIdx.x; gid < TOT1; gid += COL_THREADS) {
-            const int g = gid & ((1 << LGW) - 1);
-            const int rest = gid >> LGW;
-            const int j0 = rest & (ST - 1);
-            const int blk = rest >> LGST;
-            const int i0 = (blk << LGM) + j0;
-            uint32_t x[32];
-            if constexpr (SRC_G) {
-                const int64_t n0 = ((int64_t)i0 << SBG_ROW_LG) + c0 + g;
-#pragma unroll
-                for (int t = 0; t < 32; ++t) {
-                    const int64_t n = n0 + ((int64_t)(ST * t) << SBG_ROW_LG);
-                    if constexpr (FWD)
-                        x[t] = n < xn ? limb_residue(__ldg(&X[n]), pc) : 0u;
-                    else
-                        x[t] = Y[n];
-                }
-            } else {
-                const uint32_t* s0 = sm + g * LD;
-#pragma unroll
-                for (int t = 0; t < 32; ++t) x[t] = s0[padded_at<LGST>(i0, t)];
-            }
-            if constexpr (FWD)
-                dif_regs<32>(x, tw, j0, ST, LGM, p);
-            else
-                dit_regs<32>(x, tw, j0, ST, LGM, p);
-            if constexpr (DST_G) {
-                const int64_t n0 = ((int64_t)i0 << SBG_ROW_LG) + c0 + g;
-#pragma unroll
-                for (int t = 0; t < 32; ++t) Y[n0 + ((int64_t)(ST * t) << SBG_ROW_LG)] = x[t];
-            } else {
-                uint32_t* s0 = sm + g * LD;
-#pragma unroll
-                for (int t = 0; t < 32; ++t) s0[padded_at<LGST>(i0, t)] = x[t];
-            }
-        }
-    } else {
     // groups per thread is a compile-time constant (TOTAL / COL_THREADS, or 1
     // when the tile has fewer groups than threads): unrolled, so every
     // group's global loads are in flight together
@@ -224,27 +232,18 @@ __device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restr
         if (TOTAL < COL_THREADS && gid >= TOTAL) break;
         const int j0 = gid & (ST - 1);
         const int rest = gid >> LGST;
-        const int blk = rest & ((1 << (LGN1 - LGM)) - 1);
-        const int cp = rest >> (LGN1 - LGM);
+        const int blk = rest & ((1 << (LGS - LGM)) - 1);
+        const int cp = rest >> (LGS - LGM);
         const int i0 = (blk << LGM) + j0;
         const int g0 = 2 * cp;
         uint32_t x[R], y[R];
         if constexpr (SRC_G) {
-            const int64_t n0 = ((int64_t)i0 << SBG_ROW_LG) + c0 + g0;
+            const int64_t n0 = ((int64_t)(i0 + row0) << SBG_ROW_LG) + c0 + g0;
             if constexpr (FWD) {
                 const bool al16 = (reinterpret_cast<uintptr_t>(X) & 15) == 0;
 #pragma unroll
-                for (int t = 0; t < R; ++t) {
-                    const int64_t n = n0 + ((int64_t)(ST * t) << SBG_ROW_LG);
-                    if (al16 && n + 1 < xn) {
-                        ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(X + n));
-                        x[t] = limb_residue(v.x, pc);
-                        y[t] = limb_residue(v.y, pc);
-                    } else {
-                        x[t] = n < xn ? limb_residue(__ldg(&X[n]), pc) : 0u;
-                        y[t] = n + 1 < xn ? limb_residue(__ldg(&X[n + 1]), pc) : 0u;
-                    }
-                }
+                for (int t = 0; t < R; ++t)
+                    load_limb_pair(X, xn, n0 + ((int64_t)(ST * t) << SBG_ROW_LG), al16, pc, x[t], y[t]);
             } else {
 #pragma unroll
                 for (int t = 0; t < R; ++t) {
@@ -268,7 +267,7 @@ __device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restr
         else
             dit_regs2<R>(x, y, tw, j0, ST, LGM, p);
         if constexpr (DST_G) {
-            const int64_t n0 = ((int64_t)i0 << SBG_ROW_LG) + c0 + g0;
+            const int64_t n0 = ((int64_t)(i0 + row0) << SBG_ROW_LG) + c0 + g0;
 #pragma unroll
             for (int t = 0; t < R; ++t) {
                 const int64_t n = n0 + ((int64_t)(ST * t) << SBG_ROW_LG);
@@ -284,116 +283,318 @@ __device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restr
             }
         }
     }
+}
+
+__device__ __forceinline__ uint32_t load_limb(const uint64_t* __restrict__ X, int64_t xn, int64_t n,
+                                              const PrimeConst& pc) {
+    return n < xn ? limb_residue(__ldg(&X[n]), pc) : 0u;
+}
+
+// Pass K of the lane-per-column mapping (a warp = 32 adjacent columns of one
+// group, one column per lane).
+template <int LGS, int K, bool FWD, bool SRC_G, bool DST_G>
+__device__ __forceinline__ void col_pass_lane(uint32_t* sm, const uint64_t* __restrict__ X,
+                                           int64_t xn, uint32_t* __restrict__ Y, int c0, int row0,
+                                           const uint2* __restrict__ tw, const PrimeConst& pc) {
+    constexpr int r = prl(LGS, K);
+    constexpr int R = 1 << r;
+    constexpr int LGM = lgm_of(LGS, K);
+    constexpr int LGST = LGM - r;
+    constexpr int ST = 1 << LGST;
+    constexpr int LGW = col_lgw_of(true, LGS);
+    constexpr int LD = col_ld_of(true, LGS);
+    constexpr int TOTAL = 1 << (LGW + LGS - r);     // (column, group) pairs
+    const uint32_t p = pc.p;
+    constexpr int ITER = TOTAL >= COL_THREADS ? TOTAL / COL_THREADS : 1;
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int gid = threadIdx.x + it * COL_THREADS;
+        if (TOTAL < COL_THREADS && gid >= TOTAL) break;
+        const int col = gid & ((1 << LGW) - 1);
+        const int grp = gid >> LGW;
+        const int j0 = grp & (ST - 1);
+        const int i0 = ((grp >> LGST) << LGM) + j0;
+        uint32_t x[R];
+        if constexpr (SRC_G) {
+            const int64_t n0 = ((int64_t)(i0 + row0) << SBG_ROW_LG) + c0 + col;
+#pragma unroll
+            for (int t = 0; t < R; ++t) {
+                const int64_t n = n0 + ((int64_t)(ST * t) << SBG_ROW_LG);
+                if constexpr (FWD)
+                    x[t] = load_limb(X, xn, n, pc);
+                else
+                    x[t] = Y[n];
+            }
+        } else {
+            const uint32_t* s0 = sm + col * LD + i0;
+#pragma unroll
+            for (int t = 0; t < R; ++t) x[t] = s0[ST * t];
+        }
+        if constexpr (FWD)
+            dif_regs<R>(x, tw, j0, ST, LGM, p);
+        else
+            dit_regs<R>(x, tw, j0, ST, LGM, p);
+        if constexpr (DST_G) {
+            const int64_t n0 = ((int64_t)(i0 + row0) << SBG_ROW_LG) + c0 + col;
+#pragma unroll
+            for (int t = 0; t < R; ++t) Y[n0 + ((int64_t)(ST * t) << SBG_ROW_LG)] = x[t];
+        } else {
+            uint32_t* s0 = sm + col * LD + i0;
+#pragma unroll
+            for (int t = 0; t < R; ++t) s0[ST * t] = x[t];
+        }
+    }
+}
+
+// Pass K (0-based, forward numbering) of the DIF/DIT of length 2^LGS on the
+// slab whose first row is row0, in the mapping LANES selects.  SRC_G: read
+// from global (limbs when FWD, residues otherwise); DST_G: write residues to
+// global; else shared memory.
+template <bool LANES, int LGS, int K, bool FWD, bool SRC_G, bool DST_G>
+__device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restrict__ X,
+                                           int64_t xn, uint32_t* __restrict__ Y, int c0, int row0,
+                                           const uint2* __restrict__ tw, const PrimeConst& pc) {
+    if constexpr (LANES)
+        col_pass_lane<LGS, K, FWD, SRC_G, DST_G>(sm, X, xn, Y, c0, row0, tw, pc);
+    else
+        col_pass_pair<LGS, K, FWD, SRC_G, DST_G>(sm, X, xn, Y, c0, row0, tw, pc);
+}
+
+// The local passes of a slab: forward K = 0 .. NP-1, inverse NP-1 .. 0.
+// FIRST_G / LAST_G: whether the first / last pass touches global memory.
+template <bool LANES, int LGS, bool FIRST_G, bool LAST_G>
+__device__ __forceinline__ void col_slab_fwd(uint32_t* sm, const uint64_t* __restrict__ X, int64_t xn,
+                                             uint32_t* __restrict__ Y, int c0, int row0,
+                                             const uint2* __restrict__ tw, const PrimeConst& pc) {
+    constexpr int NP = col_np(LGS);
+    col_pass_t<LANES, LGS, 0, true, FIRST_G, LAST_G && NP == 1>(sm, X, xn, Y, c0, row0, tw, pc);
+    if constexpr (NP > 1) {
+        __syncthreads();
+        col_pass_t<LANES, LGS, 1, true, false, LAST_G && NP == 2>(sm, X, xn, Y, c0, row0, tw, pc);
+    }
+    if constexpr (NP > 2) {
+        __syncthreads();
+        col_pass_t<LANES, LGS, 2, true, false, LAST_G && NP == 3>(sm, X, xn, Y, c0, row0, tw, pc);
+    }
+    if constexpr (NP > 3) {
+        __syncthreads();
+        col_pass_t<LANES, LGS, 3, true, false, LAST_G && NP == 4>(sm, X, xn, Y, c0, row0, tw, pc);
+    }
+}
+
+template <bool LANES, int LGS, bool FIRST_G, bool LAST_G>
+__device__ __forceinline__ void col_slab_inv(uint32_t* sm, uint32_t* __restrict__ Y, int c0, int row0,
+                                             const uint2* __restrict__ tw, const PrimeConst& pc) {
+    constexpr int NP = col_np(LGS);
+    if constexpr (NP > 3) {
+        col_pass_t<LANES, LGS, 3, false, FIRST_G, false>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+        __syncthreads();
+    }
+    if constexpr (NP > 2) {
+        col_pass_t<LANES, LGS, 2, false, FIRST_G && NP == 3, false>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+        __syncthreads();
+    }
+    if constexpr (NP > 1) {
+        col_pass_t<LANES, LGS, 1, false, FIRST_G && NP == 2, false>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+        __syncthreads();
+    }
+    col_pass_t<LANES, LGS, 0, false, FIRST_G && NP == 1, LAST_G>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+}
+
+// cluster barrier; RELEASE publishes this CTA's shared-memory stores (local
+// and remote) to the cluster, otherwise it only waits for every CTA to arrive
+template <bool RELEASE>
+__device__ __forceinline__ void cluster_barrier() {
+    if constexpr (RELEASE)
+        asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+    else
+        asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// Cluster levels (forward): this CTA's share of the radix-C groups
+// {r + M t : t < C}, rows r in [slab * M / C, (slab + 1) * M / C) of every
+// column pair, read from global, DIF'd, and scattered into the owning slabs.
+template <int LGN1>
+__device__ __forceinline__ void col_cross_fwd(uint32_t* sm, const uint64_t* __restrict__ X, int64_t xn,
+                                              int c0, int slab, const uint2* __restrict__ tw,
+                                              const PrimeConst& pc) {
+    constexpr int LGC = col_lgc(LGN1);
+    constexpr int C = 1 << LGC;
+    constexpr int LGS = col_lgs(LGN1);
+    constexpr int M = 1 << LGS;
+    constexpr int LGW = col_lgw(LGN1);
+    constexpr int LD = col_ld(LGN1);
+    constexpr int RPS = M >> LGC;
+    constexpr int TOTAL = RPS << (LGW - 1);
+    static_assert(TOTAL % COL_THREADS == 0, "cluster groups must fill the CTA");
+    constexpr int ITER = TOTAL / COL_THREADS;
+    cg::cluster_group cl = cg::this_cluster();
+    const bool al16 = (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int gid = threadIdx.x + it * COL_THREADS;
+        const int g0 = 2 * (gid & ((1 << (LGW - 1)) - 1));
+        const int r = slab * RPS + (gid >> (LGW - 1));
+        uint32_t x[C], y[C];
+        const int64_t n0 = ((int64_t)r << SBG_ROW_LG) + c0 + g0;
+#pragma unroll
+        for (int t = 0; t < C; ++t)
+            load_limb_pair(X, xn, n0 + ((int64_t)(M * t) << SBG_ROW_LG), al16, pc, x[t], y[t]);
+        dif_regs2<C>(x, y, tw, r, M, LGN1, pc.p);
+        const int a = g0 * LD + pad_idx(r);
+#pragma unroll
+        for (int t = 0; t < C; ++t) {
+            uint32_t* d = cl.map_shared_rank(sm, t);
+            d[a] = x[t];
+            d[a + LD] = y[t];
+        }
+    }
+}
+
+// Cluster levels (inverse): gather the C slabs' rows r + M t from their
+// CTAs' shared memory, DIT, and write them to global memory.
+template <int LGN1>
+__device__ __forceinline__ void col_cross_inv(uint32_t* sm, uint32_t* __restrict__ Y, int c0, int slab,
+                                              const uint2* __restrict__ tw, const PrimeConst& pc) {
+    constexpr int LGC = col_lgc(LGN1);
+    constexpr int C = 1 << LGC;
+    constexpr int LGS = col_lgs(LGN1);
+    constexpr int M = 1 << LGS;
+    constexpr int LGW = col_lgw(LGN1);
+    constexpr int LD = col_ld(LGN1);
+    constexpr int RPS = M >> LGC;
+    constexpr int TOTAL = RPS << (LGW - 1);
+    static_assert(TOTAL % COL_THREADS == 0, "cluster groups must fill the CTA");
+    constexpr int ITER = TOTAL / COL_THREADS;
+    cg::cluster_group cl = cg::this_cluster();
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int gid = threadIdx.x + it * COL_THREADS;
+        const int g0 = 2 * (gid & ((1 << (LGW - 1)) - 1));
+        const int r = slab * RPS + (gid >> (LGW - 1));
+        uint32_t x[C], y[C];
+        const int a = g0 * LD + pad_idx(r);
+#pragma unroll
+        for (int t = 0; t < C; ++t) {
+            const uint32_t* s = cl.map_shared_rank(sm, t);
+            x[t] = s[a];
+            y[t] = s[a + LD];
+        }
+        dit_regs2<C>(x, y, tw, r, M, LGN1, pc.p);
+        const int64_t n0 = ((int64_t)r << SBG_ROW_LG) + c0 + g0;
+#pragma unroll
+        for (int t = 0; t < C; ++t)
+            *reinterpret_cast<uint2*>(Y + n0 + ((int64_t)(M * t) << SBG_ROW_LG)) = make_uint2(x[t], y[t]);
     }
 }
 
 // K1: limbs -> residues -> column DIF (bit-reversed rows) for one operand,
-// one prime, one tile.
+// one prime, one tile (one slab of it when the column spans a cluster).
 template <int LGN1>
-__device__ __forceinline__ void col_fwd_body(int q, int tile, int op,
+__device__ __forceinline__ void col_fwd_body(int q, int tile, int slab, int op,
                                              const uint64_t* __restrict__ a, int64_t an,
                                              const uint64_t* __restrict__ b, int64_t bn,
                                              const uint2* __restrict__ twf,
                                              uint32_t* __restrict__ YA,
                                              uint32_t* __restrict__ YB) {
     extern __shared__ uint32_t sm[];
-    constexpr int NP = col_np(LGN1);
-    constexpr int LGW = col_lgw(LGN1);
+    constexpr int LGC = col_lgc(LGN1);
+    constexpr int LGS = col_lgs(LGN1);
     const uint64_t* X = op ? b : a;
     const int64_t xn = op ? bn : an;
     uint32_t* Y = (op ? YB : YA) + ((size_t)q << (LGN1 + SBG_ROW_LG));
     const PrimeConst pc = c_pr[q];
     const uint2* tw = twf + (size_t)q * SBG_TW_N;
-    const int c0 = tile << LGW;
-    col_pass_t<LGN1, 0, true>(sm, X, xn, Y, c0, tw, pc);
-    if constexpr (NP > 1) {
-        __syncthreads();
-        col_pass_t<LGN1, (NP > 1 ? 1 : 0), true>(sm, X, xn, Y, c0, tw, pc);
-    }
-    if constexpr (NP > 2) {
-        __syncthreads();
-        col_pass_t<LGN1, (NP > 2 ? 2 : 0), true>(sm, X, xn, Y, c0, tw, pc);
-    }
-    if constexpr (NP > 3) {
-        __syncthreads();
-        col_pass_t<LGN1, (NP > 3 ? 3 : 0), true>(sm, X, xn, Y, c0, tw, pc);
+    const int c0 = tile << col_lgw(LGN1);
+    if constexpr (LGC == 0) {
+        col_slab_fwd<col_lanes(LGN1), LGS, true, true>(sm, X, xn, Y, c0, 0, tw, pc);
+    } else {
+        cluster_barrier<false>();       // every CTA of the cluster is running
+        col_cross_fwd<LGN1>(sm, X, xn, c0, slab, tw, pc);
+        cluster_barrier<true>();        // all slabs complete in shared memory
+        col_slab_fwd<col_lanes(LGN1), LGS, false, true>(sm, X, xn, Y, c0, slab << LGS, tw, pc);
     }
 }
 
-// K1: limbs -> residues -> column DIF (bit-reversed rows) for one operand,
-// one prime, one tile.  Block order: prime slowest, so the CTAs resident on an
-// SM share one prime's twiddles.
+// Block order: cluster slab fastest, then prime, so the five primes' CTAs of
+// one tile run together and share its limbs through L2.
 template <int LGN1>
-__global__ void __launch_bounds__(512, 2) k_col_fwd(const uint64_t* __restrict__ a, int64_t an,
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col_fwd(const uint64_t* __restrict__ a, int64_t an,
                                                     const uint64_t* __restrict__ b, int64_t bn,
                                                     const uint2* __restrict__ twf,
                                                     uint32_t* __restrict__ YA,
                                                     uint32_t* __restrict__ YB, int nops) {
-    constexpr int NTILES = 1 << (SBG_ROW_LG - col_lgw(LGN1));
-    const int per_q = NTILES * nops;
-    const int q = blockIdx.x / per_q;
-    const int rest = blockIdx.x - q * per_q;
-    col_fwd_body<LGN1>(q, rest % NTILES, rest / NTILES, a, an, b, bn, twf, YA, YB);
+    constexpr int LGC = col_lgc(LGN1);
+    constexpr int NTILES = col_ntiles(LGN1);
+    const int slab = blockIdx.x & ((1 << LGC) - 1);
+    int rest = blockIdx.x >> LGC;
+    const int q = rest % SBG_NP;
+    rest /= SBG_NP;
+    col_fwd_body<LGN1>(q, rest % NTILES, slab, rest / NTILES, a, an, b, bn, twf, YA, YB);
 }
 
-// batched: blocks (job, prime, operand, tile), job slowest; the second
-// operand's blocks of a squaring exit at once
+// batched: blocks (job, operand, tile, prime, slab), job slowest; the second
+// operand's blocks of a squaring exit at once (whole clusters together)
 template <int LGN1>
-__global__ void __launch_bounds__(512, 2) k_col_fwd_b(const JobDesc* __restrict__ jobs,
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col_fwd_b(const JobDesc* __restrict__ jobs,
                                                       const uint2* __restrict__ twf) {
-    constexpr int NTILES = 1 << (SBG_ROW_LG - col_lgw(LGN1));
-    constexpr int PER_JOB = SBG_NP * 2 * NTILES;
+    constexpr int LGC = col_lgc(LGN1);
+    constexpr int NTILES = col_ntiles(LGN1);
+    constexpr int PER_JOB = (SBG_NP * 2 * NTILES) << LGC;
     const JobDesc& J = jobs[blockIdx.x / PER_JOB];
     const int r = blockIdx.x % PER_JOB;
-    const int q = r / (2 * NTILES);
-    const int r2 = r % (2 * NTILES);
-    const int op = r2 / NTILES;
+    const int slab = r & ((1 << LGC) - 1);
+    int rest = r >> LGC;
+    const int q = rest % SBG_NP;
+    rest /= SBG_NP;
+    const int op = rest / NTILES;
     if (op && J.sq) return;
     uint32_t* YB = J.ws + ((size_t)SBG_NP << (LGN1 + SBG_ROW_LG));
-    col_fwd_body<LGN1>(q, r2 % NTILES, op, J.a, J.an, J.b, J.bn, twf, J.ws, YB);
+    col_fwd_body<LGN1>(q, rest % NTILES, slab, op, J.a, J.an, J.b, J.bn, twf, J.ws, YB);
 }
 
 // K3: column DIT (reverse of K1), in place, natural row order out.
 template <int LGN1>
-__device__ __forceinline__ void col_inv_body(int q, int tile, uint32_t* __restrict__ YA,
+__device__ __forceinline__ void col_inv_body(int q, int tile, int slab, uint32_t* __restrict__ YA,
                                              const uint2* __restrict__ twi) {
     extern __shared__ uint32_t sm[];
-    constexpr int NP = col_np(LGN1);
-    constexpr int LGW = col_lgw(LGN1);
+    constexpr int LGC = col_lgc(LGN1);
+    constexpr int LGS = col_lgs(LGN1);
     uint32_t* Y = YA + ((size_t)q << (LGN1 + SBG_ROW_LG));
     const PrimeConst pc = c_pr[q];
     const uint2* tw = twi + (size_t)q * SBG_TW_N;
-    const int c0 = tile << LGW;
-    if constexpr (NP > 3) {
-        col_pass_t<LGN1, (NP > 3 ? 3 : 0), false>(sm, nullptr, 0, Y, c0, tw, pc);
-        __syncthreads();
+    const int c0 = tile << col_lgw(LGN1);
+    if constexpr (LGC == 0) {
+        col_slab_inv<col_lanes(LGN1), LGS, true, true>(sm, Y, c0, 0, tw, pc);
+    } else {
+        col_slab_inv<col_lanes(LGN1), LGS, true, false>(sm, Y, c0, slab << LGS, tw, pc);
+        cluster_barrier<true>();        // all slabs complete in shared memory
+        col_cross_inv<LGN1>(sm, Y, c0, slab, tw, pc);
+        cluster_barrier<false>();       // peers read this CTA's slab until here
     }
-    if constexpr (NP > 2) {
-        col_pass_t<LGN1, (NP > 2 ? 2 : 0), false>(sm, nullptr, 0, Y, c0, tw, pc);
-        __syncthreads();
-    }
-    if constexpr (NP > 1) {
-        col_pass_t<LGN1, (NP > 1 ? 1 : 0), false>(sm, nullptr, 0, Y, c0, tw, pc);
-        __syncthreads();
-    }
-    col_pass_t<LGN1, 0, false>(sm, nullptr, 0, Y, c0, tw, pc);
 }
 
 template <int LGN1>
-__global__ void __launch_bounds__(512, 2) k_col_inv(uint32_t* __restrict__ YA,
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col_inv(uint32_t* __restrict__ YA,
                                                     const uint2* __restrict__ twi) {
-    constexpr int NTILES = 1 << (SBG_ROW_LG - col_lgw(LGN1));
-    col_inv_body<LGN1>(blockIdx.x / NTILES, blockIdx.x % NTILES, YA, twi);
+    constexpr int LGC = col_lgc(LGN1);
+    const int slab = blockIdx.x & ((1 << LGC) - 1);
+    const int rest = blockIdx.x >> LGC;
+    col_inv_body<LGN1>(rest % SBG_NP, rest / SBG_NP, slab, YA, twi);
 }
 
 template <int LGN1>
-__global__ void __launch_bounds__(512, 2) k_col_inv_b(const JobDesc* __restrict__ jobs,
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col_inv_b(const JobDesc* __restrict__ jobs,
                                                       const uint2* __restrict__ twi) {
-    constexpr int NTILES = 1 << (SBG_ROW_LG - col_lgw(LGN1));
-    constexpr int PER_JOB = SBG_NP * NTILES;
+    constexpr int LGC = col_lgc(LGN1);
+    constexpr int NTILES = col_ntiles(LGN1);
+    constexpr int PER_JOB = (SBG_NP * NTILES) << LGC;
     const JobDesc& J = jobs[blockIdx.x / PER_JOB];
     const int r = blockIdx.x % PER_JOB;
-    col_inv_body<LGN1>(r / NTILES, r % NTILES, J.ws, twi);
+    const int slab = r & ((1 << LGC) - 1);
+    const int rest = r >> LGC;
+    col_inv_body<LGN1>(rest % SBG_NP, rest / SBG_NP, slab, J.ws, twi);
 }
 
 // K2: one row of N2 = 2^12 points for one prime, 256 threads.
@@ -853,6 +1054,16 @@ static cudaError_t col_attr() {
         e = cudaFuncSetAttribute(k_col_fwd_b<LGN1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_col_inv_b<LGN1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (col_lgc(LGN1) > 3) {        // clusters of 16 CTAs
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_col_fwd<LGN1>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_col_inv<LGN1>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_col_fwd_b<LGN1>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_col_inv_b<LGN1>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    }
     return e;
 }
 
@@ -930,6 +1141,26 @@ size_t ws_words(int lgL, int sq) {
     return (sq ? 1 : 2) * SBG_NP * L;
 }
 
+// Column kernels: 512 threads, dynamic shared memory, and a cluster of
+// 2^col_lgc CTAs when the columns span several slabs.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_col(void (*kern)(KArgs...), int lgN1, int64_t blocks, cudaStream_t st,
+                              Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks, 1, 1);
+    cfg.blockDim = dim3(COL_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = (size_t)col_smem_bytes(lgN1);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1u << col_lgc(lgN1);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = col_lgc(lgN1) > 0 ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_t bn, int sq,
                         int lgL, const LenPlan* lp, const uint2* tw_f, const uint2* tw_i,
                         uint32_t* ws, cudaStream_t st, KTimer* kt) {
@@ -952,21 +1183,21 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
     FsTables fsf{lp->fs_lo_f, lp->fs_hi_f, lp->hi_n};
     FsTables fsi{lp->fs_lo_i, lp->fs_hi_i, lp->hi_n};
     const int nops = sq ? 1 : 2;
-    const int ntiles = 1 << (SBG_ROW_LG - col_lgw(lgN1));
-    const size_t col_smem = (size_t)col_smem_bytes(lgN1);
+    const int64_t col_blocks = ((int64_t)col_ntiles(lgN1) * SBG_NP) << col_lgc(lgN1);
+    cudaError_t e = cudaSuccess;
     KT_BEGIN(kt, KID_COL_FWD, st);
     switch (lgN1) {
-#define SBG_LAUNCH_F(n)                                                                  \
-    case n:                                                                              \
-        k_col_fwd<n><<<nops * ntiles * SBG_NP, 512, col_smem, st>>>(a, an, b, bn, tw_f, YA, \
-                                                                    YB, nops);           \
+#define SBG_LAUNCH_F(n)                                                                      \
+    case n:                                                                                  \
+        e = launch_col(k_col_fwd<n>, n, nops * col_blocks, st, a, an, b, bn, tw_f, YA, YB, nops); \
         break;
         SBG_COL_CASES(SBG_LAUNCH_F)
 #undef SBG_LAUNCH_F
         default: return cudaErrorInvalidValue;
     }
     KT_END(kt, KID_COL_FWD, st);
-    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     KT_BEGIN(kt, KID_ROW, st);
     k_row12<<<(1 << lgN1) * SBG_NP, 256, 0, st>>>(YA, YB, sq, lgN1, fsf, fsi, sc, tw_f, tw_i);
@@ -975,13 +1206,14 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
     if (e != cudaSuccess) return e;
     KT_BEGIN(kt, KID_COL_INV, st);
     switch (lgN1) {
-#define SBG_LAUNCH_I(n)                                                          \
-    case n: k_col_inv<n><<<ntiles * SBG_NP, 512, col_smem, st>>>(YA, tw_i); break;
+#define SBG_LAUNCH_I(n) \
+    case n: e = launch_col(k_col_inv<n>, n, col_blocks, st, YA, tw_i); break;
         SBG_COL_CASES(SBG_LAUNCH_I)
 #undef SBG_LAUNCH_I
         default: return cudaErrorInvalidValue;
     }
     KT_END(kt, KID_COL_INV, st);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
@@ -1007,25 +1239,24 @@ cudaError_t launch_batch_class(const JobDesc* djobs, int njobs, int lgL, const L
         const int lgN1 = lp->lgN1;
         FsTables fsf{lp->fs_lo_f, lp->fs_hi_f, lp->hi_n};
         FsTables fsi{lp->fs_lo_i, lp->fs_hi_i, lp->hi_n};
-        const int ntiles = 1 << (SBG_ROW_LG - col_lgw(lgN1));
-        const size_t col_smem = (size_t)col_smem_bytes(lgN1);
+        const int64_t col_blocks = ((int64_t)njobs * col_ntiles(lgN1) * SBG_NP) << col_lgc(lgN1);
         switch (lgN1) {
-#define SBG_LAUNCH_FB(n)                                                              \
-    case n:                                                                           \
-        k_col_fwd_b<n><<<njobs * SBG_NP * 2 * ntiles, 512, col_smem, st>>>(djobs, tw_f); \
-        break;
+#define SBG_LAUNCH_FB(n) \
+    case n: e = launch_col(k_col_fwd_b<n>, n, 2 * col_blocks, st, djobs, tw_f); break;
             SBG_COL_CASES(SBG_LAUNCH_FB)
 #undef SBG_LAUNCH_FB
             default: return cudaErrorInvalidValue;
         }
+        if (e != cudaSuccess) return e;
         k_row12_b<<<(njobs * SBG_NP) << lgN1, 256, 0, st>>>(djobs, lgN1, fsf, fsi, sc, tw_f, tw_i);
         switch (lgN1) {
-#define SBG_LAUNCH_IB(n)                                                           \
-    case n: k_col_inv_b<n><<<njobs * SBG_NP * ntiles, 512, col_smem, st>>>(djobs, tw_i); break;
+#define SBG_LAUNCH_IB(n) \
+    case n: e = launch_col(k_col_inv_b<n>, n, col_blocks, st, djobs, tw_i); break;
             SBG_COL_CASES(SBG_LAUNCH_IB)
 #undef SBG_LAUNCH_IB
             default: return cudaErrorInvalidValue;
         }
+        if (e != cudaSuccess) return e;
     }
     const int bpj = (int)crt_blocks(max_nout);
     k_crt_carry_b<<<njobs * bpj, CRT_T, 0, st>>>(djobs, lgL, bpj, err);

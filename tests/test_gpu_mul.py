@@ -193,3 +193,23 @@ def test_large_2p24_random_spot_check(ctx):
     # properties independent of size: commutativity, and the top limbs of a
     # product of two top-nonzero operands
     assert np.array_equal(gpu_mul(c, a), u)
+
+
+@pytest.mark.parametrize("n", [(1 << 21) + 3, (1 << 22) + 5, (1 << 23) - 7])
+def test_cluster_lengths_all_ones_closed_form(ctx, n):
+    """Transform lengths 2^23 and 2^24: columns of 2^11 and 2^12 rows split
+    over clusters of 2 and 4 CTAs; the all-0xFF square is the CRT-headroom
+    worst case and has a closed form."""
+    a = O.pattern(n, "ones")
+    assert np.array_equal(gpu_sqr(a), ones_square(n))
+
+
+@pytest.mark.parametrize("an,bn", [(3 * (1 << 21) + 1, (1 << 21) - 5), ((1 << 23) + 1, 1 << 22),
+                                   ((1 << 22) - 1, (1 << 22) - 1)])
+def test_cluster_lengths_random_spot_check(ctx, an, bn):
+    rng = np.random.default_rng(an ^ bn)
+    a = rand_limbs(an, rng)
+    b = rand_limbs(bn, rng)
+    r = gpu_mul(a, b)
+    assert spot_check(a, b, r)
+    assert np.array_equal(gpu_mul(b, a), r)
