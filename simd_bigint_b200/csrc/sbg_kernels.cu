@@ -160,8 +160,10 @@ __host__ __device__ constexpr int col_lgw_of(bool lanes, int lgs) {
     return (13 - lgs) > 12 ? 12 : ((lanes && 13 - lgs < 5) ? 5 : 13 - lgs);
 }
 __host__ __device__ constexpr int col_lgw(int lgN1) { return col_lgw_of(col_lanes(lgN1), col_lgs(lgN1)); }
+// Plane strides: lanes, M + 1 (odd); pairs, padded length + 32/W, so that a
+// warp's W/2 column pairs x 64/W consecutive rows fall in distinct banks.
 __host__ __device__ constexpr int col_ld_of(bool lanes, int lgs) {
-    return lanes ? (1 << lgs) + 1 : padded_len(1 << lgs) + 1;
+    return lanes ? (1 << lgs) + 1 : padded_len(1 << lgs) + (32 >> col_lgw_of(false, lgs));
 }
 __host__ __device__ constexpr int col_ld(int lgN1) { return col_ld_of(col_lanes(lgN1), col_lgs(lgN1)); }
 // Column radix schedule: passes of 16 from the top, the remainder (1..3
@@ -230,10 +232,21 @@ __device__ __forceinline__ void col_pass_pair(uint32_t* sm, const uint64_t* __re
     for (int it = 0; it < ITER; ++it) {
         const int gid = threadIdx.x + it * COL_THREADS;
         if (TOTAL < COL_THREADS && gid >= TOTAL) break;
-        const int j0 = gid & (ST - 1);
-        const int rest = gid >> LGST;
-        const int blk = rest & ((1 << (LGS - LGM)) - 1);
-        const int cp = rest >> (LGS - LGM);
+        // passes that touch global memory put the column pairs of a row
+        // fastest (a warp covers W/2 pairs x 64/W rows: few row pieces per
+        // access); shared-memory-only passes put consecutive groups fastest
+        int j0, blk, cp;
+        if constexpr (SRC_G || DST_G) {
+            cp = gid & ((1 << (LGW - 1)) - 1);
+            const int rest = gid >> (LGW - 1);
+            j0 = rest & (ST - 1);
+            blk = rest >> LGST;
+        } else {
+            j0 = gid & (ST - 1);
+            const int rest = gid >> LGST;
+            blk = rest & ((1 << (LGS - LGM)) - 1);
+            cp = rest >> (LGS - LGM);
+        }
         const int i0 = (blk << LGM) + j0;
         const int g0 = 2 * cp;
         uint32_t x[R], y[R];
