@@ -97,6 +97,19 @@ int sbg_sqr(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an);
 int sbg_mulmid(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an, const uint64_t *bp,
                int64_t bn);
 
+/* ---- host-pointer entries, stream-ordered ---------------------------------
+ * The product of HOST operands into a HOST result, queued and returned at
+ * once: upload, transforms and download run on the context's streams, and
+ * consecutive calls alternate two staging slots so one product's download
+ * overlaps the next one's upload (use page-locked buffers for the overlap;
+ * pageable ones work but copy synchronously).  The buffers must stay valid
+ * and rp unread until sbg_ctx_sync returns.  Asynchronous form of nt_mul /
+ * nt_sqr (reference include/ntmul.h:71-80), which multiply host arrays one
+ * call at a time. */
+int sbg_mul_host(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an, const uint64_t *bp,
+                 int64_t bn);
+int sbg_sqr_host(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an);
+
 /* ---- batches ---------------------------------------------------------------
  * Thousands of independent products of uneven sizes in a few launches: jobs
  * are grouped by transform length, each group runs one launch per stage for

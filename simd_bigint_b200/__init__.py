@@ -80,6 +80,10 @@ def lib(build_if_missing: bool = False):
             getattr(L, name).restype = C.c_int
         L.sbg_sqr.argtypes = [_vp, _vp, _vp, _i64]
         L.sbg_sqr.restype = C.c_int
+        L.sbg_mul_host.argtypes = [_vp, _vp, _vp, _i64, _vp, _i64]
+        L.sbg_mul_host.restype = C.c_int
+        L.sbg_sqr_host.argtypes = [_vp, _vp, _vp, _i64]
+        L.sbg_sqr_host.restype = C.c_int
         L.sbg_nt_mul.argtypes = [_vp, _vp, C.c_ssize_t, _vp, C.c_ssize_t]
         L.sbg_nt_mul.restype = C.c_int
         L.sbg_nt_sqr.argtypes = [_vp, _vp, C.c_ssize_t]
@@ -211,6 +215,15 @@ class Context:
     def sqr(self, r, a, an: int | None = None):
         an = a.numel() if an is None else an
         _check(self._L.sbg_sqr(self.handle, _dptr(r), _dptr(a), an), "sbg_sqr")
+
+    def mul_host(self, r: np.ndarray, a: np.ndarray, b: np.ndarray):
+        """Queue r = a * b on HOST uint64 arrays (sbg_mul_host); r is valid
+        after sync().  Page-locked arrays overlap consecutive products."""
+        _check(self._L.sbg_mul_host(self.handle, r.ctypes.data, a.ctypes.data, len(a), b.ctypes.data, len(b)),
+               "sbg_mul_host")
+
+    def sqr_host(self, r: np.ndarray, a: np.ndarray):
+        _check(self._L.sbg_sqr_host(self.handle, r.ctypes.data, a.ctypes.data, len(a)), "sbg_sqr_host")
 
     def launches(self) -> int:
         """Kernel launches this context has queued so far."""

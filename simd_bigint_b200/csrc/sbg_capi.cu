@@ -374,6 +374,7 @@ void sbg_ctx_destroy(sbg_ctx* c) {
     cudaFree(c->flags);
     cudaFree(c->err);
     cudaFree(c->d_stage);
+    host_pipe_release(c);
     cudaFree(c->pw);
     cudaFree(c->dscr);
     cudaFree(c->derr);
@@ -400,6 +401,7 @@ int sbg_ctx_sync(sbg_ctx* c) {
     if (!c) return SBG_EINVAL;
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
+    if (host_pipe_sync(c) != SBG_OK) return SBG_ECUDA;
     uint32_t h = 0;
     CK(cudaMemcpy(&h, c->err, sizeof(h), cudaMemcpyDeviceToHost));
     if (h) {

@@ -243,6 +243,16 @@ struct sbg_ctx {
     size_t dscr_cap = 0;
     uint32_t* derr = nullptr;
     std::atomic<int64_t> launches{0};   // kernels queued by this context (diagnostics)
+    // host-operand products (sbg_mul_host): two staging slots so that one
+    // product's download overlaps the next one's upload and compute
+    struct HostSlot {
+        uint64_t* d = nullptr;          // operands then result
+        size_t cap = 0;                 // limbs
+        cudaEvent_t in_done = nullptr, comp_done = nullptr, out_done = nullptr;
+    };
+    HostSlot hslot[2];
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    int hnext = 0;
 };
 
 namespace sbg {
@@ -261,5 +271,8 @@ size_t div_scratch_limbs(int64_t n);
 // to the largest list seen.  Device error bits go to `err` (null: the
 // context's own word).
 int enqueue_products(sbg_ctx* c, const sbg_job* jobs, int64_t count, uint32_t* err = nullptr);
+// host-operand pipeline of a context: wait for its copies / free it
+int host_pipe_sync(sbg_ctx* c);
+void host_pipe_release(sbg_ctx* c);
 }  // namespace sbg
 

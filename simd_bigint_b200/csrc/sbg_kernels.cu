@@ -150,7 +150,9 @@ __device__ __forceinline__ uint32_t fs_value(const FsTables& fs, int q, uint32_t
 #define SBG_COL_SLAB_LG 10
 #define SBG_COL_LANE_MAX_LG 8
 #define COL_THREADS 256
+#ifndef COL_MINB
 #define COL_MINB 4
+#endif
 __host__ __device__ constexpr bool col_lanes(int lgN1) { return lgN1 <= SBG_COL_LANE_MAX_LG; }
 __host__ __device__ constexpr int col_lgc(int lgN1) {
     return lgN1 > SBG_COL_SLAB_LG ? lgN1 - SBG_COL_SLAB_LG : 0;
@@ -620,6 +622,9 @@ __global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col_inv_b(const JobDe
 // register group, so that stage never touches shared memory.
 #define ROW_LG 12
 #define ROW_N (1 << ROW_LG)
+#ifndef ROW_MINB
+#define ROW_MINB 4                // resident CTAs per SM the register budget is set for
+#endif
 __device__ __forceinline__ void row_body(int q, int row, uint32_t* __restrict__ YA,
                                          const uint32_t* __restrict__ YB, int sq, int lgN1,
                                          const FsTables& fsf, const FsTables& fsi,
@@ -739,7 +744,7 @@ __device__ __forceinline__ void row_body(int q, int row, uint32_t* __restrict__ 
     }
 }
 
-__global__ void __launch_bounds__(256, 4) k_row12(uint32_t* __restrict__ YA,
+__global__ void __launch_bounds__(256, ROW_MINB) k_row12(uint32_t* __restrict__ YA,
                                                   const uint32_t* __restrict__ YB, int sq,
                                                   int lgN1, FsTables fsf, FsTables fsi, ScaleArg sc,
                                                   const uint2* __restrict__ twf,
@@ -749,7 +754,7 @@ __global__ void __launch_bounds__(256, 4) k_row12(uint32_t* __restrict__ YA,
 }
 
 // batched: blocks (job, prime, row), job slowest
-__global__ void __launch_bounds__(256, 4) k_row12_b(const JobDesc* __restrict__ jobs, int lgN1,
+__global__ void __launch_bounds__(256, ROW_MINB) k_row12_b(const JobDesc* __restrict__ jobs, int lgN1,
                                                     FsTables fsf, FsTables fsi, ScaleArg sc,
                                                     const uint2* __restrict__ twf,
                                                     const uint2* __restrict__ twi) {
