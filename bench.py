@@ -78,6 +78,22 @@ def kernel_model(op: str, an: int, bn: int) -> dict:
     }
 
 
+def profiled_traffic(workload: str, kernel: str) -> int | None:
+    """DRAM read + write bytes per launch of `kernel` from the committed ncu
+    summary profiles/dram_traffic_<workload>.md (its table's 4th column)."""
+    f = ROOT / "profiles" / f"dram_traffic_{workload}.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) >= 4 and cells[0] == kernel:
+            try:
+                return int(cells[3])
+            except ValueError:
+                return None
+    return None
+
+
 def measured_peaks() -> tuple[float, str]:
     try:
         d = json.loads(PEAKS_FILE.read_text())
@@ -673,14 +689,22 @@ def serve_drive(srv, ops, base: int, arrivals, check_every: int, limit_s: float 
         try:
             t0 = time.perf_counter()
             sub_t[0] = t0
-            for i, (kind, ao, an, bo, bn) in enumerate(ops):
-                if arrivals is not None:
+            if arrivals is None:            # one burst: queued 1024 at a time
+                for i0 in range(0, len(ops), 1024):
+                    chunk = [(kind, base + 8 * ao, an, base + 8 * bo, bn)
+                             for kind, ao, an, bo, bn in ops[i0:i0 + 1024]]
+                    ts = srv.submit_many(chunk)
+                    with lock:
+                        for k, t in enumerate(ts):
+                            idx[t] = i0 + k
+            else:
+                for i, (kind, ao, an, bo, bn) in enumerate(ops):
                     d = t0 + arrivals[i] - time.perf_counter()
                     if d > 0:
                         time.sleep(d)
-                t = srv.submit(kind, base + 8 * ao, an, base + 8 * bo, bn)
-                with lock:
-                    idx[t] = i
+                    t = srv.submit(kind, base + 8 * ao, an, base + 8 * bo, bn)
+                    with lock:
+                        idx[t] = i
             sub_t[1] = time.perf_counter()
         except Exception as e:  # reported by the poller
             failed.append(repr(e))
@@ -807,7 +831,7 @@ def run_serve(args, ws, rank, local, pg) -> dict | None:
         "data": "synthetic: seeded uniform u64 limbs from a 2^25-limb device pool, divisors top bit set",
         "config": {"workload": f"serving: {n_main} mul/sqr/reciprocal requests (50/30/20%), sizes log-uniform "
                                "[32, 2^20] limbs, 70% balanced / 30% unbalanced (ratio up to 16), seed 2025; "
-                               "all submitted at once (saturation), then a Poisson arrival-rate sweep of "
+                               "submitted as one burst (sbg_server_submit_many, saturation), then a Poisson arrival-rate sweep of "
                                f"{n_sweep} requests at {list(SERVE_FRACS)} of that capacity",
                    "requests": n_main, "parallelism": f"replicas x{ws}",
                    "server": {"arena_gb": args.arena_gb, "slots": 4, "max_batch": 256},
@@ -1016,13 +1040,7 @@ def run_ours(args, ws, rank, local, pg) -> dict | None:
     bfly_peak = sbg.probe_bfly_peak(local)
     d = rows[dom]
     achieved = d["gbs"]
-    traffic = None
-    tfile = ROOT / "profiles" / "traffic.json"
-    if tfile.exists():
-        try:
-            traffic = json.loads(tfile.read_text()).get(args.workload, {}).get(dom)
-        except Exception:
-            traffic = None
+    traffic = profiled_traffic(args.workload, dom)
     bfly_rate = d["alg_bfly"] / (d["avg_ms"] * 1e-3) if d["alg_bfly"] else 0.0
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "traffic": traffic,

@@ -172,7 +172,7 @@ int sbg_divrem_batch(sbg_ctx *ctx, const sbg_div_job *jobs, int64_t count);
  * A scheduler thread forms batches from the head of the request FIFO while
  * their footprint (workspace + result) fits the arena, and runs up to
  * `slots` batches concurrently on their own streams; reciprocal requests are
- * batched by a second thread.  Latency is measured from sbg_server_submit to
+ * batched by `recip_workers` threads, each with its own context.  Latency is measured from sbg_server_submit to
  * the moment the server observes the result on the device. */
 enum { SBG_REQ_MUL = 0, SBG_REQ_SQR = 1, SBG_REQ_RECIP = 2 };
 typedef struct {
@@ -195,11 +195,18 @@ typedef struct {
     size_t arena_bytes;    /* HBM budget for workspaces and results (default 8 GiB) */
     int32_t slots;         /* batches in flight (default 4) */
     int32_t max_batch;     /* requests per batch (default 512) */
+    int32_t recip_workers; /* reciprocal batches in flight, own context each (default 2) */
+    int32_t reserved;
 } sbg_server_config;
 typedef struct sbg_server sbg_server;
 int sbg_server_create(sbg_ctx *ctx, const sbg_server_config *cfg, sbg_server **out);
 /* Thread-safe, non-blocking.  SBG_EADMIT: the request can never fit the arena. */
 int sbg_server_submit(sbg_server *srv, const sbg_request *req, uint64_t *ticket);
+/* A burst of requests under one lock: queues reqs[0..] in order until the
+ * first one that fails validation (its status is returned); *accepted = the
+ * number queued, tickets[i] their tickets. */
+int sbg_server_submit_many(sbg_server *srv, const sbg_request *reqs, int64_t count, uint64_t *tickets,
+                           int64_t *accepted);
 /* Up to max completions; waits up to wait_ms for the first. */
 int sbg_server_poll(sbg_server *srv, sbg_completion *out, int max, int *n, int wait_ms);
 /* Frees a completed request's result buffer. */

@@ -113,6 +113,8 @@ def lib(build_if_missing: bool = False):
         L.sbg_server_create.restype = C.c_int
         L.sbg_server_submit.argtypes = [_vp, _vp, C.POINTER(C.c_uint64)]
         L.sbg_server_submit.restype = C.c_int
+        L.sbg_server_submit_many.argtypes = [_vp, _vp, _i64, _vp, C.POINTER(_i64)]
+        L.sbg_server_submit_many.restype = C.c_int
         L.sbg_server_poll.argtypes = [_vp, _vp, C.c_int, C.POINTER(C.c_int), C.c_int]
         L.sbg_server_poll.restype = C.c_int
         L.sbg_server_release.argtypes = [_vp, C.c_uint64]
@@ -327,17 +329,19 @@ class Completion(C.Structure):
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("arena_bytes", C.c_size_t), ("slots", C.c_int32), ("max_batch", C.c_int32)]
+    _fields_ = [("arena_bytes", C.c_size_t), ("slots", C.c_int32), ("max_batch", C.c_int32),
+                ("recip_workers", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Server:
     """The serving loop (sbg_server_*): submit device-operand requests from
     any thread, poll completions (device result pointer + latency), release."""
 
-    def __init__(self, ctx: Context, arena_bytes: int = 8 << 30, slots: int = 4, max_batch: int = 512):
+    def __init__(self, ctx: Context, arena_bytes: int = 8 << 30, slots: int = 4, max_batch: int = 512,
+                 recip_workers: int = 2):
         self._L = lib()
         self.ctx = ctx
-        cfg = ServerConfig(arena_bytes, slots, max_batch)
+        cfg = ServerConfig(arena_bytes, slots, max_batch, recip_workers, 0)
         h = _vp()
         _check(self._L.sbg_server_create(ctx.handle, C.byref(cfg), C.byref(h)), "sbg_server_create")
         self.handle = h
@@ -354,6 +358,18 @@ class Server:
         t = C.c_uint64(0)
         st = self._L.sbg_server_submit(self.handle, C.byref(req), C.byref(t))
         return st, t.value
+
+    def submit_many(self, reqs: list[tuple]) -> list[int]:
+        """reqs: (kind, ap, an, bp, bn) tuples, queued under one lock; returns tickets."""
+        n = len(reqs)
+        arr = (Request * max(1, n))()
+        for i, (kind, ap, an, bp, bn) in enumerate(reqs):
+            arr[i].kind, arr[i].ap, arr[i].an, arr[i].bp, arr[i].bn = kind, ap, an, bp or None, bn
+        t = (C.c_uint64 * max(1, n))()
+        acc = _i64(0)
+        _check(self._L.sbg_server_submit_many(self.handle, C.cast(arr, _vp), n, C.cast(t, _vp), C.byref(acc)),
+               "sbg_server_submit_many")
+        return list(t[: acc.value])
 
     def poll(self, wait_ms: int = 0) -> list[tuple[int, int, int, int, float]]:
         """[(ticket, status, result device pointer, result limbs, latency_s)]"""

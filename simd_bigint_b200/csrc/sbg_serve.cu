@@ -11,11 +11,11 @@
 // other batches run join the next batch of a free slot, so batches from
 // different arrivals overlap on the device; finished batches are retired as
 // soon as their completion event fires, which frees their workspace for the
-// next admissions.  Reciprocal requests are batched the same way by a second
-// thread running the Newton reciprocal (all divisors of a batch in lockstep)
-// on its own context and stream.  A request is complete when its result is
-// in device memory; its latency is measured from submission to the moment the
-// server observes the completion.  Results stay in the arena until the client
+// next admissions.  Reciprocal requests are batched the same way by worker
+// threads (recip_workers, default 2) running the Newton reciprocal (all
+// divisors of a batch in lockstep), each on its own context and stream.  A
+// request is complete when its result is in device memory; its latency is
+// measured from submission to the moment the server observes the completion.  Results stay in the arena until the client
 // releases them.  There is no counterpart in the reference, which has no
 // serving layer; each result is the one sbg_mul / sbg_sqr / sbg_recip
 // compute for the same request alone.
@@ -127,7 +127,7 @@ using namespace sbg;
 
 struct sbg_server {
     sbg_ctx* ctx = nullptr;              // multiplies
-    sbg_ctx* rctx = nullptr;             // reciprocals (own stream and workspace)
+    std::vector<sbg_ctx*> rctx;          // reciprocal workers (own stream and workspace each)
     sbg_server_config cfg{};
     uint8_t* arena_base = nullptr;
     Arena arena;
@@ -138,7 +138,8 @@ struct sbg_server {
     std::deque<sbg_completion> done;
     std::unordered_map<uint64_t, std::pair<size_t, size_t>> results;   // ticket -> out block
     std::atomic<bool> stop{false};
-    std::thread sched, recip;
+    std::thread sched;
+    std::vector<std::thread> recip;
     uint64_t next_ticket = 1;
     int64_t n_done = 0, n_batches = 0;
     int64_t mul_launches = 0;            // kernels of multiply batches
@@ -162,8 +163,10 @@ static void complete(sbg_server* s, const SReq& q, int status, double t) {
     s->n_done++;
 }
 
-// one batch of multiplies on a free slot (called with s->mu held)
-static int launch_slot(sbg_server* s, Slot& sl) {
+// one batch of multiplies on a free slot: requests and arena blocks are
+// taken with s->mu held (lk), the CUDA calls run with it released so that
+// submissions and polls do not wait behind them
+static int launch_slot(sbg_server* s, Slot& sl, std::unique_lock<std::mutex>& lk) {
     sbg_ctx* c = s->ctx;
     std::vector<SReq> take;
     const size_t batch_cap = s->arena.size() / (size_t)std::max(1, s->cfg.slots);
@@ -204,6 +207,7 @@ static int launch_slot(sbg_server* s, Slot& sl) {
     // a failed enqueue fails the whole batch: wait for what was enqueued, free its memory
     auto fail_batch = [&]() {
         cudaStreamSynchronize(sl.st);
+        lk.lock();
         const double t = now_s();
         for (auto& q : take) {
             s->arena.release(q.ws_off, q.ws_bytes);
@@ -212,6 +216,7 @@ static int launch_slot(sbg_server* s, Slot& sl) {
         s->arena.release(mo, meta);
         return -1;
     };
+    lk.unlock();
     uint32_t* flags = (uint32_t*)(s->arena_base + mo + ((take.size() * sizeof(JobDesc) + 255) & ~(size_t)255));
     uint32_t* derr = flags + nflags - 4;
     uint32_t* fcur = flags;
@@ -239,6 +244,7 @@ static int launch_slot(sbg_server* s, Slot& sl) {
         cudaMemsetAsync(flags, 0, nflags * 4, sl.st) != cudaSuccess)
         return fail_batch();
     // one launch sequence per length class (flags already zeroed above)
+    int64_t nlaunch = 0;
     size_t i = 0;
     while (i < take.size()) {
         size_t j = i;
@@ -251,12 +257,14 @@ static int launch_slot(sbg_server* s, Slot& sl) {
                                c->tw_i, max_nout, sl.staging[i].flags, 0, derr, sl.st) !=
             cudaSuccess)
             return fail_batch();
-        s->mul_launches += class_launches(take[i].lgL);
+        nlaunch += class_launches(take[i].lgL);
         i = j;
     }
     if (cudaMemcpyAsync(sl.herr, derr, 4, cudaMemcpyDeviceToHost, sl.st) != cudaSuccess ||
         cudaEventRecord(sl.done, sl.st) != cudaSuccess)
         return fail_batch();
+    lk.lock();
+    s->mul_launches += nlaunch;
     sl.reqs = std::move(take);
     sl.meta_off = mo;
     sl.meta_bytes = meta;
@@ -288,7 +296,7 @@ static void sched_loop(sbg_server* s) {
         if (progress) s->cv_done.notify_all();
         for (auto& sl : s->slots) {
             if (sl.busy || s->pending_mul.empty()) continue;
-            if (launch_slot(s, sl) != 0) progress = true;
+            if (launch_slot(s, sl, lk) != 0) progress = true;
         }
         bool any_busy = false;
         for (auto& sl : s->slots) any_busy |= sl.busy;
@@ -301,8 +309,8 @@ static void sched_loop(sbg_server* s) {
     }
 }
 
-static void recip_loop(sbg_server* s) {
-    cudaSetDevice(s->rctx->device);
+static void recip_loop(sbg_server* s, sbg_ctx* rc) {
+    cudaSetDevice(rc->device);
     std::unique_lock<std::mutex> lk(s->mu);
     while (!s->stop) {
         if (s->pending_recip.empty()) {
@@ -336,7 +344,7 @@ static void recip_loop(sbg_server* s) {
             n.push_back(q.r.an);
         }
         lk.unlock();
-        int st = recip_batch(s->rctx, D.data(), V.data(), n.data(), (int)take.size());
+        int st = recip_batch(rc, D.data(), V.data(), n.data(), (int)take.size());
         lk.lock();
         const double t = now_s();
         for (auto& q : take) {
@@ -356,12 +364,18 @@ extern "C" int sbg_server_create(sbg_ctx* ctx, const sbg_server_config* cfg, sbg
     s->cfg.arena_bytes = cfg && cfg->arena_bytes ? cfg->arena_bytes : ((size_t)8 << 30);
     s->cfg.slots = cfg && cfg->slots > 0 ? cfg->slots : 4;
     s->cfg.max_batch = cfg && cfg->max_batch > 0 ? cfg->max_batch : 512;
+    s->cfg.recip_workers = cfg && cfg->recip_workers > 0 ? cfg->recip_workers : 2;
     int st = SBG_OK;
     do {
         if ((st = cuda_fail(cudaSetDevice(ctx->device), "device"))) break;
         for (int l = 4; l <= 22 && !st; ++l) st = ensure_plan(ctx, l);   // tables to 2^22 points
         if (st) break;
-        if ((st = sbg_ctx_create(ctx->device, &s->rctx))) break;
+        for (int w = 0; w < s->cfg.recip_workers && !st; ++w) {
+            sbg_ctx* rc = nullptr;
+            if ((st = sbg_ctx_create(ctx->device, &rc))) break;
+            s->rctx.push_back(rc);
+        }
+        if (st) break;
         if ((st = cuda_fail(cudaMalloc(&s->arena_base, s->cfg.arena_bytes), "arena"))) break;
         s->arena.init(s->cfg.arena_bytes);
         s->slots.resize((size_t)s->cfg.slots);
@@ -382,7 +396,7 @@ extern "C" int sbg_server_create(sbg_ctx* ctx, const sbg_server_config* cfg, sbg
         return st;
     }
     s->sched = std::thread(sched_loop, s);
-    s->recip = std::thread(recip_loop, s);
+    for (sbg_ctx* rc : s->rctx) s->recip.emplace_back(recip_loop, s, rc);
     *out = s;
     return SBG_OK;
 }
@@ -392,7 +406,8 @@ extern "C" void sbg_server_destroy(sbg_server* s) {
     s->stop = true;
     s->cv_work.notify_all();
     if (s->sched.joinable()) s->sched.join();
-    if (s->recip.joinable()) s->recip.join();
+    for (auto& t : s->recip)
+        if (t.joinable()) t.join();
     if (s->ctx) cudaSetDevice(s->ctx->device);
     for (auto& sl : s->slots) {
         if (sl.st) cudaStreamSynchronize(sl.st);
@@ -402,15 +417,15 @@ extern "C" void sbg_server_destroy(sbg_server* s) {
         cudaFreeHost(sl.herr);
     }
     cudaFree(s->arena_base);
-    if (s->rctx) sbg_ctx_destroy(s->rctx);
+    for (sbg_ctx* rc : s->rctx) sbg_ctx_destroy(rc);
     delete s;
 }
 
-extern "C" int sbg_server_submit(sbg_server* s, const sbg_request* req, uint64_t* ticket) {
-    if (!s || !req || !req->ap || req->an <= 0) return SBG_EINVAL;
-    SReq q;
+// validation and footprint of one request (no lock needed)
+static int prepare(sbg_server* s, const sbg_request* req, SReq& q) {
+    if (!req || !req->ap || req->an <= 0) return SBG_EINVAL;
+    q = SReq{};
     q.r = *req;
-    q.t_arrive = now_s();
     if (req->kind == SBG_REQ_RECIP) {
         q.nout = req->an;
         q.ws_bytes = div_scratch_limbs(req->an) * 8;
@@ -431,21 +446,58 @@ extern "C" int sbg_server_submit(sbg_server* s, const sbg_request* req, uint64_t
         q.ws_bytes = mul_ws_bytes(q);
     }
     if (q.ws_bytes + q.out_bytes + 4096 > s->arena.size()) return SBG_EADMIT;   // can never fit
-    {
-        std::lock_guard<std::mutex> g(s->mu);
-        if (q.lgL > 0 && s->ctx->plans[q.lgL].lgL != q.lgL) {
-            int st = ensure_plan(s->ctx, q.lgL);
+    return SBG_OK;
+}
+
+// queue prepared requests (s->mu held); stops at the first failure
+static int enqueue(sbg_server* s, SReq* q, int64_t n, uint64_t* tickets, int64_t* accepted) {
+    const double t = now_s();
+    for (int64_t i = 0; i < n; ++i) {
+        if (q[i].lgL > 0 && s->ctx->plans[q[i].lgL].lgL != q[i].lgL) {
+            int st = ensure_plan(s->ctx, q[i].lgL);
             if (st) return st;
         }
-        q.ticket = s->next_ticket++;
-        if (req->kind == SBG_REQ_RECIP)
-            s->pending_recip.push_back(q);
+        q[i].t_arrive = t;
+        q[i].ticket = s->next_ticket++;
+        if (q[i].r.kind == SBG_REQ_RECIP)
+            s->pending_recip.push_back(q[i]);
         else
-            s->pending_mul.push_back(q);
+            s->pending_mul.push_back(q[i]);
+        if (tickets) tickets[i] = q[i].ticket;
+        if (accepted) *accepted = i + 1;
+    }
+    return SBG_OK;
+}
+
+extern "C" int sbg_server_submit(sbg_server* s, const sbg_request* req, uint64_t* ticket) {
+    if (!s) return SBG_EINVAL;
+    SReq q;
+    int st = prepare(s, req, q);
+    if (st) return st;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        st = enqueue(s, &q, 1, ticket, nullptr);
     }
     s->cv_work.notify_all();
-    if (ticket) *ticket = q.ticket;
-    return SBG_OK;
+    return st;
+}
+
+extern "C" int sbg_server_submit_many(sbg_server* s, const sbg_request* reqs, int64_t count,
+                                      uint64_t* tickets, int64_t* accepted) {
+    if (!s || (count > 0 && !reqs) || count < 0) return SBG_EINVAL;
+    if (accepted) *accepted = 0;
+    std::vector<SReq> q((size_t)count);
+    int st = SBG_OK;
+    int64_t ok = 0;
+    for (; ok < count; ++ok)
+        if ((st = prepare(s, &reqs[ok], q[ok]))) break;
+    if (ok > 0) {
+        std::lock_guard<std::mutex> g(s->mu);
+        int st2 = enqueue(s, q.data(), ok, tickets, accepted);
+        if (st2) st = st2;
+    }
+    s->cv_work.notify_all();
+    return st;
 }
 
 extern "C" int sbg_server_poll(sbg_server* s, sbg_completion* out, int max, int* n, int wait_ms) {
@@ -476,7 +528,9 @@ extern "C" int sbg_server_release(sbg_server* s, uint64_t ticket) {
 extern "C" int64_t sbg_server_launches(sbg_server* s) {
     if (!s) return 0;
     std::lock_guard<std::mutex> g(s->mu);
-    return s->mul_launches + (s->rctx ? s->rctx->launches.load() : 0);
+    int64_t n = s->mul_launches;
+    for (sbg_ctx* rc : s->rctx) n += rc->launches.load();
+    return n;
 }
 
 extern "C" int sbg_server_stats(sbg_server* s, int64_t* pending, int64_t* completed,

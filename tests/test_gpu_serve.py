@@ -108,3 +108,46 @@ def test_admission_rejects_what_cannot_fit(ctx):
     assert done and done[0][0] == t and done[0][1] == 0
     srv.release(t)
     srv.close()
+
+
+def test_burst_submission_matches_single_requests(ctx):
+    import torch
+
+    import simd_bigint_b200 as sbg
+    rng = np.random.default_rng(502)
+    reqs = _requests(rng, 40, 1 << 15)
+    ops, keep = [], []
+    for kind, an, bn in reqs:
+        a = rng.integers(0, 2**64, an, dtype=np.uint64)
+        if kind == sbg.REQ_RECIP:
+            a[-1] |= np.uint64(1 << 63)
+        b = rng.integers(0, 2**64, bn, dtype=np.uint64)
+        ta = torch.from_numpy(a.view(np.int64)).cuda()
+        tb = torch.from_numpy(b.view(np.int64)).cuda()
+        keep.append((kind, an, bn, ta, tb))
+        ops.append((kind, ta.data_ptr(), an, tb.data_ptr(), bn))
+    srv = sbg.Server(ctx, arena_bytes=1 << 30, slots=3, max_batch=16, recip_workers=3)
+    tickets = srv.submit_many(ops)
+    assert len(tickets) == len(ops) and tickets == sorted(tickets)
+    where = {t: i for i, t in enumerate(tickets)}
+    got = {}
+    deadline = time.time() + 60
+    while len(got) < len(ops) and time.time() < deadline:
+        for ticket, status, rp, rn, lat in srv.poll(wait_ms=50):
+            assert status == 0
+            got[where[ticket]] = srv.result(rp, rn).cpu().numpy().view(np.uint64)
+            srv.release(ticket)
+    assert len(got) == len(ops)
+    assert srv.launches() > 0
+    srv.close()
+    for i, (kind, an, bn, ta, tb) in enumerate(keep):
+        n = an + bn if kind == sbg.REQ_MUL else (2 * an if kind == sbg.REQ_SQR else an)
+        r = torch.empty(n, dtype=torch.int64, device="cuda")
+        if kind == sbg.REQ_MUL:
+            ctx.mul(r, ta, tb)
+        elif kind == sbg.REQ_SQR:
+            ctx.sqr(r, ta)
+        else:
+            ctx.recip(r, ta)
+        ctx.sync()
+        assert np.array_equal(got[i], r.cpu().numpy().view(np.uint64)), (kind, an, bn)
