@@ -710,6 +710,7 @@ def serve_drive(srv, ops, base: int, arrivals, check_every: int, limit_s: float 
             failed.append(repr(e))
 
     lat = np.zeros(n)
+    que = np.zeros(n)
     samples = []
     got = 0
     th = threading.Thread(target=submitter)
@@ -720,7 +721,7 @@ def serve_drive(srv, ops, base: int, arrivals, check_every: int, limit_s: float 
             raise RuntimeError("submit failed: " + failed[0])
         if time.perf_counter() - t_start > limit_s:
             raise RuntimeError(f"serving run exceeded {limit_s:.0f}s ({got}/{n} done)")
-        for ticket, status, rp, rn, l in srv.poll(wait_ms=20):
+        for ticket, status, rp, rn, l, qs in srv.poll_detail(wait_ms=20):
             if status:
                 raise RuntimeError(f"request failed with status {status}")
             while True:
@@ -730,13 +731,14 @@ def serve_drive(srv, ops, base: int, arrivals, check_every: int, limit_s: float 
                     break
                 time.sleep(0.0001)
             lat[i] = l
+            que[i] = qs
             if check_every and i % check_every == 0:
                 samples.append((i, srv.result(rp, rn).cpu().numpy().view(np.uint64).copy()))
             srv.release(ticket)
             got += 1
     t_end = time.perf_counter()
     th.join()
-    return {"lat": lat, "samples": samples, "wall_s": t_end - t_start,
+    return {"lat": lat, "queue": que, "samples": samples, "wall_s": t_end - t_start,
             "submit_s": sub_t[1] - sub_t[0]}
 
 
@@ -780,7 +782,8 @@ def run_serve(args, ws, rank, local, pg) -> dict | None:
     ops = serve_operands(reqs, pool, seed=77 + rank)
     limbs = sum(serve_out_limbs(k, an, bn) for k, an, bn in reqs)
     ctx = sbg.Context(local)
-    srv = sbg.Server(ctx, arena_bytes=args.arena_gb << 30, slots=4, max_batch=256)
+    srv = sbg.Server(ctx, arena_bytes=args.arena_gb << 30, slots=args.slots, max_batch=256,
+                     batch_lg_points=args.batch_lg_points)
     clocks = ClockSampler(local)
     if rank == 0:
         clocks.start()
@@ -815,7 +818,9 @@ def run_serve(args, ws, rank, local, pg) -> dict | None:
         sweep.append({"offered_req_s": round(rate, 1), "achieved_req_s": round(n_sweep / r["wall_s"], 1),
                       "submit_req_s": round(n_sweep / max(r["submit_s"], 1e-9), 1),
                       "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99),
-                      "by_kind": {nm: {"p50_ms": _pct(lat[skinds == k], 50), "p99_ms": _pct(lat[skinds == k], 99)}
+                      "queue_p50_ms": _pct(r["queue"], 50), "queue_p99_ms": _pct(r["queue"], 99),
+                      "by_kind": {nm: {"p50_ms": _pct(lat[skinds == k], 50), "p99_ms": _pct(lat[skinds == k], 99),
+                                       "queue_p50_ms": _pct(r["queue"][skinds == k], 50)}
                                   for k, nm in ((0, "mul"), (1, "sqr"), (2, "recip"))}})
     clk = clocks.stop() if rank == 0 else None
     st = srv.stats()
@@ -834,7 +839,8 @@ def run_serve(args, ws, rank, local, pg) -> dict | None:
                                "submitted as one burst (sbg_server_submit_many, saturation), then a Poisson arrival-rate sweep of "
                                f"{n_sweep} requests at {list(SERVE_FRACS)} of that capacity",
                    "requests": n_main, "parallelism": f"replicas x{ws}",
-                   "server": {"arena_gb": args.arena_gb, "slots": 4, "max_batch": 256},
+                   "server": {"arena_gb": args.arena_gb, "slots": args.slots, "max_batch": 256,
+                              "batch_lg_points": args.batch_lg_points or 26},
                    "l2": "operand pool and results exceed L2; no flush"},
         "bit_exact": exact, "checked_results": checked, "recip_unchecked_large": skipped,
         "served_mlimb_s": round(limbs * ws / wall / 1e6, 1),
@@ -1126,6 +1132,8 @@ def main():
     ap.add_argument("--requests", type=int, default=200000, help="serve: requests at saturation")
     ap.add_argument("--sweep-requests", type=int, default=20000, help="serve: requests per sweep point")
     ap.add_argument("--arena-gb", type=int, default=16, help="serve: server arena (GiB)")
+    ap.add_argument("--slots", type=int, default=4, help="serve: batches in flight")
+    ap.add_argument("--batch-lg-points", type=int, default=0, help="serve: log2 points per batch (0: default)")
     ap.add_argument("--cpu-requests", type=int, default=640, help="serve: CPU baseline sample")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

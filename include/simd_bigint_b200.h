@@ -189,14 +189,16 @@ typedef struct {
     int32_t reserved;
     uint64_t *rp;          /* device result: an+bn (mul), 2an (sqr), an (recip) limbs */
     int64_t rn;
-    double latency_s;
+    double latency_s;      /* submission -> result observed on the device */
+    double queue_s;        /* submission -> launch of its batch (the rest is device time) */
 } sbg_completion;
 typedef struct {
     size_t arena_bytes;    /* HBM budget for workspaces and results (default 8 GiB) */
     int32_t slots;         /* batches in flight (default 4) */
     int32_t max_batch;     /* requests per batch (default 512) */
     int32_t recip_workers; /* reciprocal batches in flight, own context each (default 2) */
-    int32_t reserved;
+    int32_t batch_lg_points; /* log2 of the transform points one multiply batch may hold
+                                (default 26): smaller batches turn slots over sooner */
 } sbg_server_config;
 typedef struct sbg_server sbg_server;
 int sbg_server_create(sbg_ctx *ctx, const sbg_server_config *cfg, sbg_server **out);

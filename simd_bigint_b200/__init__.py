@@ -325,12 +325,12 @@ class Request(C.Structure):
 class Completion(C.Structure):
     """sbg_completion."""
     _fields_ = [("ticket", C.c_uint64), ("status", C.c_int32), ("reserved", C.c_int32),
-                ("rp", C.c_void_p), ("rn", C.c_int64), ("latency_s", C.c_double)]
+                ("rp", C.c_void_p), ("rn", C.c_int64), ("latency_s", C.c_double), ("queue_s", C.c_double)]
 
 
 class ServerConfig(C.Structure):
     _fields_ = [("arena_bytes", C.c_size_t), ("slots", C.c_int32), ("max_batch", C.c_int32),
-                ("recip_workers", C.c_int32), ("reserved", C.c_int32)]
+                ("recip_workers", C.c_int32), ("batch_lg_points", C.c_int32)]
 
 
 class Server:
@@ -338,10 +338,10 @@ class Server:
     any thread, poll completions (device result pointer + latency), release."""
 
     def __init__(self, ctx: Context, arena_bytes: int = 8 << 30, slots: int = 4, max_batch: int = 512,
-                 recip_workers: int = 2):
+                 recip_workers: int = 2, batch_lg_points: int = 0):
         self._L = lib()
         self.ctx = ctx
-        cfg = ServerConfig(arena_bytes, slots, max_batch, recip_workers, 0)
+        cfg = ServerConfig(arena_bytes, slots, max_batch, recip_workers, batch_lg_points)
         h = _vp()
         _check(self._L.sbg_server_create(ctx.handle, C.byref(cfg), C.byref(h)), "sbg_server_create")
         self.handle = h
@@ -372,11 +372,19 @@ class Server:
         return list(t[: acc.value])
 
     def poll(self, wait_ms: int = 0) -> list[tuple[int, int, int, int, float]]:
-        """[(ticket, status, result device pointer, result limbs, latency_s)]"""
+        """[(ticket, status, result device pointer, result limbs, latency_s)];
+        poll_detail() adds the queueing part of each latency."""
         n = C.c_int(0)
         _check(self._L.sbg_server_poll(self.handle, C.cast(self._buf, _vp), 4096, C.byref(n), wait_ms),
                "sbg_server_poll")
         return [(c.ticket, c.status, c.rp or 0, c.rn, c.latency_s) for c in self._buf[: n.value]]
+
+    def poll_detail(self, wait_ms: int = 0) -> list[tuple[int, int, int, int, float, float]]:
+        """[(ticket, status, result pointer, result limbs, latency_s, queue_s)]"""
+        n = C.c_int(0)
+        _check(self._L.sbg_server_poll(self.handle, C.cast(self._buf, _vp), 4096, C.byref(n), wait_ms),
+               "sbg_server_poll")
+        return [(c.ticket, c.status, c.rp or 0, c.rn, c.latency_s, c.queue_s) for c in self._buf[: n.value]]
 
     def result(self, rp: int, rn: int):
         """torch.int64 view of a completed result in the server's arena; valid

@@ -254,7 +254,7 @@ int enqueue_products(sbg_ctx* c, const sbg_job* jobs, int64_t count, uint32_t* e
     }
     if (!c->fork) {
         for (int k = 0; k < SBG_AUX_STREAMS; ++k) {
-            CK(cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking));
+            CK(cudaStreamCreateWithPriority(&c->aux[k], cudaStreamNonBlocking, c->stream_priority));
             CK(cudaEventCreateWithFlags(&c->join[k], cudaEventDisableTiming));
         }
         CK(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));

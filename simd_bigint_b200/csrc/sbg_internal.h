@@ -243,6 +243,7 @@ struct sbg_ctx {
     size_t dscr_cap = 0;
     uint32_t* derr = nullptr;
     std::atomic<int64_t> launches{0};   // kernels queued by this context (diagnostics)
+    int stream_priority = 0;            // priority of the streams the context creates itself
     // host-operand products (sbg_mul_host): two staging slots so that one
     // product's download overlaps the next one's upload and compute
     struct HostSlot {

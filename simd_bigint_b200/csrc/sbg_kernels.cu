@@ -781,7 +781,9 @@ __global__ void __launch_bounds__(256, ROW_MINB) k_row12_b(const JobDesc* __rest
 // and threads whose carry-in is 1 ripple the +1 into their limbs.
 // ------------------------------------------------------------------------
 #define CRT_T 256
+#ifndef CRT_PER
 #define CRT_PER 16
+#endif
 #define CRT_BLK (CRT_T * CRT_PER)
 #define LB_SPIN_LIMIT (1 << 22)
 #define FLAG_AGG 1u

@@ -1,21 +1,25 @@
 // sbg_serve.cu -- the serving loop: continuous batching of mul / sqr /
 // reciprocal requests with admission by HBM footprint.
 //
-// Requests arrive through sbg_server_submit (any host thread) and wait in a
-// FIFO.  A scheduler thread owns S "slots" (CUDA streams).  Whenever a slot is
-// free it takes the pending multiply requests from the head of the FIFO while
-// their footprint -- transform workspace, carry flags, job descriptor and the
-// result buffer -- fits in the server's HBM arena (first-fit allocator over
-// one device allocation), groups them by transform length and launches the
-// batch engine's stages on the slot's stream.  Requests that arrive while
-// other batches run join the next batch of a free slot, so batches from
-// different arrivals overlap on the device; finished batches are retired as
-// soon as their completion event fires, which frees their workspace for the
-// next admissions.  Reciprocal requests are batched the same way by worker
-// threads (recip_workers, default 2) running the Newton reciprocal (all
-// divisors of a batch in lockstep), each on its own context and stream.  A
-// request is complete when its result is in device memory; its latency is
-// measured from submission to the moment the server observes the completion.  Results stay in the arena until the client
+// Requests arrive through sbg_server_submit / sbg_server_submit_many (any
+// host thread) and wait in FIFOs.  A scheduler thread owns S "slots" (CUDA
+// streams).  Whenever a slot is free it takes multiply requests from the head
+// of a FIFO while their footprint -- transform workspace, carry flags, job
+// descriptor and the result buffer -- fits in the server's HBM arena (first-
+// fit allocator over one device allocation) and the batch's transform points
+// stay under a cap, groups them by transform length and launches the batch
+// engine's stages on the slot's stream.  Short requests (transforms up to
+// 2^17 points) have their own FIFO, served first by slot 0, whose stream has
+// the highest priority, so they do not queue behind long batches.  Requests
+// that arrive while other batches run join the next batch of a free slot, so
+// batches from different arrivals overlap on the device; finished batches are
+// retired as soon as their completion event fires, which frees their
+// workspace for the next admissions.  Reciprocal requests are batched the same
+// way by worker threads (recip_workers, default 2) running the Newton
+// reciprocal (all divisors of a batch in lockstep), each on its own context
+// and low-priority stream.  A request is complete when its result is in
+// device memory; its latency is measured from submission to the moment the
+// server observes the completion.  Results stay in the arena until the client
 // releases them.  There is no counterpart in the reference, which has no
 // serving layer; each result is the one sbg_mul / sbg_sqr / sbg_recip
 // compute for the same request alone.
@@ -94,7 +98,7 @@ class Arena {
 struct SReq {
     uint64_t ticket = 0;
     sbg_request r{};
-    double t_arrive = 0.0;
+    double t_arrive = 0.0, t_launch = 0.0;
     // shape
     int lgL = 0, sq = 0;
     int64_t cmin = 0, cmax = 0, off = 0, nout = 0;
@@ -128,12 +132,17 @@ using namespace sbg;
 struct sbg_server {
     sbg_ctx* ctx = nullptr;              // multiplies
     std::vector<sbg_ctx*> rctx;          // reciprocal workers (own stream and workspace each)
+    std::vector<cudaStream_t> rstreams;  // their low-priority streams
+    int prio_high = 0, prio_low = 0;
     sbg_server_config cfg{};
     uint8_t* arena_base = nullptr;
     Arena arena;
     std::mutex mu;                       // guards queues, arena, completions
     std::condition_variable cv_work, cv_done;
-    std::deque<SReq> pending_mul, pending_recip;
+    // multiply FIFOs by size: transforms up to 2^SMALL_LG points go to
+    // pending_small, served first by slot 0 (and by the others when no large
+    // request waits), so short requests do not queue behind long batches
+    std::deque<SReq> pending_small, pending_mul, pending_recip;
     std::vector<Slot> slots;
     std::deque<sbg_completion> done;
     std::unordered_map<uint64_t, std::pair<size_t, size_t>> results;   // ticket -> out block
@@ -145,6 +154,8 @@ struct sbg_server {
     int64_t mul_launches = 0;            // kernels of multiply batches
 };
 
+#define SMALL_LG 17
+
 static size_t flag_words_of(const SReq& q) { return (size_t)(crt_blocks(q.nout) + 1 + 3) / 4 * 4; }
 static size_t mul_ws_bytes(const SReq& q) { return ws_words(q.lgL, q.sq) * 4; }
 
@@ -155,6 +166,7 @@ static void complete(sbg_server* s, const SReq& q, int status, double t) {
     c.rp = status == SBG_OK ? (uint64_t*)(s->arena_base + q.out_off) : nullptr;
     c.rn = q.nout;
     c.latency_s = t - q.t_arrive;
+    c.queue_s = (q.t_launch > 0.0 ? q.t_launch : t) - q.t_arrive;
     if (status == SBG_OK)
         s->results[q.ticket] = {q.out_off, q.out_bytes};
     else
@@ -166,15 +178,20 @@ static void complete(sbg_server* s, const SReq& q, int status, double t) {
 // one batch of multiplies on a free slot: requests and arena blocks are
 // taken with s->mu held (lk), the CUDA calls run with it released so that
 // submissions and polls do not wait behind them
-static int launch_slot(sbg_server* s, Slot& sl, std::unique_lock<std::mutex>& lk) {
+static int launch_slot(sbg_server* s, Slot& sl, std::deque<SReq>& fifo,
+                       std::unique_lock<std::mutex>& lk) {
     sbg_ctx* c = s->ctx;
     std::vector<SReq> take;
     const size_t batch_cap = s->arena.size() / (size_t)std::max(1, s->cfg.slots);
+    const int64_t point_cap = (int64_t)1 << s->cfg.batch_lg_points;
     size_t batch_bytes = 0;
-    while (!s->pending_mul.empty() && (int)take.size() < s->cfg.max_batch) {
-        SReq& q = s->pending_mul.front();
+    int64_t batch_points = 0;
+    while (!fifo.empty() && (int)take.size() < s->cfg.max_batch) {
+        SReq& q = fifo.front();
         const size_t need = mul_ws_bytes(q) + q.out_bytes;
         if (!take.empty() && batch_bytes + need > batch_cap) break;   // leave room for other slots
+        // bounded work per batch, so that slots turn over and late arrivals start soon
+        if (!take.empty() && batch_points + ((int64_t)1 << q.lgL) > point_cap) break;
         size_t wo, oo;
         if (!s->arena.alloc(mul_ws_bytes(q), &wo)) break;             // FIFO: wait for memory
         if (!s->arena.alloc(q.out_bytes, &oo)) {
@@ -186,9 +203,12 @@ static int launch_slot(sbg_server* s, Slot& sl, std::unique_lock<std::mutex>& lk
         q.out_off = oo;
         take.push_back(q);
         batch_bytes += need;
-        s->pending_mul.pop_front();
+        batch_points += (int64_t)1 << q.lgL;
+        fifo.pop_front();
     }
     if (take.empty()) return 0;
+    const double t_launch = now_s();
+    for (auto& q : take) q.t_launch = t_launch;
     // descriptors grouped by length; the batch's carry flags follow them
     std::stable_sort(take.begin(), take.end(), [](const SReq& a, const SReq& b) { return a.lgL < b.lgL; });
     size_t nflags = 0;
@@ -201,7 +221,7 @@ static int launch_slot(sbg_server* s, Slot& sl, std::unique_lock<std::mutex>& lk
             s->arena.release(q.ws_off, q.ws_bytes);
             s->arena.release(q.out_off, q.out_bytes);
         }
-        for (auto it = take.rbegin(); it != take.rend(); ++it) s->pending_mul.push_front(*it);
+        for (auto it = take.rbegin(); it != take.rend(); ++it) fifo.push_front(*it);
         return 0;
     }
     // a failed enqueue fails the whole batch: wait for what was enqueued, free its memory
@@ -294,9 +314,14 @@ static void sched_loop(sbg_server* s) {
             progress = true;
         }
         if (progress) s->cv_done.notify_all();
-        for (auto& sl : s->slots) {
-            if (sl.busy || s->pending_mul.empty()) continue;
-            if (launch_slot(s, sl, lk) != 0) progress = true;
+        for (size_t k = 0; k < s->slots.size(); ++k) {
+            Slot& sl = s->slots[k];
+            if (sl.busy) continue;
+            const bool small_only = k == 0 && s->slots.size() > 1;
+            std::deque<SReq>& fifo =
+                (small_only || s->pending_mul.empty()) ? s->pending_small : s->pending_mul;
+            if (fifo.empty()) continue;
+            if (launch_slot(s, sl, fifo, lk) != 0) progress = true;
         }
         bool any_busy = false;
         for (auto& sl : s->slots) any_busy |= sl.busy;
@@ -318,8 +343,12 @@ static void recip_loop(sbg_server* s, sbg_ctx* rc) {
             continue;
         }
         std::vector<SReq> take;
+        const int64_t point_cap = (int64_t)1 << s->cfg.batch_lg_points;
+        int64_t points = 0;
         while (!s->pending_recip.empty() && (int)take.size() < s->cfg.max_batch) {
             SReq& q = s->pending_recip.front();
+            // a Newton reciprocal of n limbs costs about a product of 4n points
+            if (!take.empty() && points + 4 * q.r.an > point_cap) break;
             size_t wo, oo;
             if (!s->arena.alloc(q.ws_bytes, &wo)) break;
             if (!s->arena.alloc(q.out_bytes, &oo)) {
@@ -329,12 +358,15 @@ static void recip_loop(sbg_server* s, sbg_ctx* rc) {
             q.ws_off = wo;
             q.out_off = oo;
             take.push_back(q);
+            points += 4 * q.r.an;
             s->pending_recip.pop_front();
         }
         if (take.empty()) {
             s->cv_work.wait_for(lk, std::chrono::milliseconds(1));
             continue;
         }
+        const double t_launch = now_s();
+        for (auto& q : take) q.t_launch = t_launch;
         std::vector<const uint64_t*> D;
         std::vector<uint64_t*> V;
         std::vector<int64_t> n;
@@ -365,22 +397,39 @@ extern "C" int sbg_server_create(sbg_ctx* ctx, const sbg_server_config* cfg, sbg
     s->cfg.slots = cfg && cfg->slots > 0 ? cfg->slots : 4;
     s->cfg.max_batch = cfg && cfg->max_batch > 0 ? cfg->max_batch : 512;
     s->cfg.recip_workers = cfg && cfg->recip_workers > 0 ? cfg->recip_workers : 2;
+    s->cfg.batch_lg_points =
+        cfg && cfg->batch_lg_points > 0 ? std::min(cfg->batch_lg_points, 40) : 26;
     int st = SBG_OK;
     do {
         if ((st = cuda_fail(cudaSetDevice(ctx->device), "device"))) break;
         for (int l = 4; l <= 22 && !st; ++l) st = ensure_plan(ctx, l);   // tables to 2^22 points
         if (st) break;
+        // stream priorities: multiply slots highest, reciprocal workers lowest,
+        // so short multiplies are not queued behind long Newton batches
+        int prio_low = 0, prio_high = 0;
+        if ((st = cuda_fail(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high), "priorities"))) break;
+        s->prio_high = prio_high;
+        s->prio_low = prio_low;
         for (int w = 0; w < s->cfg.recip_workers && !st; ++w) {
             sbg_ctx* rc = nullptr;
             if ((st = sbg_ctx_create(ctx->device, &rc))) break;
             s->rctx.push_back(rc);
+            rc->stream_priority = prio_low;
+            cudaStream_t rs = nullptr;
+            if ((st = cuda_fail(cudaStreamCreateWithPriority(&rs, cudaStreamNonBlocking, prio_low), "rstream")))
+                break;
+            s->rstreams.push_back(rs);
+            sbg_ctx_set_stream(rc, rs);
         }
         if (st) break;
         if ((st = cuda_fail(cudaMalloc(&s->arena_base, s->cfg.arena_bytes), "arena"))) break;
         s->arena.init(s->cfg.arena_bytes);
         s->slots.resize((size_t)s->cfg.slots);
         for (auto& sl : s->slots) {
-            if ((st = cuda_fail(cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking), "slot")))
+            // slot 0 (short requests) above the other slots, which are above
+            // the reciprocal workers
+            const int pr = &sl == &s->slots[0] ? s->prio_high : std::min(s->prio_high + 1, s->prio_low);
+            if ((st = cuda_fail(cudaStreamCreateWithPriority(&sl.st, cudaStreamNonBlocking, pr), "slot")))
                 break;
             if ((st = cuda_fail(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "ev")))
                 break;
@@ -418,6 +467,7 @@ extern "C" void sbg_server_destroy(sbg_server* s) {
     }
     cudaFree(s->arena_base);
     for (sbg_ctx* rc : s->rctx) sbg_ctx_destroy(rc);
+    for (cudaStream_t rs : s->rstreams) cudaStreamDestroy(rs);
     delete s;
 }
 
@@ -462,7 +512,7 @@ static int enqueue(sbg_server* s, SReq* q, int64_t n, uint64_t* tickets, int64_t
         if (q[i].r.kind == SBG_REQ_RECIP)
             s->pending_recip.push_back(q[i]);
         else
-            s->pending_mul.push_back(q[i]);
+            (q[i].lgL <= SMALL_LG ? s->pending_small : s->pending_mul).push_back(q[i]);
         if (tickets) tickets[i] = q[i].ticket;
         if (accepted) *accepted = i + 1;
     }
@@ -537,7 +587,8 @@ extern "C" int sbg_server_stats(sbg_server* s, int64_t* pending, int64_t* comple
                                 int64_t* batches, size_t* arena_used) {
     if (!s) return SBG_EINVAL;
     std::lock_guard<std::mutex> g(s->mu);
-    if (pending) *pending = (int64_t)(s->pending_mul.size() + s->pending_recip.size());
+    if (pending)
+        *pending = (int64_t)(s->pending_small.size() + s->pending_mul.size() + s->pending_recip.size());
     if (completed) *completed = s->n_done;
     if (batches) *batches = s->n_batches;
     if (arena_used) *arena_used = s->arena.used();
