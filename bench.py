@@ -159,7 +159,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def dist_init():
+def dist_init(backend: str | None = None):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE).  The
+    products are independent replicas: the only collective is the max over
+    ranks of the timings (NCCL on GPUs; gloo where there is none)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -167,17 +170,22 @@ def dist_init():
     if ws > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=None)
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return ws, rank, local, pg
 
 
 def barrier_max(pg, value: float, device) -> float:
+    """Max of a per-rank timing over all ranks (the job ends with the slowest)."""
     if pg is None:
         return value
     import torch
+    if pg.get_backend() == "gloo":
+        device = "cpu"
     t = torch.tensor([value], dtype=torch.float64, device=device)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
@@ -234,6 +242,7 @@ def cpu_threads_for(an: int, bn: int, want: int | None = None, cap: int = 64) ->
         avail = 8 << 30
     per = 140 * (an + bn) + (1 << 28)          # reference p50 working set per thread (~4.2 GB at 2^25)
     t = max(1, min(cores, int(avail * 0.6 // per)))
+    want = want or int(os.environ.get("SBG_CPU_THREADS", "0")) or None   # an explicit cap, if any
     if want:
         t = min(t, want)
     return t
