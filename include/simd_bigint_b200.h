@@ -75,6 +75,17 @@ const char *sbg_strerror(int status);
 int sbg_ctx_set_timing(sbg_ctx *ctx, int on);
 /* Number of kernel launches this context has queued so far (diagnostics). */
 int64_t sbg_ctx_launches(sbg_ctx *ctx);
+/* Transform lengths.  A product of N coefficients runs at L = 2^a >= N or,
+ * for 2^(k+1) < N <= 3 * 2^k with 16 <= k <= 23, at L = 3 * 2^k when bit k
+ * of the context's mask is set.  sbg_ctx_autotune times one product of each
+ * such size class at both lengths on this device (about a second; allocates
+ * 400 MB temporarily) and sets the mask to the faster; times (optional, 16
+ * doubles) receives {ms at 2^(k+2), ms at 3 * 2^k} for k = 16 .. 23.  No
+ * counterpart in the reference (its p30 engine picks lengths by its own
+ * table, include/p30.h:31-37). */
+int sbg_ctx_autotune(sbg_ctx *ctx, double *times);
+int sbg_ctx_set_len3_mask(sbg_ctx *ctx, uint32_t mask);
+uint32_t sbg_ctx_get_len3_mask(sbg_ctx *ctx);
 int sbg_ctx_kernel_times(sbg_ctx *ctx, double *ms, int64_t *counts, int n);
 /* Largest an + bn accepted by one product (2^25 + 1). */
 int64_t sbg_max_total_limbs(void);

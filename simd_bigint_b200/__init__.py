@@ -126,6 +126,12 @@ def lib(build_if_missing: bool = False):
         L.sbg_server_launches.restype = _i64
         L.sbg_ctx_launches.argtypes = [_vp]
         L.sbg_ctx_launches.restype = _i64
+        L.sbg_ctx_autotune.argtypes = [_vp, C.POINTER(C.c_double)]
+        L.sbg_ctx_autotune.restype = C.c_int
+        L.sbg_ctx_set_len3_mask.argtypes = [_vp, C.c_uint32]
+        L.sbg_ctx_set_len3_mask.restype = C.c_int
+        L.sbg_ctx_get_len3_mask.argtypes = [_vp]
+        L.sbg_ctx_get_len3_mask.restype = C.c_uint32
         L.sbg_server_destroy.argtypes = [_vp]
         L.sbg_server_destroy.restype = None
         _lib = L
@@ -230,6 +236,20 @@ class Context:
     def launches(self) -> int:
         """Kernel launches this context has queued so far."""
         return int(self._L.sbg_ctx_launches(self.handle))
+
+    def autotune(self) -> dict:
+        """sbg_ctx_autotune: {k: (ms at 2^(k+2), ms at 3*2^k)} and the chosen mask."""
+        t = (C.c_double * 16)()
+        _check(self._L.sbg_ctx_autotune(self.handle, t), "sbg_ctx_autotune")
+        return {"times": {16 + i: (t[2 * i], t[2 * i + 1]) for i in range(8)},
+                "len3_mask": int(self._L.sbg_ctx_get_len3_mask(self.handle))}
+
+    def set_len3_mask(self, mask: int):
+        _check(self._L.sbg_ctx_set_len3_mask(self.handle, mask), "sbg_ctx_set_len3_mask")
+
+    @property
+    def len3_mask(self) -> int:
+        return int(self._L.sbg_ctx_get_len3_mask(self.handle))
 
     def recip(self, i, d, n: int | None = None):
         """i[0..n) = floor((B^2n - 1) / D) - B^n for a normalised n-limb D."""

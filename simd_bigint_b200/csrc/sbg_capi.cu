@@ -33,10 +33,17 @@ int lg_ceil(int64_t n) {
     return l;
 }
 
-// Transform length for a convolution whose wanted coefficients need L >= need.
-int conv_lg(int64_t need) {
+// Transform length (code) for a convolution whose wanted coefficients need
+// L >= need: 2^a >= need, or 3 * 2^b >= need when that is shorter and bit b
+// of `mask3` allows it (the context's choice per size class, sbg_ctx_autotune).
+int conv_lg(int64_t need, uint32_t mask3) {
     int l = lg_ceil(need);
-    return l < 4 ? 4 : l;
+    if (l < 4) l = 4;
+    int k = lg_ceil((need + 2) / 3);
+    if (k >= SBG_THREE_MIN_LG && k <= SBG_MAX_LG - 2 && ((int64_t)3 << k) < ((int64_t)1 << l) &&
+        ((mask3 >> k) & 1u))
+        return SBG_CODE3 + k;
+    return l;
 }
 
 int ensure_plan(sbg_ctx* c, int lgL) {
@@ -44,22 +51,42 @@ int ensure_plan(sbg_ctx* c, int lgL) {
     if (lp->lgL == lgL) return SBG_OK;
     LenPlan np;
     np.lgL = lgL;
+    np.L = code_len(lgL);
     if (lgL <= 12) {
         np.lgN1 = 0;
         np.lgN2 = lgL;
     } else {
         np.lgN2 = 12;
-        np.lgN1 = lgL - 12;
-        np.hi_n = 1 << (lgL - 13);
+        if (code_three(lgL)) {
+            np.m3 = code_lg(lgL) - 12;
+            np.lgN1 = 0;
+        } else {
+            np.lgN1 = lgL - 12;
+        }
+        np.hi_n = (int)(np.L >> 13);
         size_t lo_b = (size_t)SBG_NP * 8192 * sizeof(uint2);
         size_t hi_b = (size_t)SBG_NP * np.hi_n * sizeof(uint2);
         CK(cudaMalloc(&np.fs_lo_f, lo_b));
         CK(cudaMalloc(&np.fs_lo_i, lo_b));
         CK(cudaMalloc(&np.fs_hi_f, hi_b));
         CK(cudaMalloc(&np.fs_hi_i, hi_b));
+        if (np.m3 >= 0) {
+            size_t t3_b = (size_t)SBG_NP * (2 << np.m3) * sizeof(uint2);
+            CK(cudaMalloc(&np.t3_f, t3_b));
+            CK(cudaMalloc(&np.t3_i, t3_b));
+            for (int q = 0; q < SBG_NP; ++q) {     // cube roots of unity w_N1^M
+                const uint32_t p = kPrimes[q];
+                const uint32_t w = host_powmod(kGenerators[q], (p - 1) / 3, p);
+                const uint32_t wi = host_powmod(w, 2, p);
+                np.w3f[q] = w;
+                np.w3fs[q] = host_shoup(w, p);
+                np.w3i[q] = wi;
+                np.w3is[q] = host_shoup(wi, p);
+            }
+        }
         CK(gen_len_tables(&np, c->stream));
     }
-    for (int q = 0; q < SBG_NP; ++q) np.scale[q] = host_scale(lgL, q);
+    for (int q = 0; q < SBG_NP; ++q) np.scale[q] = host_scale(np.L, q);
     *lp = np;
     return SBG_OK;
 }
@@ -92,7 +119,7 @@ static int ensure_ws(sbg_ctx* c, size_t words, size_t flag_words) {
 static int run_conv(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, const uint64_t* bp,
                     int64_t bn, int sq, int lgL, int64_t cmin, int64_t cmax, int64_t off,
                     int64_t nout) {
-    if (lgL > SBG_MAX_LG) return SBG_EBAND;
+    if (lgL > SBG_NCODES || code_len(lgL) > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
     int st = ensure_plan(c, lgL);
     if (st) return st;
     st = ensure_ws(c, ws_words(lgL, sq), carry_flag_words(nout));
@@ -133,25 +160,25 @@ struct sbg_batch {
     int64_t count = 0;
 };
 
-static int job_shape(const sbg_job& j, int* lgL, int64_t* cmin, int64_t* cmax, int64_t* off,
-                     int64_t* nout, int* sq) {
+static int job_shape(const sbg_job& j, uint32_t mask3, int* lgL, int64_t* cmin, int64_t* cmax,
+                     int64_t* off, int64_t* nout, int* sq) {
     if (!j.rp || !j.ap || j.an <= 0) return SBG_EINVAL;
     switch (j.kind) {
         case SBG_JOB_MUL:
             if (!j.bp || j.bn <= 0) return SBG_EINVAL;
             if (j.an + j.bn - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
-            *lgL = conv_lg(j.an + j.bn - 1);
+            *lgL = conv_lg(j.an + j.bn - 1, mask3);
             *cmin = 0; *cmax = j.an + j.bn - 2; *off = 0; *nout = j.an + j.bn; *sq = 0;
             return SBG_OK;
         case SBG_JOB_SQR:
             if (2 * j.an - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
-            *lgL = conv_lg(2 * j.an - 1);
+            *lgL = conv_lg(2 * j.an - 1, mask3);
             *cmin = 0; *cmax = 2 * j.an - 2; *off = 0; *nout = 2 * j.an; *sq = 1;
             return SBG_OK;
         case SBG_JOB_MULMID:
             if (!j.bp || j.bn <= 0 || j.an < j.bn) return SBG_EINVAL;
             if (j.an > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
-            *lgL = conv_lg(j.an);
+            *lgL = conv_lg(j.an, mask3);
             *cmin = j.bn - 1; *cmax = j.an - 1; *off = j.bn - 1; *nout = j.an - j.bn + 3; *sq = 0;
             return SBG_OK;
         default: return SBG_EINVAL;
@@ -215,12 +242,12 @@ void UploadRing::release() {
 
 int enqueue_products(sbg_ctx* c, const sbg_job* jobs, int64_t count, uint32_t* err) {
     if (count <= 0) return SBG_OK;
-    std::vector<JobDesc> by_lg[SBG_MAX_LG + 1];
-    int64_t max_nout[SBG_MAX_LG + 1] = {};
+    std::vector<JobDesc> by_lg[SBG_NCODES + 1];
+    int64_t max_nout[SBG_NCODES + 1] = {};
     for (int64_t i = 0; i < count; ++i) {
         int lgL, sq;
         int64_t cmin, cmax, off, nout;
-        int st = job_shape(jobs[i], &lgL, &cmin, &cmax, &off, &nout, &sq);
+        int st = job_shape(jobs[i], c->len3_mask, &lgL, &cmin, &cmax, &off, &nout, &sq);
         if (st) return st;
         JobDesc d{};
         d.a = jobs[i].ap;
@@ -234,7 +261,7 @@ int enqueue_products(sbg_ctx* c, const sbg_job* jobs, int64_t count, uint32_t* e
         max_nout[lgL] = std::max(max_nout[lgL], nout);
     }
     size_t ws_total = 0, flag_total = 0;
-    for (int l = 0; l <= SBG_MAX_LG; ++l) {
+    for (int l = 0; l <= SBG_NCODES; ++l) {
         if (by_lg[l].empty()) continue;
         int st = ensure_plan(c, l);
         if (st) return st;
@@ -269,7 +296,12 @@ int enqueue_products(sbg_ctx* c, const sbg_job* jobs, int64_t count, uint32_t* e
     std::vector<Cls> cls;
     std::vector<JobDesc> all;
     all.reserve((size_t)count);
-    for (int l = SBG_MAX_LG; l >= 0; --l) {           // longest transforms first
+    int order[SBG_NCODES + 1];                        // longest transforms first
+    for (int l = 0; l <= SBG_NCODES; ++l) order[l] = l;
+    std::stable_sort(order, order + SBG_NCODES + 1,
+                     [](int x, int y) { return code_order_key(x) > code_order_key(y); });
+    for (int oi = 0; oi <= SBG_NCODES; ++oi) {
+        const int l = order[oi];
         if (by_lg[l].empty()) continue;
         const size_t fpj = ((size_t)crt_blocks(max_nout[l]) + 1 + 3) / 4 * 4;
         cls.push_back(Cls{l, (int)by_lg[l].size(), all.size(), fpj * by_lg[l].size(), fl});
@@ -361,8 +393,10 @@ void sbg_ctx_destroy(sbg_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (int l = 0; l <= SBG_MAX_LG; ++l) {
+    for (int l = 0; l <= SBG_NCODES; ++l) {
         LenPlan* lp = &c->plans[l];
+        cudaFree(lp->t3_f);
+        cudaFree(lp->t3_i);
         cudaFree(lp->fs_lo_f);
         cudaFree(lp->fs_lo_i);
         cudaFree(lp->fs_hi_f);
@@ -441,8 +475,10 @@ int sbg_ctx_reserve(sbg_ctx* c, int64_t total) {
     if (!c || total < 2) return SBG_EINVAL;
     if (total - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
     CK(cudaSetDevice(c->device));
-    int lg = conv_lg(total - 1);
-    for (int l = 4; l <= lg; ++l) {
+    int lg = conv_lg(total - 1, c->len3_mask);
+    for (int l = 4; l <= SBG_NCODES; ++l) {            // every length up to the largest
+        if (l > SBG_MAX_LG && l < SBG_CODE3 + SBG_THREE_MIN_LG) continue;
+        if (code_len(l) > code_len(lg)) continue;
         int st = ensure_plan(c, l);
         if (st) return st;
     }
@@ -457,7 +493,7 @@ int sbg_mul(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, const uint
     if (!c || !rp || !ap || !bp || an <= 0 || bn <= 0) return SBG_EINVAL;
     if (an + bn - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
     CK(cudaSetDevice(c->device));
-    int lgL = conv_lg(an + bn - 1);
+    int lgL = conv_lg(an + bn - 1, c->len3_mask);
     return run_conv(c, rp, ap, an, bp, bn, 0, lgL, 0, an + bn - 2, 0, an + bn);
 }
 
@@ -465,7 +501,7 @@ int sbg_sqr(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an) {
     if (!c || !rp || !ap || an <= 0) return SBG_EINVAL;
     if (2 * an - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
     CK(cudaSetDevice(c->device));
-    int lgL = conv_lg(2 * an - 1);
+    int lgL = conv_lg(2 * an - 1, c->len3_mask);
     return run_conv(c, rp, ap, an, ap, an, 1, lgL, 0, 2 * an - 2, 0, 2 * an);
 }
 
@@ -494,12 +530,12 @@ int sbg_batch_create(sbg_ctx* c, const sbg_job* jobs, int64_t count, sbg_batch**
     *out = nullptr;
     CK(cudaSetDevice(c->device));
     // bucket by transform length
-    std::vector<std::vector<JobDesc>> by_lg(SBG_MAX_LG + 1);
-    std::vector<int64_t> max_nout(SBG_MAX_LG + 1, 0);
+    std::vector<std::vector<JobDesc>> by_lg(SBG_NCODES + 1);
+    std::vector<int64_t> max_nout(SBG_NCODES + 1, 0);
     for (int64_t i = 0; i < count; ++i) {
         int lgL, sq;
         int64_t cmin, cmax, off, nout;
-        int st = job_shape(jobs[i], &lgL, &cmin, &cmax, &off, &nout, &sq);
+        int st = job_shape(jobs[i], c->len3_mask, &lgL, &cmin, &cmax, &off, &nout, &sq);
         if (st) return st;
         JobDesc d{};
         d.a = jobs[i].ap;
@@ -514,7 +550,7 @@ int sbg_batch_create(sbg_ctx* c, const sbg_job* jobs, int64_t count, sbg_batch**
     }
     // sizes: workspace, flags, descriptors -- one allocation
     size_t ws_total = 0, flag_total = 0, desc_total = 0;
-    for (int l = 0; l <= SBG_MAX_LG; ++l) {
+    for (int l = 0; l <= SBG_NCODES; ++l) {
         if (by_lg[l].empty()) continue;
         int st = ensure_plan(c, l);
         if (st) return st;
@@ -537,7 +573,7 @@ int sbg_batch_create(sbg_ctx* c, const sbg_job* jobs, int64_t count, sbg_batch**
     JobDesc* dd = (JobDesc*)(((uintptr_t)(fl + flag_total) + 255) & ~(uintptr_t)255);
     std::vector<JobDesc> host_all;
     host_all.reserve(desc_total);
-    for (int l = 0; l <= SBG_MAX_LG; ++l) {
+    for (int l = 0; l <= SBG_NCODES; ++l) {
         if (by_lg[l].empty()) continue;
         const size_t bpj = (size_t)crt_blocks(max_nout[l]);
         const size_t fpj = (bpj + 1 + 3) / 4 * 4;
@@ -560,7 +596,7 @@ int sbg_batch_create(sbg_ctx* c, const sbg_job* jobs, int64_t count, sbg_batch**
     // largest classes first: they start early on the forked streams
     std::stable_sort(b->classes.begin(), b->classes.end(),
                      [](const sbg_batch::Cls& x, const sbg_batch::Cls& y) {
-                         return ((int64_t)x.njobs << x.lgL) > ((int64_t)y.njobs << y.lgL);
+                         return (int64_t)x.njobs * code_len(x.lgL) > (int64_t)y.njobs * code_len(y.lgL);
                      });
     do {
         if ((st = cuda_fail(cudaMemcpy(dd, host_all.data(), host_all.size() * sizeof(JobDesc),
@@ -614,6 +650,65 @@ int sbg_batch_run(sbg_batch* b) {
 
 int64_t sbg_ctx_launches(sbg_ctx* c) { return c ? c->launches.load() : 0; }
 
+// For every size class k where a 3 * 2^k transform could replace 2^(k+2),
+// time one full product (an = bn = 3 * 2^(k-1), the largest of the class)
+// at both lengths on this context's stream and keep the faster.
+int sbg_ctx_autotune(sbg_ctx* c, double* times) {
+    if (!c) return SBG_EINVAL;
+    CK(cudaSetDevice(c->device));
+    const int kmax = SBG_MAX_LG - 2;
+    const int64_t nmax = (int64_t)3 << (kmax - 1);
+    uint64_t* buf = nullptr;
+    CK(cudaMalloc(&buf, (size_t)4 * nmax * 8));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int st = cuda_fail(cudaEventCreate(&e0), "event");
+    if (!st) st = cuda_fail(cudaEventCreate(&e1), "event");
+    if (!st) st = cuda_fail(cudaMemsetAsync(buf, 0x5a, (size_t)2 * nmax * 8, c->stream), "fill");
+    uint32_t mask = 0;
+    for (int k = SBG_THREE_MIN_LG; k <= kmax && !st; ++k) {
+        const int64_t n = (int64_t)3 << (k - 1);            // 2n - 1 = 3 * 2^k - 1 coefficients
+        float best[2] = {0.f, 0.f};
+        for (int v = 0; v < 2 && !st; ++v) {
+            const int code = v ? SBG_CODE3 + k : k + 2;
+            auto one = [&]() {
+                return run_conv(c, buf + 2 * nmax, buf, n, buf + nmax, n, 0, code, 0, 2 * n - 2, 0, 2 * n);
+            };
+            st = one();                                      // builds plan and workspace
+            float ms_min = 1e30f;
+            for (int rep = 0; rep < 3 && !st; ++rep) {
+                if ((st = cuda_fail(cudaEventRecord(e0, c->stream), "rec"))) break;
+                if ((st = one())) break;
+                if ((st = cuda_fail(cudaEventRecord(e1, c->stream), "rec"))) break;
+                if ((st = cuda_fail(cudaEventSynchronize(e1), "sync"))) break;
+                float ms = 0.f;
+                if ((st = cuda_fail(cudaEventElapsedTime(&ms, e0, e1), "elapsed"))) break;
+                ms_min = std::min(ms_min, ms);
+            }
+            best[v] = ms_min;
+        }
+        if (st) break;
+        if (times) {
+            times[2 * (k - SBG_THREE_MIN_LG)] = best[0];
+            times[2 * (k - SBG_THREE_MIN_LG) + 1] = best[1];
+        }
+        if (best[1] < best[0]) mask |= 1u << k;
+    }
+    if (!st) st = sbg_ctx_sync(c);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(buf);
+    if (!st) c->len3_mask = mask;
+    return st;
+}
+
+int sbg_ctx_set_len3_mask(sbg_ctx* c, uint32_t mask) {
+    if (!c) return SBG_EINVAL;
+    c->len3_mask = mask;
+    return SBG_OK;
+}
+
+uint32_t sbg_ctx_get_len3_mask(sbg_ctx* c) { return c ? c->len3_mask : 0u; }
+
 int sbg_mul_batch(sbg_ctx* c, const sbg_job* jobs, int64_t count) {
     if (!c || (count > 0 && !jobs) || count < 0) return SBG_EINVAL;
     CK(cudaSetDevice(c->device));
@@ -628,7 +723,7 @@ int sbg_mulmid(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, const u
     if (an > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
     CK(cudaSetDevice(c->device));
     // the wanted coefficients [bn-1, an-1] are untouched by wrap-around once L >= an
-    int lgL = conv_lg(an);
+    int lgL = conv_lg(an, c->len3_mask);
     return run_conv(c, rp, ap, an, bp, bn, 0, lgL, bn - 1, an - 1, bn - 1, an - bn + 3);
 }
 

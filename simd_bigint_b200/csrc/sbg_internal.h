@@ -13,6 +13,20 @@
 
 namespace sbg {
 
+// Transform lengths are identified by a code: c <= SBG_MAX_LG is L = 2^c,
+// c = SBG_CODE3 + k is L = 3 * 2^k (four-step only, k >= SBG_THREE_MIN_LG),
+// chosen when it is the smaller of the two lengths that hold a product.
+#define SBG_CODE3 32
+#define SBG_NCODES (SBG_CODE3 + SBG_MAX_LG)
+#define SBG_THREE_MIN_LG 16
+// k = 21 .. 23: where 3 * 2^k measured faster than 2^(k+2) on B200 (below,
+// the cross-CTA radix-3 exchange of the short columns costs more than the
+// quarter of the points it saves)
+#define SBG_LEN3_DEFAULT 0x00E00000u
+inline bool code_three(int c) { return c >= SBG_CODE3; }
+inline int code_lg(int c) { return c >= SBG_CODE3 ? c - SBG_CODE3 : c; }
+inline int64_t code_len(int c) { return (int64_t)(c >= SBG_CODE3 ? 3 : 1) << code_lg(c); }
+
 // A (w, shoup) pair as stored in device tables.
 struct ShoupPair {
     uint32_t w, ws;
@@ -31,8 +45,14 @@ struct CrtConst {
 // Per-transform-length plan: the four-step twiddle tables (device) and the
 // CRT scale 2^32 * L^-1 mod p (host-side Shoup pairs passed by value).
 struct LenPlan {
-    int lgL = -1;
-    int lgN1 = 0, lgN2 = 0;       // column / row sizes (lgN1 = 0: single-CTA)
+    int lgL = -1;                 // length code (see code_len)
+    int lgN1 = 0, lgN2 = 0;       // column / row sizes (lgN1 = 0: single-CTA); 3 * 2^m3 columns
+    int m3 = -1;                  //   rows when m3 >= 0 (L = 3 * 2^(m3 + 12))
+    int64_t L = 0;
+    uint2* t3_f = nullptr;        // [q][2^(m3+1)] w_N1^j, the radix-3 level's twiddles
+    uint2* t3_i = nullptr;
+    uint32_t w3f[SBG_NP] = {}, w3fs[SBG_NP] = {};   // cube roots of unity (forward)
+    uint32_t w3i[SBG_NP] = {}, w3is[SBG_NP] = {};   // and their inverses
     uint2* fs_lo_f = nullptr;     // [q][8192]      w_L^e, e < 2^13
     uint2* fs_hi_f = nullptr;     // [q][L >> 13]   w_L^(e << 13)
     uint2* fs_lo_i = nullptr;
@@ -49,6 +69,13 @@ struct FsTables {
 };
 
 struct ScaleArg {
+    uint32_t w[SBG_NP];
+    uint32_t ws[SBG_NP];
+};
+
+// radix-3 level of a 3 * 2^k transform: twiddle table + cube roots
+struct Radix3Arg {
+    const uint2* t3;        // + q * 2M
     uint32_t w[SBG_NP];
     uint32_t ws[SBG_NP];
 };
@@ -102,7 +129,7 @@ uint32_t host_powmod(uint64_t a, uint64_t e, uint32_t p);
 uint32_t host_shoup(uint32_t w, uint32_t p);
 void host_prime_consts(PrimeConst out[SBG_NP]);
 void host_crt_consts(CrtConst* out);
-ShoupPair host_scale(int lgL, int q);
+ShoupPair host_scale(int64_t L, int q);
 
 // ---- launchers (sbg_kernels.cu) ----
 cudaError_t upload_constants(cudaStream_t st);
@@ -112,7 +139,8 @@ cudaError_t gen_master_tables(uint2* tw_f, uint2* tw_i, cudaStream_t st);
 cudaError_t gen_len_tables(LenPlan* lp, cudaStream_t st);
 
 // Whole product through the transform pipeline.  Workspace `ws` must hold
-// ws_words(lgL) u32.  `err` is a device word that receives sticky error bits.
+// ws_words(code) u32.  `err` is a device word that receives sticky error bits.
+// Every `lgL` below is a length code.
 size_t ws_words(int lgL, int sq);
 cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_t bn, int sq,
                         int lgL, const LenPlan* lp, const uint2* tw_f, const uint2* tw_i,
@@ -211,6 +239,8 @@ struct UploadRing {
 // kernel launches of one product (or one length class of a batch): the
 // fused single-CTA transform or the three four-step transforms, then CRT+carry
 inline int class_launches(int lgL) { return lgL <= SBG_SMALL_MAX_LG ? 2 : 4; }
+// codes in the order batches launch them: longest transforms first
+inline int64_t code_order_key(int c) { return code_len(c); }
 
 }  // namespace sbg
 
@@ -220,7 +250,7 @@ struct sbg_ctx {
     cudaStream_t stream = nullptr;
     uint2* tw_f = nullptr;          // master tables [q][2^12]
     uint2* tw_i = nullptr;
-    sbg::LenPlan plans[SBG_MAX_LG + 1];
+    sbg::LenPlan plans[SBG_NCODES + 1];
     uint32_t* ws = nullptr;         // transform workspace (u32 words)
     size_t ws_cap = 0;
     uint32_t* flags = nullptr;      // carry look-back flags
@@ -244,6 +274,9 @@ struct sbg_ctx {
     uint32_t* derr = nullptr;
     std::atomic<int64_t> launches{0};   // kernels queued by this context (diagnostics)
     int stream_priority = 0;            // priority of the streams the context creates itself
+    // 3 * 2^k transform lengths in use (bit k), by measurement where
+    // sbg_ctx_autotune ran, else the default measured on B200
+    uint32_t len3_mask = SBG_LEN3_DEFAULT;
     // host-operand products (sbg_mul_host): two staging slots so that one
     // product's download overlaps the next one's upload and compute
     struct HostSlot {
@@ -259,7 +292,7 @@ struct sbg_ctx {
 namespace sbg {
 int cuda_fail(cudaError_t e, const char* where);
 int lg_ceil(int64_t n);
-int conv_lg(int64_t need);
+int conv_lg(int64_t need, uint32_t mask3);
 int ensure_plan(sbg_ctx* c, int lgL);
 // Newton reciprocals of `count` normalised divisors (device pointers), all
 // recursion levels in lockstep; synchronous on the context stream.

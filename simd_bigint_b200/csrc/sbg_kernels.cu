@@ -612,6 +612,234 @@ __global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col_inv_b(const JobDe
     col_inv_body<LGN1>(rest % SBG_NP, rest / SBG_NP, slab, J.ws, twi);
 }
 
+// ------------------------------------------------------------------------
+// Columns of 3 * 2^m rows (transform lengths L = 3 * 2^(m + 12)).
+//
+// DIF: a radix-3 level over the thirds (rows r, r + M, r + 2M, M = 2^m; the
+// second and third outputs twiddled by w_N1^r and w_N1^2r), then a 2^m-point
+// DIF in each third, so row t M + j ends up holding frequency 3 bitrev(j) + t.
+// A cluster of C = 3 * 2^c CTAs (one slab of M / 2^c <= 2^10 rows each, same
+// tile geometry as the power-of-two columns) runs the radix-3 level -- and,
+// for c = 1, the top radix-2 level of each third -- in registers across the
+// slabs, exchanging through distributed shared memory, then each CTA
+// transforms its slab.  The inverse is the exact reverse (DIT, inverse
+// twiddles and cube root); its factor 3 is part of the CRT scale 1/L.
+//   radix-3 DIF:  y0 = a + b + c, y1 = (a - c + w(b - c)) t, y2 = (a - b - w(b - c)) t^2
+// with w the cube root of unity w_N1^M (w^2 = -1 - w).
+// ------------------------------------------------------------------------
+__device__ __forceinline__ void r3_dif(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t w3,
+                                       uint32_t w3s, uint2 t1, uint2 t2, uint32_t p) {
+    const uint32_t e = mul_shoup(sub_mod(b, c, p), w3, w3s, p);
+    const uint32_t y0 = add_mod(a, add_mod(b, c, p), p);
+    const uint32_t y1 = add_mod(sub_mod(a, c, p), e, p);
+    const uint32_t y2 = sub_mod(sub_mod(a, b, p), e, p);
+    a = y0;
+    b = mul_shoup(y1, t1.x, t1.y, p);
+    c = mul_shoup(y2, t2.x, t2.y, p);
+}
+
+// exact reverse of r3_dif (inverse twiddles t1 = w_N1^-r, t2 = w_N1^-2r and
+// inverse cube root): returns 3 (a, b, c)
+__device__ __forceinline__ void r3_dit(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t w3i,
+                                       uint32_t w3is, uint2 t1, uint2 t2, uint32_t p) {
+    const uint32_t y1 = mul_shoup(b, t1.x, t1.y, p);
+    const uint32_t y2 = mul_shoup(c, t2.x, t2.y, p);
+    const uint32_t e = mul_shoup(sub_mod(y1, y2, p), w3i, w3is, p);
+    const uint32_t x0 = add_mod(a, add_mod(y1, y2, p), p);
+    const uint32_t x1 = add_mod(sub_mod(a, y2, p), e, p);
+    const uint32_t x2 = sub_mod(sub_mod(a, y1, p), e, p);
+    a = x0;
+    b = x1;
+    c = x2;
+}
+
+__host__ __device__ constexpr int col3_lgs(int m) { return m < SBG_COL_SLAB_LG ? m : SBG_COL_SLAB_LG; }
+__host__ __device__ constexpr int col3_lgc(int m) { return m - col3_lgs(m); }
+__host__ __device__ constexpr int col3_csize(int m) { return 3 << col3_lgc(m); }
+__host__ __device__ constexpr bool col3_lanes(int m) { return col3_lgs(m) <= SBG_COL_LANE_MAX_LG; }
+__host__ __device__ constexpr int col3_lgw(int m) { return col_lgw_of(col3_lanes(m), col3_lgs(m)); }
+__host__ __device__ constexpr int col3_smem_bytes(int m) {
+    return (1 << col3_lgw(m)) * col_ld_of(col3_lanes(m), col3_lgs(m)) * 4;
+}
+__host__ __device__ constexpr int col3_ntiles(int m) { return 1 << (SBG_ROW_LG - col3_lgw(m)); }
+#define SBG_COL3_CASES(X) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11)
+
+// shared-memory address of (column, row) in a slab's planes
+template <bool LANES, int LD>
+__device__ __forceinline__ int slab_addr(int col, int r) {
+    return col * LD + (LANES ? r : pad_idx(r));
+}
+
+// cross-slab levels, forward: this CTA's share of rows r of a slab (split
+// evenly among the C CTAs), all columns; rows r + MS t of the whole column
+template <int M3>
+__device__ __forceinline__ void col3_cross_fwd(uint32_t* sm, const uint64_t* __restrict__ X, int64_t xn,
+                                               int c0, int slab, const uint2* __restrict__ tw,
+                                               const uint2* __restrict__ t3, uint32_t w3, uint32_t w3s,
+                                               const PrimeConst& pc) {
+    constexpr int LGS = col3_lgs(M3);
+    constexpr int MS = 1 << LGS;
+    constexpr int G = 1 << col3_lgc(M3);          // slabs per third
+    constexpr int C = 3 * G;
+    constexpr bool LANES = col3_lanes(M3);
+    constexpr int LGW = col3_lgw(M3);
+    constexpr int LD = col_ld_of(LANES, LGS);
+    const int r_lo = (slab * MS) / C, r_hi = ((slab + 1) * MS) / C;
+    const int items = (r_hi - r_lo) << LGW;
+    cg::cluster_group cl = cg::this_cluster();
+    for (int gid = threadIdx.x; gid < items; gid += COL_THREADS) {
+        const int col = gid & ((1 << LGW) - 1);
+        const int r = r_lo + (gid >> LGW);
+        uint32_t x[C];
+        const int64_t n0 = ((int64_t)r << SBG_ROW_LG) + c0 + col;
+#pragma unroll
+        for (int t = 0; t < C; ++t) x[t] = load_limb(X, xn, n0 + ((int64_t)(MS * t) << SBG_ROW_LG), pc);
+#pragma unroll
+        for (int u = 0; u < G; ++u) {
+            const int rr = r + u * MS;                 // row within a third
+            r3_dif(x[u], x[u + G], x[u + 2 * G], w3, w3s, __ldg(&t3[rr]), __ldg(&t3[2 * rr]), pc.p);
+        }
+        if constexpr (G == 2) {                        // top radix-2 level of each third
+            const uint2 w = __ldg(&tw[tw_idx(M3, r)]);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) bfly_gs(x[2 * k], x[2 * k + 1], w.x, w.y, pc.p);
+        }
+        const int a = slab_addr<LANES, LD>(col, r);
+#pragma unroll
+        for (int t = 0; t < C; ++t) cl.map_shared_rank(sm, t)[a] = x[t];
+    }
+}
+
+template <int M3>
+__device__ __forceinline__ void col3_cross_inv(uint32_t* sm, uint32_t* __restrict__ Y, int c0, int slab,
+                                               const uint2* __restrict__ tw, const uint2* __restrict__ t3,
+                                               uint32_t w3, uint32_t w3s, const PrimeConst& pc) {
+    constexpr int LGS = col3_lgs(M3);
+    constexpr int MS = 1 << LGS;
+    constexpr int G = 1 << col3_lgc(M3);
+    constexpr int C = 3 * G;
+    constexpr bool LANES = col3_lanes(M3);
+    constexpr int LGW = col3_lgw(M3);
+    constexpr int LD = col_ld_of(LANES, LGS);
+    const int r_lo = (slab * MS) / C, r_hi = ((slab + 1) * MS) / C;
+    const int items = (r_hi - r_lo) << LGW;
+    cg::cluster_group cl = cg::this_cluster();
+    for (int gid = threadIdx.x; gid < items; gid += COL_THREADS) {
+        const int col = gid & ((1 << LGW) - 1);
+        const int r = r_lo + (gid >> LGW);
+        uint32_t x[C];
+        const int a = slab_addr<LANES, LD>(col, r);
+#pragma unroll
+        for (int t = 0; t < C; ++t) x[t] = cl.map_shared_rank(sm, t)[a];
+        if constexpr (G == 2) {
+            const uint2 w = __ldg(&tw[tw_idx(M3, r)]);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) bfly_ct(x[2 * k], x[2 * k + 1], w.x, w.y, pc.p);
+        }
+#pragma unroll
+        for (int u = 0; u < G; ++u) {
+            const int rr = r + u * MS;
+            r3_dit(x[u], x[u + G], x[u + 2 * G], w3, w3s, __ldg(&t3[rr]), __ldg(&t3[2 * rr]), pc.p);
+        }
+        const int64_t n0 = ((int64_t)r << SBG_ROW_LG) + c0 + col;
+#pragma unroll
+        for (int t = 0; t < C; ++t) Y[n0 + ((int64_t)(MS * t) << SBG_ROW_LG)] = x[t];
+    }
+}
+
+template <int M3>
+__device__ __forceinline__ void col3_fwd_body(int q, int tile, int slab, int op,
+                                              const uint64_t* __restrict__ a, int64_t an,
+                                              const uint64_t* __restrict__ b, int64_t bn,
+                                              const uint2* __restrict__ twf, const Radix3Arg& r3,
+                                              uint32_t* __restrict__ YA, uint32_t* __restrict__ YB) {
+    extern __shared__ uint32_t sm[];
+    constexpr int LGS = col3_lgs(M3);
+    constexpr size_t L = (size_t)3 << (M3 + SBG_ROW_LG);
+    const uint64_t* X = op ? b : a;
+    const int64_t xn = op ? bn : an;
+    uint32_t* Y = (op ? YB : YA) + (size_t)q * L;
+    const PrimeConst pc = c_pr[q];
+    const uint2* tw = twf + (size_t)q * SBG_TW_N;
+    const int c0 = tile << col3_lgw(M3);
+    cluster_barrier<false>();           // every CTA of the cluster is running
+    col3_cross_fwd<M3>(sm, X, xn, c0, slab, tw, r3.t3 + ((size_t)q << (M3 + 1)), r3.w[q], r3.ws[q], pc);
+    cluster_barrier<true>();            // all slabs complete in shared memory
+    col_slab_fwd<col3_lanes(M3), LGS, false, true>(sm, X, xn, Y, c0, slab << LGS, tw, pc);
+}
+
+template <int M3>
+__device__ __forceinline__ void col3_inv_body(int q, int tile, int slab, uint32_t* __restrict__ YA,
+                                              const uint2* __restrict__ twi, const Radix3Arg& r3) {
+    extern __shared__ uint32_t sm[];
+    constexpr int LGS = col3_lgs(M3);
+    constexpr size_t L = (size_t)3 << (M3 + SBG_ROW_LG);
+    uint32_t* Y = YA + (size_t)q * L;
+    const PrimeConst pc = c_pr[q];
+    const uint2* tw = twi + (size_t)q * SBG_TW_N;
+    const int c0 = tile << col3_lgw(M3);
+    col_slab_inv<col3_lanes(M3), LGS, true, false>(sm, Y, c0, slab << LGS, tw, pc);
+    cluster_barrier<true>();            // all slabs complete in shared memory
+    col3_cross_inv<M3>(sm, Y, c0, slab, tw, r3.t3 + ((size_t)q << (M3 + 1)), r3.w[q], r3.ws[q], pc);
+    cluster_barrier<false>();           // peers read this CTA's slab until here
+}
+
+// blocks: slab fastest (a cluster), then prime, tile, operand
+template <int M3>
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3_fwd(const uint64_t* __restrict__ a, int64_t an,
+                                                                  const uint64_t* __restrict__ b, int64_t bn,
+                                                                  const uint2* __restrict__ twf, Radix3Arg r3,
+                                                                  uint32_t* __restrict__ YA,
+                                                                  uint32_t* __restrict__ YB) {
+    constexpr int C = col3_csize(M3);
+    constexpr int NTILES = col3_ntiles(M3);
+    const int slab = blockIdx.x % C;
+    int rest = blockIdx.x / C;
+    const int q = rest % SBG_NP;
+    rest /= SBG_NP;
+    col3_fwd_body<M3>(q, rest % NTILES, slab, rest / NTILES, a, an, b, bn, twf, r3, YA, YB);
+}
+
+template <int M3>
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3_fwd_b(const JobDesc* __restrict__ jobs,
+                                                                    const uint2* __restrict__ twf, Radix3Arg r3) {
+    constexpr int C = col3_csize(M3);
+    constexpr int NTILES = col3_ntiles(M3);
+    constexpr int PER_JOB = SBG_NP * 2 * NTILES * C;
+    constexpr size_t L = (size_t)3 << (M3 + SBG_ROW_LG);
+    const JobDesc& J = jobs[blockIdx.x / PER_JOB];
+    const int r = blockIdx.x % PER_JOB;
+    const int slab = r % C;
+    int rest = r / C;
+    const int q = rest % SBG_NP;
+    rest /= SBG_NP;
+    const int op = rest / NTILES;
+    if (op && J.sq) return;             // whole clusters together
+    col3_fwd_body<M3>(q, rest % NTILES, slab, op, J.a, J.an, J.b, J.bn, twf, r3, J.ws, J.ws + SBG_NP * L);
+}
+
+template <int M3>
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3_inv(uint32_t* __restrict__ YA,
+                                                                  const uint2* __restrict__ twi, Radix3Arg r3) {
+    constexpr int C = col3_csize(M3);
+    const int slab = blockIdx.x % C;
+    const int rest = blockIdx.x / C;
+    col3_inv_body<M3>(rest % SBG_NP, rest / SBG_NP, slab, YA, twi, r3);
+}
+
+template <int M3>
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3_inv_b(const JobDesc* __restrict__ jobs,
+                                                                    const uint2* __restrict__ twi, Radix3Arg r3) {
+    constexpr int C = col3_csize(M3);
+    constexpr int NTILES = col3_ntiles(M3);
+    constexpr int PER_JOB = SBG_NP * NTILES * C;
+    const JobDesc& J = jobs[blockIdx.x / PER_JOB];
+    const int r = blockIdx.x % PER_JOB;
+    const int slab = r % C;
+    const int rest = r / C;
+    col3_inv_body<M3>(rest % SBG_NP, rest / SBG_NP, slab, J.ws, twi, r3);
+}
+
 // K2: one row of N2 = 2^12 points for one prime, 256 threads.
 //   P1  global -> four-step twiddle -> DIF levels 1-4 (A and B) -> smem
 //   P2  DIF levels 5-8 (A and B)
@@ -626,7 +854,7 @@ __global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col_inv_b(const JobDe
 #define ROW_MINB 4                // resident CTAs per SM the register budget is set for
 #endif
 __device__ __forceinline__ void row_body(int q, int row, uint32_t* __restrict__ YA,
-                                         const uint32_t* __restrict__ YB, int sq, int lgN1,
+                                         const uint32_t* __restrict__ YB, int sq, int lgN1, int m3,
                                          const FsTables& fsf, const FsTables& fsi,
                                          const ScaleArg& sc, const uint2* __restrict__ twf,
                                          const uint2* __restrict__ twi) {
@@ -637,14 +865,17 @@ __device__ __forceinline__ void row_body(int q, int row, uint32_t* __restrict__ 
     const int tid = threadIdx.x;
     const PrimeConst pc = c_pr[q];
     const uint32_t p = pc.p;
-    const uint32_t Lmask = (1u << (lgN1 + ROW_LG)) - 1u;
-    const size_t base = ((size_t)q << (lgN1 + ROW_LG)) + ((size_t)row << ROW_LG);
+    // rows: 2^lgN1, or 3 * 2^m3 (m3 >= 0); the column DIF left row p holding
+    // frequency bitrev(p) resp. 3 bitrev(p mod 2^m3) + p / 2^m3
+    const size_t n1 = m3 >= 0 ? (size_t)3 << m3 : (size_t)1 << lgN1;
+    const size_t base = ((size_t)q * n1 << ROW_LG) + ((size_t)row << ROW_LG);
     const uint2* tf = twf + (size_t)q * SBG_TW_N;
     const uint2* ti = twi + (size_t)q * SBG_TW_N;
-    const uint32_t k1 = bitrev((uint32_t)row, lgN1);
+    const uint32_t k1 = m3 >= 0 ? 3u * bitrev((uint32_t)row & ((1u << m3) - 1u), m3) + ((uint32_t)row >> m3)
+                                : bitrev((uint32_t)row, lgN1);
     // four-step twiddles: w_L^(k1 (tid + 256 t)) = b * s^t
     if (tid < 16) {
-        uint32_t e = (k1 * 256u * (uint32_t)tid) & Lmask;
+        uint32_t e = k1 * 256u * (uint32_t)tid;          // < L: no reduction
         uint32_t v = fs_value(fsf, q, e, p);
         s_f[tid] = make_uint2(v, shoup_fast(v, pc));
         uint32_t vi = mul_shoup(fs_value(fsi, q, e, p), sc.w[q], sc.ws[q], p);
@@ -746,23 +977,25 @@ __device__ __forceinline__ void row_body(int q, int row, uint32_t* __restrict__ 
 
 __global__ void __launch_bounds__(256, ROW_MINB) k_row12(uint32_t* __restrict__ YA,
                                                   const uint32_t* __restrict__ YB, int sq,
-                                                  int lgN1, FsTables fsf, FsTables fsi, ScaleArg sc,
-                                                  const uint2* __restrict__ twf,
+                                                  int lgN1, int m3, FsTables fsf, FsTables fsi,
+                                                  ScaleArg sc, const uint2* __restrict__ twf,
                                                   const uint2* __restrict__ twi) {
-    row_body(blockIdx.x >> lgN1, blockIdx.x & ((1 << lgN1) - 1), YA, YB, sq, lgN1, fsf, fsi, sc,
-             twf, twi);
+    const int n1 = m3 >= 0 ? 3 << m3 : 1 << lgN1;
+    const int q = blockIdx.x / n1;
+    row_body(q, blockIdx.x - q * n1, YA, YB, sq, lgN1, m3, fsf, fsi, sc, twf, twi);
 }
 
 // batched: blocks (job, prime, row), job slowest
 __global__ void __launch_bounds__(256, ROW_MINB) k_row12_b(const JobDesc* __restrict__ jobs, int lgN1,
-                                                    FsTables fsf, FsTables fsi, ScaleArg sc,
+                                                    int m3, FsTables fsf, FsTables fsi, ScaleArg sc,
                                                     const uint2* __restrict__ twf,
                                                     const uint2* __restrict__ twi) {
-    const int per_job = SBG_NP << lgN1;
+    const int n1 = m3 >= 0 ? 3 << m3 : 1 << lgN1;
+    const int per_job = SBG_NP * n1;
     const JobDesc& J = jobs[blockIdx.x / per_job];
     const int r = blockIdx.x % per_job;
-    uint32_t* YB = J.ws + ((size_t)SBG_NP << (lgN1 + ROW_LG));
-    row_body(r >> lgN1, r & ((1 << lgN1) - 1), J.ws, YB, J.sq, lgN1, fsf, fsi, sc, twf, twi);
+    uint32_t* YB = J.ws + (size_t)SBG_NP * n1 * ROW_N;
+    row_body(r / n1, r % n1, J.ws, YB, J.sq, lgN1, m3, fsf, fsi, sc, twf, twi);
 }
 
 // ------------------------------------------------------------------------
@@ -851,13 +1084,12 @@ __device__ __forceinline__ uint32_t gp_compose(uint32_t left, uint32_t right) {
     return (gr | (pr & gl)) | ((pr & pl) << 1);
 }
 
-__device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restrict__ R, int lgL,
+__device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restrict__ R, int64_t L,
                                          int64_t cmin, int64_t cmax, int64_t off,
                                          uint64_t* __restrict__ out, int64_t nout,
                                          uint32_t* flags, uint32_t* err) {
     __shared__ uint32_t s_warp[CRT_T / 32];
     __shared__ uint32_t s_cin;
-    const int64_t L = (int64_t)1 << lgL;
     const int64_t m0 = (int64_t)bid * CRT_BLK + (int64_t)threadIdx.x * CRT_PER;
     const int64_t j0 = m0 + off;
     // residues of coefficients j0-4 .. j0+15 arrive in 5 chunks of 4: one
@@ -1037,19 +1269,19 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
 
 // Block order comes from an atomic ticket (flags[0]), not blockIdx, so every
 // block's look-back predecessors were scheduled before it.
-__global__ void __launch_bounds__(CRT_T) k_crt_carry(const uint32_t* __restrict__ R, int lgL,
+__global__ void __launch_bounds__(CRT_T) k_crt_carry(const uint32_t* __restrict__ R, int64_t L,
                                                      int64_t cmin, int64_t cmax, int64_t off,
                                                      uint64_t* __restrict__ out, int64_t nout,
                                                      uint32_t* flags, uint32_t* err) {
     __shared__ uint32_t s_bid;
     if (threadIdx.x == 0) s_bid = atomicAdd(&flags[0], 1u);
     __syncthreads();
-    crt_body(s_bid, R, lgL, cmin, cmax, off, out, nout, flags, err);
+    crt_body(s_bid, R, L, cmin, cmax, off, out, nout, flags, err);
 }
 
 // batched: blocks_per_job CTAs per job (enough for the longest output of the
 // launch); each takes a ticket on its own job's counter, surplus ones exit.
-__global__ void __launch_bounds__(CRT_T) k_crt_carry_b(const JobDesc* __restrict__ jobs, int lgL,
+__global__ void __launch_bounds__(CRT_T) k_crt_carry_b(const JobDesc* __restrict__ jobs, int64_t L,
                                                        int blocks_per_job, uint32_t* err) {
     __shared__ uint32_t s_bid;
     const JobDesc& J = jobs[blockIdx.x / blocks_per_job];
@@ -1057,7 +1289,7 @@ __global__ void __launch_bounds__(CRT_T) k_crt_carry_b(const JobDesc* __restrict
     __syncthreads();
     const int64_t need = (J.nout + 1 + CRT_BLK - 1) / CRT_BLK;
     if ((int64_t)s_bid >= need) return;
-    crt_body(s_bid, J.ws, lgL, J.cmin, J.cmax, J.off, J.out, J.nout, J.flags, err);
+    crt_body(s_bid, J.ws, L, J.cmin, J.cmax, J.off, J.out, J.nout, J.flags, err);
 }
 
 // ------------------------------------------------------------------------
@@ -1112,12 +1344,13 @@ cudaError_t upload_constants(cudaStream_t st) {
     return cudaMemcpyToSymbolAsync(c_crt, &cc, sizeof(cc), 0, cudaMemcpyHostToDevice, st);
 }
 
-static cudaError_t gen_table(uint2* out, int n, int lgRoot, bool inverse, uint32_t stride,
+// roots of order `order` (a divisor of every p - 1: 2^a or 3 * 2^a, a <= 25)
+static cudaError_t gen_table(uint2* out, int n, int64_t order, bool inverse, uint32_t stride,
                              cudaStream_t st, bool per_resolution = false) {
     uint32_t roots[SBG_NP];
     for (int q = 0; q < SBG_NP; ++q) {
         uint32_t p = kPrimes[q];
-        uint32_t w = host_powmod(kGenerators[q], (p - 1) >> lgRoot, p);
+        uint32_t w = host_powmod(kGenerators[q], (p - 1) / (uint64_t)order, p);
         if (inverse) w = host_powmod(w, p - 2, p);
         roots[q] = w;
     }
@@ -1140,51 +1373,72 @@ static cudaError_t gen_table(uint2* out, int n, int lgRoot, bool inverse, uint32
 size_t master_table_entries() { return (size_t)SBG_NP * SBG_TW_N; }
 
 cudaError_t gen_master_tables(uint2* tw_f, uint2* tw_i, cudaStream_t st) {
-    cudaError_t e = gen_table(tw_f, SBG_TW_N, SBG_TW_LG, false, 1, st, true);
+    cudaError_t e = gen_table(tw_f, SBG_TW_N, SBG_TW_N, false, 1, st, true);
     if (e != cudaSuccess) return e;
-    return gen_table(tw_i, SBG_TW_N, SBG_TW_LG, true, 1, st, true);
+    return gen_table(tw_i, SBG_TW_N, SBG_TW_N, true, 1, st, true);
 }
 
 cudaError_t gen_len_tables(LenPlan* lp, cudaStream_t st) {
     // lo: w_L^e for e < 2^13; hi: w_L^(e * 2^13) for e < L / 2^13
-    cudaError_t e = gen_table(lp->fs_lo_f, SBG_FS_LO_N, lp->lgL, false, 1, st);
-    if (e == cudaSuccess) e = gen_table(lp->fs_lo_i, SBG_FS_LO_N, lp->lgL, true, 1, st);
+    cudaError_t e = gen_table(lp->fs_lo_f, SBG_FS_LO_N, lp->L, false, 1, st);
+    if (e == cudaSuccess) e = gen_table(lp->fs_lo_i, SBG_FS_LO_N, lp->L, true, 1, st);
     if (e == cudaSuccess)
-        e = gen_table(lp->fs_hi_f, lp->hi_n, lp->lgL, false, SBG_FS_LO_N, st);
+        e = gen_table(lp->fs_hi_f, lp->hi_n, lp->L, false, SBG_FS_LO_N, st);
     if (e == cudaSuccess)
-        e = gen_table(lp->fs_hi_i, lp->hi_n, lp->lgL, true, SBG_FS_LO_N, st);
+        e = gen_table(lp->fs_hi_i, lp->hi_n, lp->L, true, SBG_FS_LO_N, st);
+    // radix-3 level: w_N1^j, j < 2M, N1 = 3M rows
+    if (e == cudaSuccess && lp->m3 >= 0) {
+        const int64_t n1 = (int64_t)3 << lp->m3;
+        e = gen_table(lp->t3_f, 2 << lp->m3, n1, false, 1, st);
+        if (e == cudaSuccess) e = gen_table(lp->t3_i, 2 << lp->m3, n1, true, 1, st);
+    }
     return e;
 }
 
 size_t ws_words(int lgL, int sq) {
-    size_t L = (size_t)1 << lgL;
+    size_t L = (size_t)code_len(lgL);
     return (sq ? 1 : 2) * SBG_NP * L;
 }
 
-// Column kernels: 512 threads, dynamic shared memory, and a cluster of
-// 2^col_lgc CTAs when the columns span several slabs.
+// Column kernels: COL_THREADS threads, dynamic shared memory, and a
+// cluster of `cluster` CTAs when a column spans several slabs.
 template <typename... KArgs, typename... Args>
-static cudaError_t launch_col(void (*kern)(KArgs...), int lgN1, int64_t blocks, cudaStream_t st,
-                              Args... args) {
+static cudaError_t launch_colx(void (*kern)(KArgs...), int64_t blocks, int smem, int cluster,
+                               cudaStream_t st, Args... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)blocks, 1, 1);
     cfg.blockDim = dim3(COL_THREADS, 1, 1);
-    cfg.dynamicSmemBytes = (size_t)col_smem_bytes(lgN1);
+    cfg.dynamicSmemBytes = (size_t)smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = 1u << col_lgc(lgN1);
+    attr[0].val.clusterDim.x = (unsigned)cluster;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = col_lgc(lgN1) > 0 ? 1 : 0;
+    cfg.numAttrs = cluster > 1 ? 1 : 0;
     return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_col(void (*kern)(KArgs...), int lgN1, int64_t blocks, cudaStream_t st,
+                              Args... args) {
+    return launch_colx(kern, blocks, col_smem_bytes(lgN1), 1 << col_lgc(lgN1), st, args...);
+}
+
+static Radix3Arg radix3_arg(const LenPlan* lp, bool inverse) {
+    Radix3Arg r{};
+    r.t3 = inverse ? lp->t3_i : lp->t3_f;
+    for (int q = 0; q < SBG_NP; ++q) {
+        r.w[q] = inverse ? lp->w3i[q] : lp->w3f[q];
+        r.ws[q] = inverse ? lp->w3is[q] : lp->w3fs[q];
+    }
+    return r;
 }
 
 cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_t bn, int sq,
                         int lgL, const LenPlan* lp, const uint2* tw_f, const uint2* tw_i,
                         uint32_t* ws, cudaStream_t st, KTimer* kt) {
-    const size_t L = (size_t)1 << lgL;
+    const size_t L = (size_t)code_len(lgL);
     uint32_t* YA = ws;
     uint32_t* YB = ws + SBG_NP * L;
     ScaleArg sc;
@@ -1199,12 +1453,47 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
         KT_END(kt, KID_SMALL, st);
         return cudaGetLastError();
     }
-    const int lgN1 = lp->lgN1;   // rows: 2^lgN1, columns: 2^12
+    const int lgN1 = lp->lgN1;   // rows: 2^lgN1 (or 3 * 2^m3), columns: 2^12
+    const int m3 = lp->m3;
     FsTables fsf{lp->fs_lo_f, lp->fs_hi_f, lp->hi_n};
     FsTables fsi{lp->fs_lo_i, lp->fs_hi_i, lp->hi_n};
     const int nops = sq ? 1 : 2;
-    const int64_t col_blocks = ((int64_t)col_ntiles(lgN1) * SBG_NP) << col_lgc(lgN1);
     cudaError_t e = cudaSuccess;
+    if (m3 >= 0) {
+        const Radix3Arg r3f = radix3_arg(lp, false), r3i = radix3_arg(lp, true);
+        KT_BEGIN(kt, KID_COL_FWD, st);
+        switch (m3) {
+#define SBG_LAUNCH_F3(n)                                                                          \
+    case n:                                                                                       \
+        e = launch_colx(k_col3_fwd<n>, (int64_t)nops * col3_ntiles(n) * SBG_NP * col3_csize(n),    \
+                        col3_smem_bytes(n), col3_csize(n), st, a, an, b, bn, tw_f, r3f, YA, YB); \
+        break;
+            SBG_COL3_CASES(SBG_LAUNCH_F3)
+#undef SBG_LAUNCH_F3
+            default: return cudaErrorInvalidValue;
+        }
+        KT_END(kt, KID_COL_FWD, st);
+        if (e != cudaSuccess) return e;
+        KT_BEGIN(kt, KID_ROW, st);
+        k_row12<<<(3 << m3) * SBG_NP, 256, 0, st>>>(YA, YB, sq, 0, m3, fsf, fsi, sc, tw_f, tw_i);
+        KT_END(kt, KID_ROW, st);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        KT_BEGIN(kt, KID_COL_INV, st);
+        switch (m3) {
+#define SBG_LAUNCH_I3(n)                                                                             \
+    case n:                                                                                          \
+        e = launch_colx(k_col3_inv<n>, (int64_t)col3_ntiles(n) * SBG_NP * col3_csize(n),               \
+                        col3_smem_bytes(n), col3_csize(n), st, YA, tw_i, r3i);                        \
+        break;
+            SBG_COL3_CASES(SBG_LAUNCH_I3)
+#undef SBG_LAUNCH_I3
+            default: return cudaErrorInvalidValue;
+        }
+        KT_END(kt, KID_COL_INV, st);
+        if (e != cudaSuccess) return e;
+        return cudaGetLastError();
+    }
+    const int64_t col_blocks = ((int64_t)col_ntiles(lgN1) * SBG_NP) << col_lgc(lgN1);
     KT_BEGIN(kt, KID_COL_FWD, st);
     switch (lgN1) {
 #define SBG_LAUNCH_F(n)                                                                      \
@@ -1220,7 +1509,7 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     KT_BEGIN(kt, KID_ROW, st);
-    k_row12<<<(1 << lgN1) * SBG_NP, 256, 0, st>>>(YA, YB, sq, lgN1, fsf, fsi, sc, tw_f, tw_i);
+    k_row12<<<(1 << lgN1) * SBG_NP, 256, 0, st>>>(YA, YB, sq, lgN1, -1, fsf, fsi, sc, tw_f, tw_i);
     KT_END(kt, KID_ROW, st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -1255,6 +1544,34 @@ cudaError_t launch_batch_class(const JobDesc* djobs, int njobs, int lgL, const L
     if (lgL <= SBG_SMALL_MAX_LG) {
         size_t smem = (size_t)2 * padded_len(1 << lgL) * 4;
         k_small_b<<<njobs * SBG_NP, 256, smem, st>>>(djobs, lgL, tw_f, tw_i, sc);
+    } else if (lp->m3 >= 0) {
+        const int m3 = lp->m3;
+        FsTables fsf{lp->fs_lo_f, lp->fs_hi_f, lp->hi_n};
+        FsTables fsi{lp->fs_lo_i, lp->fs_hi_i, lp->hi_n};
+        const Radix3Arg r3f = radix3_arg(lp, false), r3i = radix3_arg(lp, true);
+        switch (m3) {
+#define SBG_LAUNCH_FB3(n)                                                                       \
+    case n:                                                                                     \
+        e = launch_colx(k_col3_fwd_b<n>, (int64_t)njobs * 2 * col3_ntiles(n) * SBG_NP * col3_csize(n), \
+                        col3_smem_bytes(n), col3_csize(n), st, djobs, tw_f, r3f);                \
+        break;
+            SBG_COL3_CASES(SBG_LAUNCH_FB3)
+#undef SBG_LAUNCH_FB3
+            default: return cudaErrorInvalidValue;
+        }
+        if (e != cudaSuccess) return e;
+        k_row12_b<<<njobs * SBG_NP * (3 << m3), 256, 0, st>>>(djobs, 0, m3, fsf, fsi, sc, tw_f, tw_i);
+        switch (m3) {
+#define SBG_LAUNCH_IB3(n)                                                                     \
+    case n:                                                                                   \
+        e = launch_colx(k_col3_inv_b<n>, (int64_t)njobs * col3_ntiles(n) * SBG_NP * col3_csize(n), \
+                        col3_smem_bytes(n), col3_csize(n), st, djobs, tw_i, r3i);              \
+        break;
+            SBG_COL3_CASES(SBG_LAUNCH_IB3)
+#undef SBG_LAUNCH_IB3
+            default: return cudaErrorInvalidValue;
+        }
+        if (e != cudaSuccess) return e;
     } else {
         const int lgN1 = lp->lgN1;
         FsTables fsf{lp->fs_lo_f, lp->fs_hi_f, lp->hi_n};
@@ -1268,7 +1585,7 @@ cudaError_t launch_batch_class(const JobDesc* djobs, int njobs, int lgL, const L
             default: return cudaErrorInvalidValue;
         }
         if (e != cudaSuccess) return e;
-        k_row12_b<<<(njobs * SBG_NP) << lgN1, 256, 0, st>>>(djobs, lgN1, fsf, fsi, sc, tw_f, tw_i);
+        k_row12_b<<<(njobs * SBG_NP) << lgN1, 256, 0, st>>>(djobs, lgN1, -1, fsf, fsi, sc, tw_f, tw_i);
         switch (lgN1) {
 #define SBG_LAUNCH_IB(n) \
     case n: e = launch_col(k_col_inv_b<n>, n, col_blocks, st, djobs, tw_i); break;
@@ -1279,7 +1596,7 @@ cudaError_t launch_batch_class(const JobDesc* djobs, int njobs, int lgL, const L
         if (e != cudaSuccess) return e;
     }
     const int bpj = (int)crt_blocks(max_nout);
-    k_crt_carry_b<<<njobs * bpj, CRT_T, 0, st>>>(djobs, lgL, bpj, err);
+    k_crt_carry_b<<<njobs * bpj, CRT_T, 0, st>>>(djobs, code_len(lgL), bpj, err);
     KT_END(kt, KID_BATCH, st);
     return cudaGetLastError();
 }
@@ -1296,7 +1613,7 @@ cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int6
     cudaError_t e = cudaMemsetAsync(flags, 0, (1 + nblk) * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     KT_BEGIN(kt, KID_CRT, st);
-    k_crt_carry<<<(unsigned)nblk, CRT_T, 0, st>>>(R, lgL, cmin, cmax, off, out, nout, flags, err);
+    k_crt_carry<<<(unsigned)nblk, CRT_T, 0, st>>>(R, code_len(lgL), cmin, cmax, off, out, nout, flags, err);
     KT_END(kt, KID_CRT, st);
     return cudaGetLastError();
 }

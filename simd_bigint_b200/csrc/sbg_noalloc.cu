@@ -133,7 +133,8 @@ extern "C" int sbg_mul_noalloc(uint64_t* rp, const uint64_t* ap, int64_t an, con
     lp.lgL = lgL;
     lp.lgN1 = 0;
     lp.lgN2 = lgL;
-    for (int q = 0; q < SBG_NP; ++q) lp.scale[q] = host_scale(lgL, q);
+    lp.L = (int64_t)1 << lgL;
+    for (int q = 0; q < SBG_NP; ++q) lp.scale[q] = host_scale(lp.L, q);
     uint32_t* res = d->scratch;
     uint32_t* flags = d->scratch + SBG_NOALLOC_RES_WORDS;
     uint32_t* err = flags + SBG_NOALLOC_FLAG_WORDS;

@@ -74,9 +74,9 @@ void host_crt_consts(CrtConst* out) {
 
 // 2^32 * L^-1 mod p_q: cancels the Montgomery factor of the pointwise
 // product and the factor L of the unnormalised forward/inverse pair.
-ShoupPair host_scale(int lgL, int q) {
+ShoupPair host_scale(int64_t L, int q) {
     uint32_t p = kPrimes[q];
-    uint32_t linv = host_inv(host_powmod(2, (uint64_t)lgL, p), p);
+    uint32_t linv = host_inv((uint32_t)((uint64_t)L % p), p);
     uint32_t s = (uint32_t)((((1ull << 32) % p) * linv) % p);
     return ShoupPair{s, host_shoup(s, p)};
 }

@@ -191,7 +191,7 @@ static int launch_slot(sbg_server* s, Slot& sl, std::deque<SReq>& fifo,
         const size_t need = mul_ws_bytes(q) + q.out_bytes;
         if (!take.empty() && batch_bytes + need > batch_cap) break;   // leave room for other slots
         // bounded work per batch, so that slots turn over and late arrivals start soon
-        if (!take.empty() && batch_points + ((int64_t)1 << q.lgL) > point_cap) break;
+        if (!take.empty() && batch_points + code_len(q.lgL) > point_cap) break;
         size_t wo, oo;
         if (!s->arena.alloc(mul_ws_bytes(q), &wo)) break;             // FIFO: wait for memory
         if (!s->arena.alloc(q.out_bytes, &oo)) {
@@ -203,7 +203,7 @@ static int launch_slot(sbg_server* s, Slot& sl, std::deque<SReq>& fifo,
         q.out_off = oo;
         take.push_back(q);
         batch_bytes += need;
-        batch_points += (int64_t)1 << q.lgL;
+        batch_points += code_len(q.lgL);
         fifo.pop_front();
     }
     if (take.empty()) return 0;
@@ -403,6 +403,7 @@ extern "C" int sbg_server_create(sbg_ctx* ctx, const sbg_server_config* cfg, sbg
     do {
         if ((st = cuda_fail(cudaSetDevice(ctx->device), "device"))) break;
         for (int l = 4; l <= 22 && !st; ++l) st = ensure_plan(ctx, l);   // tables to 2^22 points
+        for (int k = SBG_THREE_MIN_LG; k <= 20 && !st; ++k) st = ensure_plan(ctx, SBG_CODE3 + k);
         if (st) break;
         // stream priorities: multiply slots highest, reciprocal workers lowest,
         // so short multiplies are not queued behind long Newton batches
@@ -415,6 +416,7 @@ extern "C" int sbg_server_create(sbg_ctx* ctx, const sbg_server_config* cfg, sbg
             if ((st = sbg_ctx_create(ctx->device, &rc))) break;
             s->rctx.push_back(rc);
             rc->stream_priority = prio_low;
+            rc->len3_mask = ctx->len3_mask;
             cudaStream_t rs = nullptr;
             if ((st = cuda_fail(cudaStreamCreateWithPriority(&rs, cudaStreamNonBlocking, prio_low), "rstream")))
                 break;
@@ -486,7 +488,7 @@ static int prepare(sbg_server* s, const sbg_request* req, SReq& q) {
         if (req->kind == SBG_REQ_MUL && (!req->bp || req->bn <= 0)) return SBG_EINVAL;
         int64_t need = req->kind == SBG_REQ_SQR ? 2 * req->an - 1 : req->an + req->bn - 1;
         if (need > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
-        q.lgL = conv_lg(need);
+        q.lgL = conv_lg(need, s->ctx->len3_mask);
         q.sq = req->kind == SBG_REQ_SQR;
         q.cmin = 0;
         q.cmax = need - 1;
@@ -512,7 +514,8 @@ static int enqueue(sbg_server* s, SReq* q, int64_t n, uint64_t* tickets, int64_t
         if (q[i].r.kind == SBG_REQ_RECIP)
             s->pending_recip.push_back(q[i]);
         else
-            (q[i].lgL <= SMALL_LG ? s->pending_small : s->pending_mul).push_back(q[i]);
+            (code_len(q[i].lgL) <= ((int64_t)1 << SMALL_LG) ? s->pending_small : s->pending_mul)
+                .push_back(q[i]);
         if (tickets) tickets[i] = q[i].ticket;
         if (accepted) *accepted = i + 1;
     }
