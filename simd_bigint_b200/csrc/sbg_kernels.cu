@@ -148,6 +148,9 @@ __device__ __forceinline__ uint32_t fs_value(const FsTables& fs, int q, uint32_t
 // rows need clusters of 16 whose shared-memory exchange costs more than the
 // wider rows save; lane-per-column wins where no exchange is needed.)
 #define SBG_COL_SLAB_LG 10
+#ifndef SBG_COL_TILE_LG
+#define SBG_COL_TILE_LG 13        // points per CTA (log2)
+#endif
 #define SBG_COL_LANE_MAX_LG 8
 #define COL_THREADS 256
 #ifndef COL_MINB
@@ -159,7 +162,8 @@ __host__ __device__ constexpr int col_lgc(int lgN1) {
 }
 __host__ __device__ constexpr int col_lgs(int lgN1) { return lgN1 - col_lgc(lgN1); }
 __host__ __device__ constexpr int col_lgw_of(bool lanes, int lgs) {
-    return (13 - lgs) > 12 ? 12 : ((lanes && 13 - lgs < 5) ? 5 : 13 - lgs);
+    return (SBG_COL_TILE_LG - lgs) > 12 ? 12
+                                         : ((lanes && SBG_COL_TILE_LG - lgs < 5) ? 5 : SBG_COL_TILE_LG - lgs);
 }
 __host__ __device__ constexpr int col_lgw(int lgN1) { return col_lgw_of(col_lanes(lgN1), col_lgs(lgN1)); }
 // Plane strides: lanes, M + 1 (odd); pairs, padded length + 32/W, so that a
@@ -1321,12 +1325,28 @@ static cudaError_t col_attr() {
 
 #define SBG_COL_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13)
 
+template <int M3>
+static cudaError_t col3_attr() {
+    const int big = 200 * 1024;
+    cudaError_t e = cudaFuncSetAttribute(k_col3_fwd<M3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_col3_inv<M3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_col3_fwd_b<M3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_col3_inv_b<M3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    return e;
+}
+
 cudaError_t set_kernel_attributes() {
     const int big = 200 * 1024;
     cudaError_t e = cudaSuccess;
 #define SBG_ATTR(n) if (e == cudaSuccess) e = col_attr<n>();
     SBG_COL_CASES(SBG_ATTR)
 #undef SBG_ATTR
+#define SBG_ATTR3(n) if (e == cudaSuccess) e = col3_attr<n>();
+    SBG_COL3_CASES(SBG_ATTR3)
+#undef SBG_ATTR3
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     if (e == cudaSuccess)
