@@ -19,10 +19,10 @@ namespace sbg {
 #define SBG_CODE3 32
 #define SBG_NCODES (SBG_CODE3 + SBG_MAX_LG)
 #define SBG_THREE_MIN_LG 16
-// k = 21 .. 23: where 3 * 2^k measured faster than 2^(k+2) on B200 (below,
-// the cross-CTA radix-3 exchange of the short columns costs more than the
-// quarter of the points it saves)
-#define SBG_LEN3_DEFAULT 0x00E00000u
+// k = 16..19 and 21..23: where 3 * 2^k measured faster than 2^(k+2) on B200
+// (at k = 20 the columns of 768 rows need the cross-CTA radix-3 exchange,
+// which costs more than the quarter of the points it saves)
+#define SBG_LEN3_DEFAULT 0x00EF0000u
 inline bool code_three(int c) { return c >= SBG_CODE3; }
 inline int code_lg(int c) { return c >= SBG_CODE3 ? c - SBG_CODE3 : c; }
 inline int64_t code_len(int c) { return (int64_t)(c >= SBG_CODE3 ? 3 : 1) << code_lg(c); }

@@ -166,6 +166,9 @@ __host__ __device__ constexpr int col_lgw_of(bool lanes, int lgs) {
                                          : ((lanes && SBG_COL_TILE_LG - lgs < 5) ? 5 : SBG_COL_TILE_LG - lgs);
 }
 __host__ __device__ constexpr int col_lgw(int lgN1) { return col_lgw_of(col_lanes(lgN1), col_lgs(lgN1)); }
+// single-CTA 3 * 2^m columns (m <= SBG_COL3S_MAX): W = 2^(12 - m) columns of 3 * 2^m rows
+#define SBG_COL3S_MAX 7
+__host__ __device__ constexpr int col3s_lgw(int m) { return 12 - m; }
 // Plane strides: lanes, M + 1 (odd); pairs, padded length + 32/W, so that a
 // warp's W/2 column pairs x 64/W consecutive rows fall in distinct banks.
 __host__ __device__ constexpr int col_ld_of(bool lanes, int lgs) {
@@ -310,8 +313,10 @@ __device__ __forceinline__ uint32_t load_limb(const uint64_t* __restrict__ X, in
 }
 
 // Pass K of the lane-per-column mapping (a warp = 32 adjacent columns of one
-// group, one column per lane).
-template <int LGS, int K, bool FWD, bool SRC_G, bool DST_G>
+// group, one column per lane).  NSUB = 3: three 2^LGS-row slabs stacked in
+// the planes (the thirds of a 3 * 2^m column held by one CTA), transformed
+// independently.
+template <int LGS, int K, bool FWD, bool SRC_G, bool DST_G, int NSUB = 1>
 __device__ __forceinline__ void col_pass_lane(uint32_t* sm, const uint64_t* __restrict__ X,
                                            int64_t xn, uint32_t* __restrict__ Y, int c0, int row0,
                                            const uint2* __restrict__ tw, const PrimeConst& pc) {
@@ -320,19 +325,23 @@ __device__ __forceinline__ void col_pass_lane(uint32_t* sm, const uint64_t* __re
     constexpr int LGM = lgm_of(LGS, K);
     constexpr int LGST = LGM - r;
     constexpr int ST = 1 << LGST;
-    constexpr int LGW = col_lgw_of(true, LGS);
-    constexpr int LD = col_ld_of(true, LGS);
-    constexpr int TOTAL = 1 << (LGW + LGS - r);     // (column, group) pairs
+    constexpr int LGW = NSUB == 1 ? col_lgw_of(true, LGS) : col3s_lgw(LGS);
+    constexpr int LD = NSUB == 1 ? col_ld_of(true, LGS) : NSUB * (1 << LGS) + 1;
+    constexpr int LGT1 = LGW + LGS - r;              // (column, group) pairs per slab
+    constexpr int TOTAL = NSUB << LGT1;
     const uint32_t p = pc.p;
     constexpr int ITER = TOTAL >= COL_THREADS ? TOTAL / COL_THREADS : 1;
-#pragma unroll
+    // bounded unrolling: at most two radix-16 groups, eight short ones in flight
+    constexpr int UNR = R >= 16 ? (ITER > 2 ? 1 : ITER) : (ITER > 8 ? 8 : ITER);
+#pragma unroll UNR
     for (int it = 0; it < ITER; ++it) {
         const int gid = threadIdx.x + it * COL_THREADS;
         if (TOTAL < COL_THREADS && gid >= TOTAL) break;
-        const int col = gid & ((1 << LGW) - 1);
-        const int grp = gid >> LGW;
+        const int g = gid & ((1 << LGT1) - 1);
+        const int col = g & ((1 << LGW) - 1);
+        const int grp = g >> LGW;
         const int j0 = grp & (ST - 1);
-        const int i0 = ((grp >> LGST) << LGM) + j0;
+        const int i0 = ((gid >> LGT1) << LGS) + ((grp >> LGST) << LGM) + j0;
         uint32_t x[R];
         if constexpr (SRC_G) {
             const int64_t n0 = ((int64_t)(i0 + row0) << SBG_ROW_LG) + c0 + col;
@@ -369,55 +378,57 @@ __device__ __forceinline__ void col_pass_lane(uint32_t* sm, const uint64_t* __re
 // slab whose first row is row0, in the mapping LANES selects.  SRC_G: read
 // from global (limbs when FWD, residues otherwise); DST_G: write residues to
 // global; else shared memory.
-template <bool LANES, int LGS, int K, bool FWD, bool SRC_G, bool DST_G>
+template <bool LANES, int LGS, int K, bool FWD, bool SRC_G, bool DST_G, int NSUB = 1>
 __device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restrict__ X,
                                            int64_t xn, uint32_t* __restrict__ Y, int c0, int row0,
                                            const uint2* __restrict__ tw, const PrimeConst& pc) {
-    if constexpr (LANES)
-        col_pass_lane<LGS, K, FWD, SRC_G, DST_G>(sm, X, xn, Y, c0, row0, tw, pc);
-    else
+    if constexpr (LANES) {
+        col_pass_lane<LGS, K, FWD, SRC_G, DST_G, NSUB>(sm, X, xn, Y, c0, row0, tw, pc);
+    } else {
+        static_assert(NSUB == 1, "stacked slabs use the lane mapping");
         col_pass_pair<LGS, K, FWD, SRC_G, DST_G>(sm, X, xn, Y, c0, row0, tw, pc);
+    }
 }
 
 // The local passes of a slab: forward K = 0 .. NP-1, inverse NP-1 .. 0.
 // FIRST_G / LAST_G: whether the first / last pass touches global memory.
-template <bool LANES, int LGS, bool FIRST_G, bool LAST_G>
+template <bool LANES, int LGS, bool FIRST_G, bool LAST_G, int NSUB = 1>
 __device__ __forceinline__ void col_slab_fwd(uint32_t* sm, const uint64_t* __restrict__ X, int64_t xn,
                                              uint32_t* __restrict__ Y, int c0, int row0,
                                              const uint2* __restrict__ tw, const PrimeConst& pc) {
     constexpr int NP = col_np(LGS);
-    col_pass_t<LANES, LGS, 0, true, FIRST_G, LAST_G && NP == 1>(sm, X, xn, Y, c0, row0, tw, pc);
+    col_pass_t<LANES, LGS, 0, true, FIRST_G, LAST_G && NP == 1, NSUB>(sm, X, xn, Y, c0, row0, tw, pc);
     if constexpr (NP > 1) {
         __syncthreads();
-        col_pass_t<LANES, LGS, 1, true, false, LAST_G && NP == 2>(sm, X, xn, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 1, true, false, LAST_G && NP == 2, NSUB>(sm, X, xn, Y, c0, row0, tw, pc);
     }
     if constexpr (NP > 2) {
         __syncthreads();
-        col_pass_t<LANES, LGS, 2, true, false, LAST_G && NP == 3>(sm, X, xn, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 2, true, false, LAST_G && NP == 3, NSUB>(sm, X, xn, Y, c0, row0, tw, pc);
     }
     if constexpr (NP > 3) {
         __syncthreads();
-        col_pass_t<LANES, LGS, 3, true, false, LAST_G && NP == 4>(sm, X, xn, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 3, true, false, LAST_G && NP == 4, NSUB>(sm, X, xn, Y, c0, row0, tw, pc);
     }
 }
 
-template <bool LANES, int LGS, bool FIRST_G, bool LAST_G>
+template <bool LANES, int LGS, bool FIRST_G, bool LAST_G, int NSUB = 1>
 __device__ __forceinline__ void col_slab_inv(uint32_t* sm, uint32_t* __restrict__ Y, int c0, int row0,
                                              const uint2* __restrict__ tw, const PrimeConst& pc) {
     constexpr int NP = col_np(LGS);
     if constexpr (NP > 3) {
-        col_pass_t<LANES, LGS, 3, false, FIRST_G, false>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 3, false, FIRST_G, false, NSUB>(sm, nullptr, 0, Y, c0, row0, tw, pc);
         __syncthreads();
     }
     if constexpr (NP > 2) {
-        col_pass_t<LANES, LGS, 2, false, FIRST_G && NP == 3, false>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 2, false, FIRST_G && NP == 3, false, NSUB>(sm, nullptr, 0, Y, c0, row0, tw, pc);
         __syncthreads();
     }
     if constexpr (NP > 1) {
-        col_pass_t<LANES, LGS, 1, false, FIRST_G && NP == 2, false>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 1, false, FIRST_G && NP == 2, false, NSUB>(sm, nullptr, 0, Y, c0, row0, tw, pc);
         __syncthreads();
     }
-    col_pass_t<LANES, LGS, 0, false, FIRST_G && NP == 1, LAST_G>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+    col_pass_t<LANES, LGS, 0, false, FIRST_G && NP == 1, LAST_G, NSUB>(sm, nullptr, 0, Y, c0, row0, tw, pc);
 }
 
 // cluster barrier; RELEASE publishes this CTA's shared-memory stores (local
@@ -666,7 +677,7 @@ __host__ __device__ constexpr int col3_smem_bytes(int m) {
     return (1 << col3_lgw(m)) * col_ld_of(col3_lanes(m), col3_lgs(m)) * 4;
 }
 __host__ __device__ constexpr int col3_ntiles(int m) { return 1 << (SBG_ROW_LG - col3_lgw(m)); }
-#define SBG_COL3_CASES(X) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11)
+#define SBG_COL3_CASES(X) X(8) X(9) X(10) X(11)
 
 // shared-memory address of (column, row) in a slab's planes
 template <bool LANES, int LD>
@@ -786,6 +797,124 @@ __device__ __forceinline__ void col3_inv_body(int q, int tile, int slab, uint32_
     cluster_barrier<true>();            // all slabs complete in shared memory
     col3_cross_inv<M3>(sm, Y, c0, slab, tw, r3.t3 + ((size_t)q << (M3 + 1)), r3.w[q], r3.ws[q], pc);
     cluster_barrier<false>();           // peers read this CTA's slab until here
+}
+
+// Short 3 * 2^m columns (m <= SBG_COL3S_MAX): the whole column in one CTA,
+// W = 2^(12 - m) >= 32 columns of 3 * 2^m rows (12288 points) stacked as
+// three 2^m-row slabs in planes of 3 * 2^m + 1 words; the radix-3 level is
+// one pass between global memory and the planes, no cluster exchange.
+template <int M3, bool FWD>
+__device__ __forceinline__ void col3s_r3_pass(uint32_t* sm, const uint64_t* __restrict__ X, int64_t xn,
+                                              uint32_t* __restrict__ Y, int c0, const uint2* __restrict__ t3,
+                                              uint32_t w3, uint32_t w3s, const PrimeConst& pc) {
+    constexpr int M = 1 << M3;
+    constexpr int LGW = col3s_lgw(M3);
+    constexpr int LD = 3 * M + 1;
+    constexpr int ITER = (M << LGW) / COL_THREADS;
+#pragma unroll 2
+    for (int it = 0; it < ITER; ++it) {
+        const int gid = threadIdx.x + it * COL_THREADS;
+        const int col = gid & ((1 << LGW) - 1);
+        const int r = gid >> LGW;
+        uint32_t* s0 = sm + col * LD + r;
+        const uint2 ta = __ldg(&t3[r]), tb = __ldg(&t3[2 * r]);
+        const int64_t n0 = ((int64_t)r << SBG_ROW_LG) + c0 + col;
+        constexpr int64_t DM = (int64_t)M << SBG_ROW_LG;
+        if constexpr (FWD) {
+            uint32_t a = load_limb(X, xn, n0, pc), b = load_limb(X, xn, n0 + DM, pc),
+                     c = load_limb(X, xn, n0 + 2 * DM, pc);
+            r3_dif(a, b, c, w3, w3s, ta, tb, pc.p);
+            s0[0] = a;
+            s0[M] = b;
+            s0[2 * M] = c;
+        } else {
+            uint32_t a = s0[0], b = s0[M], c = s0[2 * M];
+            r3_dit(a, b, c, w3, w3s, ta, tb, pc.p);
+            Y[n0] = a;
+            Y[n0 + DM] = b;
+            Y[n0 + 2 * DM] = c;
+        }
+    }
+}
+
+__host__ __device__ constexpr int col3s_smem_bytes(int m) { return (1 << col3s_lgw(m)) * (3 * (1 << m) + 1) * 4; }
+__host__ __device__ constexpr int col3s_ntiles(int m) { return 1 << m; }
+#define SBG_COL3S_CASES(X) X(4) X(5) X(6) X(7)
+
+template <int M3>
+__device__ __forceinline__ void col3s_fwd_body(int q, int tile, int op, const uint64_t* __restrict__ a, int64_t an,
+                                               const uint64_t* __restrict__ b, int64_t bn,
+                                               const uint2* __restrict__ twf, const Radix3Arg& r3,
+                                               uint32_t* __restrict__ YA, uint32_t* __restrict__ YB) {
+    extern __shared__ uint32_t sm[];
+    constexpr size_t L = (size_t)3 << (M3 + SBG_ROW_LG);
+    const uint64_t* X = op ? b : a;
+    const int64_t xn = op ? bn : an;
+    uint32_t* Y = (op ? YB : YA) + (size_t)q * L;
+    const PrimeConst pc = c_pr[q];
+    const uint2* tw = twf + (size_t)q * SBG_TW_N;
+    const int c0 = tile << col3s_lgw(M3);
+    col3s_r3_pass<M3, true>(sm, X, xn, Y, c0, r3.t3 + ((size_t)q << (M3 + 1)), r3.w[q], r3.ws[q], pc);
+    __syncthreads();
+    col_slab_fwd<true, M3, false, true, 3>(sm, X, xn, Y, c0, 0, tw, pc);
+}
+
+template <int M3>
+__device__ __forceinline__ void col3s_inv_body(int q, int tile, uint32_t* __restrict__ YA,
+                                               const uint2* __restrict__ twi, const Radix3Arg& r3) {
+    extern __shared__ uint32_t sm[];
+    constexpr size_t L = (size_t)3 << (M3 + SBG_ROW_LG);
+    uint32_t* Y = YA + (size_t)q * L;
+    const PrimeConst pc = c_pr[q];
+    const uint2* tw = twi + (size_t)q * SBG_TW_N;
+    const int c0 = tile << col3s_lgw(M3);
+    col_slab_inv<true, M3, true, false, 3>(sm, Y, c0, 0, tw, pc);
+    __syncthreads();
+    col3s_r3_pass<M3, false>(sm, nullptr, 0, Y, c0, r3.t3 + ((size_t)q << (M3 + 1)), r3.w[q], r3.ws[q], pc);
+}
+
+// blocks: prime fastest, then tile, operand
+template <int M3>
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3s_fwd(const uint64_t* __restrict__ a, int64_t an,
+                                                                   const uint64_t* __restrict__ b, int64_t bn,
+                                                                   const uint2* __restrict__ twf, Radix3Arg r3,
+                                                                   uint32_t* __restrict__ YA,
+                                                                   uint32_t* __restrict__ YB) {
+    constexpr int NTILES = col3s_ntiles(M3);
+    const int q = blockIdx.x % SBG_NP;
+    const int rest = blockIdx.x / SBG_NP;
+    col3s_fwd_body<M3>(q, rest % NTILES, rest / NTILES, a, an, b, bn, twf, r3, YA, YB);
+}
+
+template <int M3>
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3s_fwd_b(const JobDesc* __restrict__ jobs,
+                                                                     const uint2* __restrict__ twf, Radix3Arg r3) {
+    constexpr int NTILES = col3s_ntiles(M3);
+    constexpr int PER_JOB = SBG_NP * 2 * NTILES;
+    constexpr size_t L = (size_t)3 << (M3 + SBG_ROW_LG);
+    const JobDesc& J = jobs[blockIdx.x / PER_JOB];
+    const int r = blockIdx.x % PER_JOB;
+    const int q = r % SBG_NP;
+    const int rest = r / SBG_NP;
+    const int op = rest / NTILES;
+    if (op && J.sq) return;
+    col3s_fwd_body<M3>(q, rest % NTILES, op, J.a, J.an, J.b, J.bn, twf, r3, J.ws, J.ws + SBG_NP * L);
+}
+
+template <int M3>
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3s_inv(uint32_t* __restrict__ YA,
+                                                                   const uint2* __restrict__ twi, Radix3Arg r3) {
+    col3s_inv_body<M3>(blockIdx.x % SBG_NP, blockIdx.x / SBG_NP, YA, twi, r3);
+}
+
+template <int M3>
+__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3s_inv_b(const JobDesc* __restrict__ jobs,
+                                                                     const uint2* __restrict__ twi, Radix3Arg r3) {
+    constexpr int NTILES = col3s_ntiles(M3);
+    constexpr int PER_JOB = SBG_NP * NTILES;
+    const JobDesc& J = jobs[blockIdx.x / PER_JOB];
+    const int r = blockIdx.x % PER_JOB;
+    col3s_inv_body<M3>(r % SBG_NP, r / SBG_NP, J.ws, twi, r3);
 }
 
 // blocks: slab fastest (a cluster), then prime, tile, operand
@@ -1326,6 +1455,19 @@ static cudaError_t col_attr() {
 #define SBG_COL_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13)
 
 template <int M3>
+static cudaError_t col3s_attr() {
+    const int big = 200 * 1024;
+    cudaError_t e = cudaFuncSetAttribute(k_col3s_fwd<M3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_col3s_inv<M3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_col3s_fwd_b<M3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_col3s_inv_b<M3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    return e;
+}
+
+template <int M3>
 static cudaError_t col3_attr() {
     const int big = 200 * 1024;
     cudaError_t e = cudaFuncSetAttribute(k_col3_fwd<M3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
@@ -1347,6 +1489,9 @@ cudaError_t set_kernel_attributes() {
 #define SBG_ATTR3(n) if (e == cudaSuccess) e = col3_attr<n>();
     SBG_COL3_CASES(SBG_ATTR3)
 #undef SBG_ATTR3
+#define SBG_ATTR3S(n) if (e == cudaSuccess) e = col3s_attr<n>();
+    SBG_COL3S_CASES(SBG_ATTR3S)
+#undef SBG_ATTR3S
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_small, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     if (e == cudaSuccess)
@@ -1483,6 +1628,13 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
         const Radix3Arg r3f = radix3_arg(lp, false), r3i = radix3_arg(lp, true);
         KT_BEGIN(kt, KID_COL_FWD, st);
         switch (m3) {
+#define SBG_LAUNCH_F3S(n)                                                                          \
+    case n:                                                                                        \
+        e = launch_colx(k_col3s_fwd<n>, (int64_t)nops * col3s_ntiles(n) * SBG_NP, col3s_smem_bytes(n), 1, \
+                        st, a, an, b, bn, tw_f, r3f, YA, YB);                                       \
+        break;
+            SBG_COL3S_CASES(SBG_LAUNCH_F3S)
+#undef SBG_LAUNCH_F3S
 #define SBG_LAUNCH_F3(n)                                                                          \
     case n:                                                                                       \
         e = launch_colx(k_col3_fwd<n>, (int64_t)nops * col3_ntiles(n) * SBG_NP * col3_csize(n),    \
@@ -1500,6 +1652,13 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         KT_BEGIN(kt, KID_COL_INV, st);
         switch (m3) {
+#define SBG_LAUNCH_I3S(n)                                                                          \
+    case n:                                                                                        \
+        e = launch_colx(k_col3s_inv<n>, (int64_t)col3s_ntiles(n) * SBG_NP, col3s_smem_bytes(n), 1, st, YA, \
+                        tw_i, r3i);                                                                 \
+        break;
+            SBG_COL3S_CASES(SBG_LAUNCH_I3S)
+#undef SBG_LAUNCH_I3S
 #define SBG_LAUNCH_I3(n)                                                                             \
     case n:                                                                                          \
         e = launch_colx(k_col3_inv<n>, (int64_t)col3_ntiles(n) * SBG_NP * col3_csize(n),               \
@@ -1570,6 +1729,13 @@ cudaError_t launch_batch_class(const JobDesc* djobs, int njobs, int lgL, const L
         FsTables fsi{lp->fs_lo_i, lp->fs_hi_i, lp->hi_n};
         const Radix3Arg r3f = radix3_arg(lp, false), r3i = radix3_arg(lp, true);
         switch (m3) {
+#define SBG_LAUNCH_FB3S(n)                                                                              \
+    case n:                                                                                             \
+        e = launch_colx(k_col3s_fwd_b<n>, (int64_t)njobs * 2 * col3s_ntiles(n) * SBG_NP, col3s_smem_bytes(n), \
+                        1, st, djobs, tw_f, r3f);                                                        \
+        break;
+            SBG_COL3S_CASES(SBG_LAUNCH_FB3S)
+#undef SBG_LAUNCH_FB3S
 #define SBG_LAUNCH_FB3(n)                                                                       \
     case n:                                                                                     \
         e = launch_colx(k_col3_fwd_b<n>, (int64_t)njobs * 2 * col3_ntiles(n) * SBG_NP * col3_csize(n), \
@@ -1582,6 +1748,13 @@ cudaError_t launch_batch_class(const JobDesc* djobs, int njobs, int lgL, const L
         if (e != cudaSuccess) return e;
         k_row12_b<<<njobs * SBG_NP * (3 << m3), 256, 0, st>>>(djobs, 0, m3, fsf, fsi, sc, tw_f, tw_i);
         switch (m3) {
+#define SBG_LAUNCH_IB3S(n)                                                                           \
+    case n:                                                                                          \
+        e = launch_colx(k_col3s_inv_b<n>, (int64_t)njobs * col3s_ntiles(n) * SBG_NP, col3s_smem_bytes(n), \
+                        1, st, djobs, tw_i, r3i);                                                     \
+        break;
+            SBG_COL3S_CASES(SBG_LAUNCH_IB3S)
+#undef SBG_LAUNCH_IB3S
 #define SBG_LAUNCH_IB3(n)                                                                     \
     case n:                                                                                   \
         e = launch_colx(k_col3_inv_b<n>, (int64_t)njobs * col3_ntiles(n) * SBG_NP * col3_csize(n), \

@@ -125,10 +125,10 @@ def test_three_lengths_mulmid_and_batch(ctx3):
 
 
 def test_default_lengths_and_autotune(ctx):
-    """The default mask enables 3 * 2^k from k = 21 (measured on B200); the
-    drop-in's default context multiplies there at 3 * 2^23 (2^24 x 2^20)."""
+    """The default mask enables 3 * 2^k for k = 16..19 and 21..23 (measured
+    on B200); the drop-in's default context multiplies 2^24 x 2^20 at 3 * 2^23."""
     import simd_bigint_b200 as sbg
-    assert ctx.len3_mask == 0x00E00000
+    assert ctx.len3_mask == 0x00EF0000
     rng = np.random.default_rng(35)
     a = rand_limbs(1 << 24, rng)
     b = rand_limbs(1 << 20, rng)
