@@ -791,6 +791,8 @@ def run_serve(args, ws, rank, local, pg) -> dict | None:
     ops = serve_operands(reqs, pool, seed=77 + rank)
     limbs = sum(serve_out_limbs(k, an, bn) for k, an, bn in reqs)
     ctx = sbg.Context(local)
+    if args.len3_mask is not None:
+        ctx.set_len3_mask(args.len3_mask)
     srv = sbg.Server(ctx, arena_bytes=args.arena_gb << 30, slots=args.slots, max_batch=256,
                      batch_lg_points=args.batch_lg_points)
     clocks = ClockSampler(local)
@@ -1143,6 +1145,8 @@ def main():
     ap.add_argument("--arena-gb", type=int, default=16, help="serve: server arena (GiB)")
     ap.add_argument("--slots", type=int, default=4, help="serve: batches in flight")
     ap.add_argument("--batch-lg-points", type=int, default=0, help="serve: log2 points per batch (0: default)")
+    ap.add_argument("--len3-mask", type=lambda x: int(x, 0), default=None,
+                    help="serve: 3*2^k length classes to use (bit k; default: the library's)")
     ap.add_argument("--cpu-requests", type=int, default=640, help="serve: CPU baseline sample")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -204,7 +204,8 @@ typedef struct {
     double queue_s;        /* submission -> launch of its batch (the rest is device time) */
 } sbg_completion;
 typedef struct {
-    size_t arena_bytes;    /* HBM budget for workspaces and results (default 8 GiB) */
+    size_t arena_bytes;    /* HBM budget (default 8 GiB): 5/8 for transform workspaces,
+                              3/8 for results awaiting sbg_server_release */
     int32_t slots;         /* batches in flight (default 4) */
     int32_t max_batch;     /* requests per batch (default 512) */
     int32_t recip_workers; /* reciprocal batches in flight, own context each (default 2) */

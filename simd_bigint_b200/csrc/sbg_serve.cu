@@ -46,13 +46,14 @@ static double now_s() {
         .count();
 }
 
-// first-fit allocator over [0, size) in 256-byte units, coalescing on free
+// first-fit allocator over [base, base + size) in 256-byte units, coalescing
+// on free; offsets are absolute within the server's device allocation
 class Arena {
    public:
-    void init(size_t size) {
+    void init(size_t base, size_t size) {
         free_.clear();
         size_ = size & ~(size_t)255;
-        free_[0] = size_;
+        free_[base] = size_;
         used_ = 0;
     }
     bool alloc(size_t bytes, size_t* off) {
@@ -136,7 +137,12 @@ struct sbg_server {
     int prio_high = 0, prio_low = 0;
     sbg_server_config cfg{};
     uint8_t* arena_base = nullptr;
+    // two pools in one allocation: transient blocks (workspaces, descriptors,
+    // reciprocal scratch charges; freed when their batch ends) and results
+    // (held until the client releases them), so that results scattered over
+    // time never fragment the space the next batches need
     Arena arena;
+    Arena res;
     std::mutex mu;                       // guards queues, arena, completions
     std::condition_variable cv_work, cv_done;
     // multiply FIFOs by size: transforms up to 2^SMALL_LG points go to
@@ -170,7 +176,7 @@ static void complete(sbg_server* s, const SReq& q, int status, double t) {
     if (status == SBG_OK)
         s->results[q.ticket] = {q.out_off, q.out_bytes};
     else
-        s->arena.release(q.out_off, q.out_bytes);
+        s->res.release(q.out_off, q.out_bytes);
     s->done.push_back(c);
     s->n_done++;
 }
@@ -194,7 +200,7 @@ static int launch_slot(sbg_server* s, Slot& sl, std::deque<SReq>& fifo,
         if (!take.empty() && batch_points + code_len(q.lgL) > point_cap) break;
         size_t wo, oo;
         if (!s->arena.alloc(mul_ws_bytes(q), &wo)) break;             // FIFO: wait for memory
-        if (!s->arena.alloc(q.out_bytes, &oo)) {
+        if (!s->res.alloc(q.out_bytes, &oo)) {
             s->arena.release(wo, mul_ws_bytes(q));
             break;
         }
@@ -219,7 +225,7 @@ static int launch_slot(sbg_server* s, Slot& sl, std::deque<SReq>& fifo,
     if (!s->arena.alloc(meta, &mo)) {
         for (auto& q : take) {                       // give everything back, retry later
             s->arena.release(q.ws_off, q.ws_bytes);
-            s->arena.release(q.out_off, q.out_bytes);
+            s->res.release(q.out_off, q.out_bytes);
         }
         for (auto it = take.rbegin(); it != take.rend(); ++it) fifo.push_front(*it);
         return 0;
@@ -351,7 +357,7 @@ static void recip_loop(sbg_server* s, sbg_ctx* rc) {
             if (!take.empty() && points + 4 * q.r.an > point_cap) break;
             size_t wo, oo;
             if (!s->arena.alloc(q.ws_bytes, &wo)) break;
-            if (!s->arena.alloc(q.out_bytes, &oo)) {
+            if (!s->res.alloc(q.out_bytes, &oo)) {
                 s->arena.release(wo, q.ws_bytes);
                 break;
             }
@@ -425,7 +431,9 @@ extern "C" int sbg_server_create(sbg_ctx* ctx, const sbg_server_config* cfg, sbg
         }
         if (st) break;
         if ((st = cuda_fail(cudaMalloc(&s->arena_base, s->cfg.arena_bytes), "arena"))) break;
-        s->arena.init(s->cfg.arena_bytes);
+        const size_t transient = (s->cfg.arena_bytes / 8 * 5) & ~(size_t)255;
+        s->arena.init(0, transient);
+        s->res.init(transient, s->cfg.arena_bytes - transient);
         s->slots.resize((size_t)s->cfg.slots);
         for (auto& sl : s->slots) {
             // slot 0 (short requests) above the other slots, which are above
@@ -497,7 +505,8 @@ static int prepare(sbg_server* s, const sbg_request* req, SReq& q) {
         q.out_bytes = (size_t)q.nout * 8;
         q.ws_bytes = mul_ws_bytes(q);
     }
-    if (q.ws_bytes + q.out_bytes + 4096 > s->arena.size()) return SBG_EADMIT;   // can never fit
+    if (q.ws_bytes + 4096 > s->arena.size() || q.out_bytes > s->res.size())
+        return SBG_EADMIT;                           // can never fit
     return SBG_OK;
 }
 
@@ -572,7 +581,7 @@ extern "C" int sbg_server_release(sbg_server* s, uint64_t ticket) {
     std::lock_guard<std::mutex> g(s->mu);
     auto it = s->results.find(ticket);
     if (it == s->results.end()) return SBG_EINVAL;
-    s->arena.release(it->second.first, it->second.second);
+    s->res.release(it->second.first, it->second.second);
     s->results.erase(it);
     s->cv_work.notify_all();
     return SBG_OK;
@@ -594,6 +603,6 @@ extern "C" int sbg_server_stats(sbg_server* s, int64_t* pending, int64_t* comple
         *pending = (int64_t)(s->pending_small.size() + s->pending_mul.size() + s->pending_recip.size());
     if (completed) *completed = s->n_done;
     if (batches) *batches = s->n_batches;
-    if (arena_used) *arena_used = s->arena.used();
+    if (arena_used) *arena_used = s->arena.used() + s->res.used();
     return SBG_OK;
 }
