@@ -34,7 +34,7 @@
 namespace sbg {
 
 #define DIV_T 1024           // threads of the per-division linear kernels
-#define DIV_PER 4            // limbs per thread per tile
+#define DIV_PER 8            // limbs per thread per tile
 #define DIV_TILE (DIV_T * DIV_PER)
 
 // ---------------------------------------------------------------------------
@@ -128,20 +128,46 @@ __device__ uint32_t block_addsub(uint64_t* z, int64_t len, FX x, FY y, bool sub,
     return carry;
 }
 
-// sign of x - y over len limbs: -1, 0, 1 (block-uniform)
+// sign of x - y over len limbs: -1, 0, 1 (block-uniform).  Walks down from
+// the top one block-width at a time and stops at the first chunk holding a
+// difference (the top chunk, unless the operands agree there).
 template <class FX, class FY>
 __device__ int block_cmp(int64_t len, FX x, FY y) {
     __shared__ long long s_hi;
-    if (threadIdx.x == 0) s_hi = -1;
-    __syncthreads();
-    for (int64_t i = threadIdx.x; i < len; i += DIV_T) {
-        if (x(i) != y(i)) atomicMax(&s_hi, (long long)i);
+    for (int64_t top = len; top > 0; top -= DIV_T) {
+        if (threadIdx.x == 0) s_hi = -1;
+        __syncthreads();
+        const int64_t i = top - 1 - threadIdx.x;
+        if (i >= 0 && x(i) != y(i)) atomicMax(&s_hi, (long long)i);
+        __syncthreads();
+        const long long hi = s_hi;
+        __syncthreads();
+        if (hi >= 0) return x(hi) > y(hi) ? 1 : -1;
     }
-    __syncthreads();
-    long long hi = s_hi;
-    __syncthreads();
-    if (hi < 0) return 0;
-    return x(hi) > y(hi) ? 1 : -1;
+    return 0;
+}
+
+// z[0..len) += 1 (inc) or -= 1 in place: the carry / borrow ripples only
+// through the low limbs equal to ~0 / 0, so the pass stops at the first
+// limb that absorbs it (found one block-width at a time)
+__device__ void block_step1(uint64_t* z, int64_t len, bool inc) {
+    __shared__ long long s_lo;
+    const uint64_t ripple = inc ? ~0ull : 0ull;
+    for (int64_t base = 0; base < len; base += DIV_T) {
+        if (threadIdx.x == 0) s_lo = len;
+        __syncthreads();
+        const int64_t i = base + threadIdx.x;
+        const bool stop = i < len && z[i] != ripple;
+        if (stop) atomicMin(&s_lo, (long long)i);
+        __syncthreads();
+        const long long lo = s_lo;
+        __syncthreads();
+        // limbs below lo (within this chunk) ripple; limb lo absorbs
+        if (i < len && i < lo) z[i] = inc ? 0ull : ~0ull;
+        if (i == lo) z[i] = inc ? z[i] + 1 : z[i] - 1;
+        __syncthreads();
+        if (lo < len) return;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -235,9 +261,7 @@ __global__ void __launch_bounds__(DIV_T) k_recip_step1(const RecipStep* st, uint
         uint64_t* T = S.T;
         block_addsub(T, tl, [&](int64_t i) { return T[i]; },
                      [&](int64_t i) { return i < n ? A[i] : 0ull; }, true, 0);
-        uint64_t* Xh = S.Xh;
-        block_addsub(Xh, h + 1, [&](int64_t i) { return Xh[i]; },
-                     [&](int64_t i) { return i == 0 ? 1ull : 0ull; }, true, 0);
+        block_step1(S.Xh, h + 1, false);
     }
     __syncthreads();
     // B^(n+h) - T = (~T + 1) on the low n+1 limbs; the +1 reaches limb l only
@@ -302,9 +326,7 @@ __global__ void __launch_bounds__(DIV_T) k_div_fix(const DivFix* df, uint32_t* e
         }
         block_addsub(Rw, n + 1, [&](int64_t i) { return Rw[i]; },
                      [&](int64_t i) { return i < n ? D[i] : 0ull; }, true, 0);
-        uint64_t* Q = F.Q;
-        block_addsub(Q, n + 1, [&](int64_t i) { return Q[i]; },
-                     [&](int64_t i) { return i == 0 ? 1ull : 0ull; }, false, 0);
+        block_step1(F.Q, n + 1, true);
     }
     __syncthreads();
     for (int64_t i = threadIdx.x; i < n; i += DIV_T) F.R[i] = Rw[i];
@@ -324,9 +346,7 @@ __global__ void __launch_bounds__(DIV_T) k_recip_final(const DivFix* df, uint32_
                       [&](int64_t i) { return i < n ? D[i] : 0ull; });
     // Q holds X (n+1 limbs); V = X (+1) low n limbs
     uint64_t* Q = F.Q;
-    if (c >= 0)
-        block_addsub(Q, n + 1, [&](int64_t i) { return Q[i]; },
-                     [&](int64_t i) { return i == 0 ? 1ull : 0ull; }, false, 0);
+    if (c >= 0) block_step1(Q, n + 1, true);
     __syncthreads();
     if (threadIdx.x == 0 && Q[n] != 1) atomicOr(err, 64u);
     for (int64_t i = threadIdx.x; i < n; i += DIV_T) F.R[i] = Q[i];
