@@ -175,6 +175,14 @@ static int job_shape(const sbg_job& j, uint32_t mask3, int* lgL, int64_t* cmin, 
             *lgL = conv_lg(2 * j.an - 1, mask3);
             *cmin = 0; *cmax = 2 * j.an - 2; *off = 0; *nout = 2 * j.an; *sq = 1;
             return SBG_OK;
+        case SBG_JOB_CYCLIC: {
+            if (!j.bp || j.bn <= 0 || j.reserved < 0 || j.reserved > SBG_NCODES) return SBG_EINVAL;
+            const int64_t L = code_len(j.reserved);
+            if (L > ((int64_t)1 << SBG_MAX_LG) || j.an > L || j.bn > L) return SBG_EINVAL;
+            *lgL = j.reserved;
+            *cmin = 0; *cmax = L - 1; *off = 0; *nout = L + 3; *sq = 0;
+            return SBG_OK;
+        }
         case SBG_JOB_MULMID:
             if (!j.bp || j.bn <= 0 || j.an < j.bn) return SBG_EINVAL;
             if (j.an > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;

@@ -150,7 +150,7 @@ __device__ int block_cmp(int64_t len, FX x, FY y) {
 // z[0..len) += 1 (inc) or -= 1 in place: the carry / borrow ripples only
 // through the low limbs equal to ~0 / 0, so the pass stops at the first
 // limb that absorbs it (found one block-width at a time)
-__device__ void block_step1(uint64_t* z, int64_t len, bool inc) {
+__device__ bool block_step1(uint64_t* z, int64_t len, bool inc) {
     __shared__ long long s_lo;
     const uint64_t ripple = inc ? ~0ull : 0ull;
     for (int64_t base = 0; base < len; base += DIV_T) {
@@ -166,8 +166,9 @@ __device__ void block_step1(uint64_t* z, int64_t len, bool inc) {
         if (i < len && i < lo) z[i] = inc ? 0ull : ~0ull;
         if (i == lo) z[i] = inc ? z[i] + 1 : z[i] - 1;
         __syncthreads();
-        if (lo < len) return;
+        if (lo < len) return false;
     }
+    return true;                        // rippled out of the top limb
 }
 
 // ---------------------------------------------------------------------------
@@ -176,7 +177,9 @@ __device__ void block_step1(uint64_t* z, int64_t len, bool inc) {
 struct RecipStep {
     const uint64_t* A;      // top n limbs of D
     uint64_t* Xh;           // h+1 limbs (in/out: corrected in place)
-    uint64_t* T;            // n+h+1 limbs: D*Xh on entry
+    uint64_t* T;            // n+h+1 limbs: D*Xh on entry (rebuilt from C when L > 0)
+    uint64_t* C;            // L > 0: A*Xh mod (B^L - 1) as L+3 unfolded limbs
+    int64_t L;
     uint64_t* TM;           // out: h+1 limbs
     const uint64_t* U;      // n/a in step 1; 2h+2 limbs in step 2
     uint64_t* X;            // out of step 2: n+1 limbs
@@ -243,6 +246,47 @@ __global__ void k_recip_base(const uint64_t* const* A, const int64_t* m, uint64_
         q[j] = qd;
     }
     if (q[n] != 1) atomicOr(err, 8u);
+}
+
+// step 0 (wrapped first product): T = A X_h lies within 2 B^n of B^(n+h)
+// (A X_h = A_h X_h B^l + A_l X_h with B^2h - 2 A_h <= A_h X_h < B^2h and
+// 0 <= A_l X_h < 2 B^n), so it is known from T mod (B^L - 1) for any
+// L >= n + 2: with E' = (T - B^(n+h)) mod (B^L - 1) in [0, B^L - 1),
+// T = B^(n+h) + E' if E' < B^L / 2, else B^(n+h) - (B^L - 1 - E').  The
+// product itself is the cyclic convolution of length L (the FFT form of the
+// middle product), carried into L + 3 limbs and folded here.
+__global__ void __launch_bounds__(DIV_T) k_recip_wrap(const RecipStep* st, uint32_t* err) {
+    const RecipStep S = st[blockIdx.x];
+    if (S.L == 0) return;
+    const int64_t n = S.n, h = S.h, L = S.L, sft = n + h - L;   // 0 <= sft < L
+    uint64_t* C = S.C;
+    // fold: C mod (B^L - 1) = C[0..L) + C[L..L+3), end-around carry
+    const uint32_t c = block_addsub(C, L, [&](int64_t i) { return C[i]; },
+                                    [&](int64_t i) { return i < 3 ? C[L + i] : 0ull; }, false, 0);
+    __syncthreads();
+    if (c && block_step1(C, L, true)) {     // B^L = 1 again: the value is 1
+        if (threadIdx.x == 0) C[0] = 1;
+    }
+    __syncthreads();
+    // E' = C - B^sft  (a borrow out means C < B^sft: E' = C - B^sft + B^L - 1)
+    const uint32_t b = block_addsub(C, L, [&](int64_t i) { return C[i]; },
+                                    [&](int64_t i) { return i == sft ? 1ull : 0ull; }, true, 0);
+    __syncthreads();
+    if (b) block_step1(C, L, false);
+    __syncthreads();
+    const bool neg = (C[L - 1] >> 63) != 0;
+    // |E| < 2 B^n: limbs n+1 .. L-1 of E' are 0 (E >= 0) or ~0 (E < 0)
+    if (threadIdx.x == 0 && L - 1 > n && C[L - 1] != (neg ? ~0ull : 0ull)) atomicOr(err, 128u);
+    uint64_t* T = S.T;
+    const int64_t tl = n + h + 1;
+    if (!neg) {
+        for (int64_t i = threadIdx.x; i < tl; i += DIV_T)
+            T[i] = i < L ? C[i] : (i == n + h ? 1ull : 0ull);
+    } else {
+        // T = B^(n+h) - |E| = (E' + 1) on the low L limbs, ~0 up to n+h-1, 0 on top
+        block_addsub(T, L, [&](int64_t i) { return C[i]; }, [&](int64_t i) { return 0ull; }, false, 1);
+        for (int64_t i = L + threadIdx.x; i < tl; i += DIV_T) T[i] = i == n + h ? 0ull : ~0ull;
+    }
 }
 
 // step 1: correct X_h while T >= B^(n+h); T_m = limbs l..n of B^(n+h) - T
@@ -443,16 +487,26 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
             S.U = d.U;
             S.n = n;
             S.h = h;
+            // the first product wrapped at a shorter length when one exists
+            // (result into U, which the second product overwrites later)
+            const int cfull = conv_lg(n + h, c->len3_mask), cwrap = conv_lg(n + 2, c->len3_mask);
+            if (code_len(cwrap) < code_len(cfull)) {
+                S.L = code_len(cwrap);
+                S.C = d.U;
+                jt.push_back(sbg_job{S.C, S.A, S.Xh, n, h + 1, SBG_JOB_CYCLIC, cwrap});
+            } else {
+                jt.push_back(sbg_job{S.T, S.A, S.Xh, n, h + 1, SBG_JOB_MUL, 0});
+            }
             steps.push_back(S);
-            jt.push_back(sbg_job{S.T, S.A, S.Xh, n, h + 1, SBG_JOB_MUL, 0});
             ju.push_back(sbg_job{d.U, S.TM, S.Xh, h + 1, h + 1, SBG_JOB_MUL, 0});
         }
         if (steps.empty()) continue;
         RecipStep* dsteps = nullptr;
         if ((rc = upload(c, steps, &dsteps))) break;
         if ((rc = enqueue_products(c, jt.data(), (int64_t)jt.size(), err))) break;
+        k_recip_wrap<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps, err);
         k_recip_step1<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps, err);
-        c->launches += 2;                      // step1 and step2
+        c->launches += 3;                      // wrap, step1 and step2
         if (cudaGetLastError() != cudaSuccess) { rc = SBG_ECUDA; break; }
         if ((rc = enqueue_products(c, ju.data(), (int64_t)ju.size(), err))) break;
         k_recip_step2<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps);

@@ -232,6 +232,12 @@ struct UploadRing {
     void release();
 };
 
+// Internal job kind (not in the public header): the cyclic convolution of
+// a (an limbs) and b (bn limbs) at the transform length code `reserved`
+// (an, bn <= L), its L coefficients carried into rp[0 .. L+3) -- the value
+// of which is a * b mod (B^L - 1) after an end-around fold.
+#define SBG_JOB_CYCLIC 0x43
+
 #define SBG_AUX_STREAMS 4
 // transforms up to 2^12 points run in one CTA per prime (k_small)
 #define SBG_SMALL_MAX_LG 12
