@@ -451,11 +451,13 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
         pg.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ctx.launches()
     e0.record(stream)
     for _ in range(args.steps):
         batch.run()
     e1.record(stream)
     ctx.sync()
+    batch_launches = ctx.launches() - l0
     ms_step = barrier_max(pg, e0.elapsed_time(e1), dev) / args.steps
     # one multiply per launch over the same batch
     L = sbg.lib()
@@ -520,8 +522,7 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
                      "peak_source": hbm_src, "alg_bytes_per_launch": alg_bytes},
         "clocks": clk,
     }
-    nclasses = len({max(4, (sbg.out_limbs(k, an, bn) - 2).bit_length()) for k, an, bn in shapes})
-    res["gpu_launches"] = int(args.steps * nclasses * 5)
+    res["gpu_launches"] = int(batch_launches)
     batch.close()
     ctx.close()
     return res
@@ -630,11 +631,52 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
     if pg is not None:
         pg.barrier()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    l0 = ctx.launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
     for _ in range(steps):
         ctx.divrem_batch(jobs)
+    e1.record(stream)
     torch.cuda.synchronize()
-    dt = barrier_max(pg, time.perf_counter() - t0, dev) / steps
+    launches = ctx.launches() - l0
+    dt = barrier_max(pg, e0.elapsed_time(e1) * 1e-3, dev) / steps
+    # end to end: numerators and divisors from one pinned host buffer, the
+    # quotients and remainders back into another, every step
+    offs_in, offs_out, ni, no = [], [], 0, 0
+    for n in ns:
+        offs_in.append(ni)
+        ni += 3 * n                                   # N (2n) then D (n)
+        offs_out.append(no)
+        no += 2 * n + 1                               # Q (n+1) then R (n)
+    h_in = torch.empty(ni, dtype=torch.int64).pin_memory()
+    hv = h_in.numpy().view(np.uint64)
+    for N, D, n, o in zip(hostN, hostD, ns, offs_in):
+        hv[o:o + 2 * n] = N
+        hv[o + 2 * n:o + 3 * n] = D
+    h_out = torch.empty(no, dtype=torch.int64).pin_memory()
+    d_in = torch.empty(ni, dtype=torch.int64, device=dev)
+    d_out = torch.empty(no, dtype=torch.int64, device=dev)
+    bi, bo = d_in.data_ptr(), d_out.data_ptr()
+    ejobs = [(bo + 8 * oo, bo + 8 * (oo + n + 1), bi + 8 * oi, bi + 8 * (oi + 2 * n), 2 * n, n)
+             for n, oi, oo in zip(ns, offs_in, offs_out)]
+    with torch.cuda.stream(stream):
+        d_in.copy_(h_in, non_blocking=True)
+        ctx.divrem_batch(ejobs)
+        h_out.copy_(d_out, non_blocking=True)
+        stream.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            d_in.copy_(h_in, non_blocking=True)
+            ctx.divrem_batch(ejobs)
+            h_out.copy_(d_out, non_blocking=True)
+        stream.synchronize()
+        e2e_s = barrier_max(pg, time.perf_counter() - t0, dev) / steps
+    ov = h_out.numpy().view(np.uint64)
+    for q, r, n, oo in zip(tQ, tR, ns, offs_out):
+        if not (np.array_equal(ov[oo:oo + n + 1], q.cpu().numpy().view(np.uint64)) and
+                np.array_equal(ov[oo + n + 1:oo + 2 * n + 1], r.cpu().numpy().view(np.uint64))):
+            exact = False
+            break
     clk = clocks.stop() if rank == 0 else None
     total = sum(2 * n for n in ns)
     if rank != 0:
@@ -650,7 +692,10 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
                    "numerator_limbs": total, "parallelism": f"replicas x{ws}"},
         "divisions_per_s": round(len(ns) * ws / dt, 1),
         "bit_exact": bool(exact),
-        "e2e": None, "gpu_launches": None, "roofline": None, "clocks": clk,
+        "e2e": {"value": round(total * ws / e2e_s / 1e6, 2), "unit": "Mlimb/s",
+                "h2d_bytes_per_step": int(ni * 8), "d2h_bytes_per_step": int(no * 8),
+                "entry": "sbg_divrem_batch between pinned host copies of all N, D in and Q, R out"},
+        "gpu_launches": int(launches), "roofline": None, "clocks": clk,
     }
     ctx.close()
     return res
