@@ -1,12 +1,16 @@
 // sbg_kernels.cu -- the transform pipeline of one product on the GPU.
 //
-//   u64 limbs --(K1 k_col_fwd: residues + column DIF + four-step twiddle)-->
-//   spectra   --(K2 k_row: row DIF of A and B, pointwise, row DIT)-->
-//   products  --(K3 k_col_inv: inverse twiddle + column DIT)-->
+//   u64 limbs --(K1 k_col_fwd: residues + column DIF)-->
+//   spectra   --(K2 k_row12: four-step twiddle, row DIF of A and B, pointwise,
+//                row DIT, inverse twiddle x CRT scale)-->
+//   products  --(K3 k_col_inv: column DIT)-->
 //   residues  --(K4 k_crt_carry: Garner CRT + 3-stream compose + carry scan)--> limbs
 //
-// Transforms of L <= 2^12 points skip the four-step split and run whole in
-// one CTA per prime (k_small).  This is the reference's p30 pipeline
+// A length-L sequence is an N1 x 4096 matrix (N1 = L / 4096 rows, 2^a or
+// 3 * 2^m): K1 / K3 transform its columns (tiles of adjacent columns, split
+// over thread-block clusters when a column is long; k_col3* for 3 * 2^m
+// rows), K2 its rows.  Transforms of L <= 2^12 points skip the four-step
+// split and run whole in one CTA per prime (k_small).  This is the reference's p30 pipeline
 // (include/p30.h:1847-1938: input -> forward -> fused pointwise+inverse ->
 // scale -> Garner/carry), laid out as a four-step NTT over HBM: every pass
 // reads and writes each spectrum once, all levels inside a pass stay on chip.
