@@ -189,7 +189,8 @@ struct RecipStep {
 struct DivFix {
     const uint64_t* N;      // 2n limbs
     const uint64_t* D;      // n limbs
-    const uint64_t* P;      // step q0: N_hi * V (2n limbs); step fix: Q0 * D (2n+1)
+    uint64_t* P;            // step q0: N_hi * V (2n limbs); step fix: Q0 * D (2n+1), or
+    int64_t L;              //   with L > 0 Q0 * D mod (B^L - 1) as L+3 unfolded limbs
     uint64_t* Q;            // n+1 limbs
     uint64_t* R;            // n limbs (remainder out)
     uint64_t* Rw;           // n+1 limbs of scratch
@@ -349,16 +350,63 @@ __global__ void __launch_bounds__(DIV_T) k_div_q0(const DivFix* df) {
                  [&](int64_t i) { return i < n ? P[n + i] : 0ull; }, false, 0);
 }
 
-// R = (N - Q0 D) on n+1 limbs, then while R >= D: R -= D, Q += 1
+// R = (N - Q0 D) on n+1 limbs, then while R >= D: R -= D, Q += 1.  With a
+// wrapped product (L >= n + 3): 0 <= R < 6 D < B^(n+1) is the residue of
+// N - C mod (B^L - 1), N folded to L limbs, C = Q0 D mod (B^L - 1).
 __global__ void __launch_bounds__(DIV_T) k_div_fix(const DivFix* df, uint32_t* err) {
     const DivFix F = df[blockIdx.x];
     const int64_t n = F.n;
     const uint64_t* N = F.N;
-    const uint64_t* P = F.P;
+    uint64_t* P = F.P;
     const uint64_t* D = F.D;
     uint64_t* Rw = F.Rw;
-    block_addsub(Rw, n + 1, [&](int64_t i) { return N[i]; }, [&](int64_t i) { return P[i]; }, true,
-                 0);
+    if (F.L == 0) {
+        block_addsub(Rw, n + 1, [&](int64_t i) { return N[i]; }, [&](int64_t i) { return P[i]; }, true,
+                     0);
+    } else {
+        const int64_t L = F.L;
+        // C = P[0..L) + P[L..L+3), end-around
+        uint32_t c = block_addsub(P, L, [&](int64_t i) { return P[i]; },
+                                  [&](int64_t i) { return i < 3 ? P[L + i] : 0ull; }, false, 0);
+        __syncthreads();
+        if (c && block_step1(P, L, true)) {
+            if (threadIdx.x == 0) P[0] = 1;
+        }
+        __syncthreads();
+        // N_lo - C (a borrow out adds B^L = 1 + (B^L - 1): take 1 back) ...
+        const uint32_t b1 = block_addsub(P, L, [&](int64_t i) { return N[i]; },
+                                         [&](int64_t i) { return P[i]; }, true, 0);
+        __syncthreads();
+        // ... + N_hi (limbs L .. 2n-1; a carry out is B^L = 1 + (B^L - 1): give 1)
+        const uint32_t c2 = block_addsub(P, L, [&](int64_t i) { return P[i]; },
+                                         [&](int64_t i) { return L + i < 2 * n ? N[L + i] : 0ull; }, false, 0);
+        __syncthreads();
+        if (c2 && !b1) {
+            if (block_step1(P, L, true) && threadIdx.x == 0) P[0] = 1;
+        } else if (b1 && !c2) {
+            block_step1(P, L, false);
+        }
+        __syncthreads();
+        // the value is R, or R + (B^L - 1) when R = 0 and the sum came out all ones
+        __shared__ int s_hi;
+        if (threadIdx.x == 0) s_hi = 0;
+        __syncthreads();
+        for (int64_t i = n + 1 + threadIdx.x; i < L; i += DIV_T)
+            if (P[i] != 0) s_hi = 1;
+        __syncthreads();
+        if (s_hi) {
+            __shared__ int s_ones;
+            if (threadIdx.x == 0) s_ones = 1;
+            __syncthreads();
+            for (int64_t i = threadIdx.x; i < L; i += DIV_T)
+                if (P[i] != ~0ull) s_ones = 0;
+            __syncthreads();
+            if (!s_ones && threadIdx.x == 0) atomicOr(err, 256u);
+            for (int64_t i = threadIdx.x; i <= n; i += DIV_T) Rw[i] = 0;
+        } else {
+            for (int64_t i = threadIdx.x; i <= n; i += DIV_T) Rw[i] = P[i];
+        }
+    }
     for (int it = 0; it < 8; ++it) {
         __syncthreads();
         int c = block_cmp(n + 1, [&](int64_t i) { return Rw[i]; },
@@ -419,6 +467,7 @@ struct DivInst {
     uint64_t* Q;
     uint64_t* Rw;
     std::vector<int64_t> sz;   // recursion sizes, sz[0] = n
+    int wrapq = -1;            // length code of the wrapped Q0 * D, or -1 (full product)
 };
 
 static int64_t h_of(int64_t n) { return n - (n - 1) / 2; }
@@ -521,6 +570,13 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
         F.N = d.N;
         F.D = d.D;
         F.P = d.P;
+        if (quotient) {             // Q0 D wrapped at a shorter length when there is one
+            const int cfull = conv_lg(2 * d.n, c->len3_mask), cwrap = conv_lg(d.n + 3, c->len3_mask);
+            if (code_len(cwrap) < code_len(cfull)) {
+                F.L = code_len(cwrap);
+                d.wrapq = cwrap;
+            }
+        }
         F.Q = d.Q;
         F.R = quotient ? d.Rout : d.Qout;
         F.Rw = d.Rw;
@@ -548,7 +604,9 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
         c->launches += 2;                      // q0 and fix
         if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
         std::vector<sbg_job> jq;
-        for (auto& d : v) jq.push_back(sbg_job{d.P, d.Q, d.D, d.n + 1, d.n, SBG_JOB_MUL, 0});
+        for (auto& d : v)
+            jq.push_back(d.wrapq >= 0 ? sbg_job{d.P, d.Q, d.D, d.n + 1, d.n, SBG_JOB_CYCLIC, d.wrapq}
+                                      : sbg_job{d.P, d.Q, d.D, d.n + 1, d.n, SBG_JOB_MUL, 0});
         if ((rc = enqueue_products(c, jq.data(), (int64_t)jq.size(), err))) return rc;
         k_div_fix<<<(int)fx.size(), DIV_T, 0, st>>>(dfx, err);
         if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
