@@ -1144,17 +1144,27 @@ __global__ void __launch_bounds__(256, ROW_MINB) k_row12_b(const JobDesc* __rest
 // window sum  sum_j c_j 2^(64 (j - off))  is
 //     z_m = lo_{m+off} + mid_{m+off-1} + hi_{m+off-2} + carry,
 // the reference's lo/mid/hi stream recombination (include/p30.h:1695-1842).
-// Each thread owns CRT_PER consecutive limbs, resolves the carries inside
-// them assuming carry-in 0 and writes them; the carry-in of every thread is
-// then found by a block scan plus a decoupled look-back across blocks (block
-// order from an atomic ticket, so every predecessor is already resident),
-// and threads whose carry-in is 1 ripple the +1 into their limbs.
+// Each warp owns CRT_SEG = 32 * CRT_PER consecutive limbs and walks them 32
+// at a time, lane l on limb seg + 32 s + l, so the residue loads and the
+// limb stores are coalesced.  The neighbour terms mid_{j-1}, hi_{j-2} and the
+// sum carry of the limb below come from the lanes below by a rotating
+// shuffle (lanes 0 and 1 keep the previous step's top lanes; a prologue of
+// three coefficients starts the segment).  Before carries, limb m is
+// z'_m = lo + mid + hi + (sum carry of limb m-1) mod 2^64; it generates a
+// carry (G) when that wraps and propagates one (P) when z'_m = 2^64 - 1.
+// With the 32 lanes' G and P as ballot masks g and p, the carries into the
+// lanes for a step carry-in c are  (p + (g << 1 | c)) ^ p : one 32-bit add
+// resolves a step.  The z' wait in shared memory while the warp's carry-in
+// is found: the steps' (G, P) compose to the warp's, and a block scan of the
+// warps plus a decoupled look-back across blocks (block order from an atomic
+// ticket, so every predecessor is already resident) give the block's.
 // ------------------------------------------------------------------------
 #define CRT_T 256
 #ifndef CRT_PER
-#define CRT_PER 16
+#define CRT_PER 16                          // 32-limb steps per warp
 #endif
-#define CRT_BLK (CRT_T * CRT_PER)
+#define CRT_SEG (32 * CRT_PER)              // limbs per warp
+#define CRT_BLK ((CRT_T / 32) * CRT_SEG)    // limbs per block
 #define LB_SPIN_LIMIT (1 << 22)
 #define FLAG_AGG 1u
 #define FLAG_INC 2u
@@ -1225,105 +1235,112 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
                                          int64_t cmin, int64_t cmax, int64_t off,
                                          uint64_t* __restrict__ out, int64_t nout,
                                          uint32_t* flags, uint32_t* err) {
+    __shared__ uint64_t s_z[CRT_BLK];                    // limbs before carries
+    __shared__ uint32_t s_gp[CRT_T / 32][CRT_PER][2];    // per warp and step: g, p
     __shared__ uint32_t s_warp[CRT_T / 32];
     __shared__ uint32_t s_cin;
-    const int64_t m0 = (int64_t)bid * CRT_BLK + (int64_t)threadIdx.x * CRT_PER;
-    const int64_t j0 = m0 + off;
-    // residues of coefficients j0-4 .. j0+15 arrive in 5 chunks of 4: one
-    // 16-byte load per prime when aligned and in range, else guarded scalars
-    const bool vec = ((j0 & 3) == 0) && (j0 >= 4) && (j0 + CRT_PER <= L);
-    uint32_t rr[SBG_NP][4];
-    auto fetch = [&](int c) {
-        const int64_t jb = j0 - 4 + 4 * c;
-        if (vec) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int src1 = (lane + 31) & 31, src2 = (lane + 30) & 31;
+    const int64_t seg = (int64_t)bid * CRT_BLK + (int64_t)wid * CRT_SEG;
+    uint64_t* zs = s_z + wid * CRT_SEG;
+    // residues of limb m's coefficient j = m + off; zero outside [cmin, cmax],
+    // which Garner maps to lo = mid = hi = 0
+    auto fetch = [&](int64_t m, uint32_t (&r)[SBG_NP]) {
+        const int64_t j = m + off;
+        const bool in = j >= cmin && j <= cmax;
 #pragma unroll
-            for (int q = 0; q < SBG_NP; ++q) {
-                uint4 v = __ldg(reinterpret_cast<const uint4*>(R + (size_t)q * L + jb));
-                rr[q][0] = v.x; rr[q][1] = v.y; rr[q][2] = v.z; rr[q][3] = v.w;
-            }
-        } else {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int64_t j = jb + u;
-                const bool in = j >= cmin && j <= cmax;
-#pragma unroll
-                for (int q = 0; q < SBG_NP; ++q) rr[q][u] = in ? __ldg(&R[(size_t)q * L + j]) : 0u;
-            }
-        }
+        for (int q = 0; q < SBG_NP; ++q) r[q] = in ? __ldg(&R[(size_t)q * L + j]) : 0u;
     };
-    auto coeff = [&](int u, int64_t j, uint64_t& lo, uint64_t& mid, uint32_t& hi) {
-        if (j >= cmin && j <= cmax) {
-            uint32_t r[SBG_NP];
-#pragma unroll
-            for (int q = 0; q < SBG_NP; ++q) r[q] = rr[q][u];
+    uint64_t lo, mid;
+    uint32_t hi;
+    // prologue: lanes 29..31 rebuild the coefficients of limbs seg-3 .. seg-1
+    // for the first step's neighbour terms and the sum carry of limb seg-1
+    uint64_t c_mid;             // lane 0: mid of the limb below the step
+    uint32_t c_hi;              // lanes 0, 1: hi two limbs below
+    uint32_t c_kk;              // lane 0: sum carry of the limb below
+    {
+        uint32_t r[SBG_NP];
+        if (lane >= 29) {
+            fetch(seg - 32 + lane, r);
             garner(r, lo, mid, hi);
         } else {
-            lo = 0; mid = 0; hi = 0;
+            lo = 0;
+            mid = 0;
+            hi = 0;
         }
-    };
-    uint64_t lo_a, mid_a, lo_b, mid_b, lo_c, mid_c;   // a = j-2, b = j-1, c = j
-    uint32_t hi_a, hi_b, hi_c;
-    fetch(0);
-    coeff(1, j0 - 3, lo_a, mid_a, hi_a);
-    coeff(2, j0 - 2, lo_b, mid_b, hi_b);
-    coeff(3, j0 - 1, lo_c, mid_c, hi_c);
-    // kk of limb m0 - 1: S = lo_{j0-1} + mid_{j0-2} + hi_{j0-3}
-    uint32_t kk_prev;
-    {
-        uint64_t s1 = lo_c + mid_b;
-        uint32_t c1 = s1 < lo_c;
-        uint64_t s2 = s1 + hi_a;
-        c1 += s2 < s1;
-        kk_prev = (m0 - 1 >= 0) ? c1 : 0u;
+        const uint64_t mid1 = __shfl_sync(FULL, mid, src1);
+        const uint32_t hi2 = __shfl_sync(FULL, hi, src2);
+        const uint64_t s1 = lo + mid1;
+        uint32_t k = s1 < lo;
+        const uint64_t y = s1 + hi2;
+        k += y < s1;
+        c_mid = mid1;
+        c_hi = hi2;
+        c_kk = __shfl_sync(FULL, k, src1);
+        if (seg - 1 < 0) c_kk = 0;      // limb -1 carries nothing into limb 0
     }
-    uint32_t carry = 0;         // in-thread carry, assuming thread carry-in 0
-    uint32_t pmask = 0;         // bit k: z0_k == ~0
-    int nreal = 0;              // limbs < nout owned and written
-    bool has_v = false;         // owns limb nout (the spill limb, never stored)
-    uint64_t zv = 0;
-    uint32_t kv = 0;
+    uint32_t wG = 0, wP = 1;            // the warp's (G, P) so far: identity
+    uint64_t zv = 0;                    // the spill limb nout, before carries
+    uint32_t vbad = 0;                  //   and what it must not carry out
+    uint32_t r0[SBG_NP], r1[SBG_NP];    // residues two steps ahead
+    fetch(seg + lane, r0);
+    fetch(seg + 32 + lane, r1);
+#pragma unroll 2
+    for (int s = 0; s < CRT_PER; ++s) {
+        const int64_t m = seg + 32 * s + lane;
+        uint32_t rc[SBG_NP];
 #pragma unroll
-    for (int k = 0; k < CRT_PER; ++k) {
-        const int64_t m = m0 + k;
-        if (m > nout) break;
-        if ((k & 3) == 0) fetch(1 + (k >> 2));
-        lo_a = lo_b; mid_a = mid_b; hi_a = hi_b;
-        lo_b = lo_c; mid_b = mid_c; hi_b = hi_c;
-        coeff(k & 3, j0 + k, lo_c, mid_c, hi_c);
-        uint64_t s1 = lo_c + mid_b;
-        uint32_t c1 = s1 < lo_c;
-        uint64_t t = s1 + hi_a;
-        c1 += t < s1;
-        uint64_t y = t + kk_prev;
-        uint32_t g = y < t;
-        uint64_t z = y + carry;
-        uint32_t g2 = z < y;
-        kk_prev = c1;
-        if (m == nout) {
-            has_v = true;
-            zv = z;
-            kv = c1;
-            break;
+        for (int q = 0; q < SBG_NP; ++q) {
+            rc[q] = r0[q];
+            r0[q] = r1[q];
         }
-        carry = g | g2;
-        out[m] = z;
-        if (z == ~0ull) pmask |= 1u << k;
-        nreal = k + 1;
+        if (s + 2 < CRT_PER) fetch(m + 64, r1);
+        garner(rc, lo, mid, hi);
+        uint64_t mid1 = __shfl_sync(FULL, mid, src1);
+        uint32_t hi2 = __shfl_sync(FULL, hi, src2);
+        const uint64_t n_mid = mid1;    // lane 0: this step's lane 31
+        const uint32_t n_hi = hi2;      // lanes 0, 1: this step's lanes 30, 31
+        if (lane == 0) mid1 = c_mid;
+        if (lane < 2) hi2 = c_hi;
+        c_mid = n_mid;
+        c_hi = n_hi;
+        const uint64_t s1 = lo + mid1;
+        uint32_t k = s1 < lo;
+        const uint64_t y = s1 + hi2;
+        k += y < s1;
+        uint32_t kkp = __shfl_sync(FULL, k, src1);
+        const uint32_t n_kk = kkp;
+        if (lane == 0) kkp = c_kk;
+        c_kk = n_kk;
+        const uint64_t z = y + kkp;
+        uint32_t G = z < y, P = z == ~0ull;
+        if (m < nout) {
+            zs[32 * s + lane] = z;
+        } else {
+            if (m == nout) {            // must end zero with no carry beyond it
+                zv = z;
+                vbad = G | k;
+            }
+            G = 0;
+            P = 0;
+        }
+        const uint32_t g = __ballot_sync(FULL, G), p = __ballot_sync(FULL, P);
+        if (lane == 0) {
+            s_gp[wid][s][0] = g;
+            s_gp[wid][s][1] = p;
+        }
+        // the step's own (G, P): carry out with carry-in 0; all lanes propagate
+        const uint32_t sG = (uint32_t)(((uint64_t)p + (g << 1)) >> 32) | (g >> 31);
+        const uint32_t sP = p == FULL;
+        wG = sG | (sP & wG);
+        wP = sP & wP;
     }
-    uint32_t P = (pmask == ((nreal == 32) ? ~0u : ((1u << nreal) - 1u))) ? 1u : 0u;
-    uint32_t G = nreal > 0 ? carry : 0u;
-    uint32_t gp = G | (P << 1);
-
-    // block scan (exclusive) of gp
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t inc = gp;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        uint32_t o = __shfl_up_sync(0xffffffffu, inc, d);
-        if (lane >= d) inc = gp_compose(o, inc);
-    }
-    if (lane == 31) s_warp[wid] = inc;
+    const uint32_t gp = wG | (wP << 1);
+    if (lane == 0) s_warp[wid] = gp;
     __syncthreads();
+
+    // block scan of the warps' (G, P), then the look-back
     if (wid == 0) {
         uint32_t wv = lane < CRT_T / 32 ? s_warp[lane] : 2u;   // identity = (G0, P1)
         uint32_t wi = wv;
@@ -1383,25 +1400,23 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
         }
     }
     __syncthreads();
-    // thread carry-in = exclusive prefix applied to the block carry-in
-    uint32_t excl;
-    {
-        uint32_t prev_in_warp = __shfl_up_sync(0xffffffffu, inc, 1);
-        uint32_t wpre = (wid > 0) ? s_warp[wid - 1] : 2u;
-        excl = (lane > 0) ? gp_compose(wpre, prev_in_warp) : wpre;
-    }
-    uint32_t tcin = (excl & 1u) | (((excl >> 1) & 1u) & s_cin);
-    for (int k = 0; k < nreal && tcin; ++k) {
-        const int64_t m = m0 + k;
-        if ((pmask >> k) & 1u) {
-            out[m] = 0;
-        } else {
-            out[m] = out[m] + 1;
-            tcin = 0;
+    // warp carry-in, then each step's carries from its g, p masks
+    const uint32_t wpre = (wid > 0) ? s_warp[wid - 1] : 2u;
+    uint32_t cin = (wpre & 1u) | ((wpre >> 1) & s_cin);
+#pragma unroll 4
+    for (int s = 0; s < CRT_PER; ++s) {
+        const int64_t m = seg + 32 * s + lane;
+        const uint32_t g = s_gp[wid][s][0], p = s_gp[wid][s][1];
+        const uint64_t sum = (uint64_t)p + ((g << 1) | cin);
+        const uint32_t c = (((uint32_t)sum ^ p) >> lane) & 1u;
+        if (m < nout) {
+            out[m] = zs[32 * s + lane] + c;
+        } else if (m == nout) {
+            const uint64_t zf = zv + c;
+            if (vbad | (zf != 0) | (zf < zv)) atomicOr(err, 2u);
         }
+        cin = (uint32_t)(sum >> 32) | (g >> 31);
     }
-    // limb nout must come out zero, with no carry beyond it
-    if (has_v && ((zv | (uint64_t)tcin | (uint64_t)kv) != 0)) atomicOr(err, 2u);
 }
 
 // Block order comes from an atomic ticket (flags[0]), not blockIdx, so every
