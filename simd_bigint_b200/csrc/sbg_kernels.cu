@@ -1144,27 +1144,33 @@ __global__ void __launch_bounds__(256, ROW_MINB) k_row12_b(const JobDesc* __rest
 // window sum  sum_j c_j 2^(64 (j - off))  is
 //     z_m = lo_{m+off} + mid_{m+off-1} + hi_{m+off-2} + carry,
 // the reference's lo/mid/hi stream recombination (include/p30.h:1695-1842).
-// Each warp owns CRT_SEG = 32 * CRT_PER consecutive limbs and walks them 32
-// at a time, lane l on limb seg + 32 s + l, so the residue loads and the
-// limb stores are coalesced.  The neighbour terms mid_{j-1}, hi_{j-2} and the
-// sum carry of the limb below come from the lanes below by a rotating
-// shuffle (lanes 0 and 1 keep the previous step's top lanes; a prologue of
-// three coefficients starts the segment).  Before carries, limb m is
-// z'_m = lo + mid + hi + (sum carry of limb m-1) mod 2^64; it generates a
-// carry (G) when that wraps and propagates one (P) when z'_m = 2^64 - 1.
-// With the 32 lanes' G and P as ballot masks g and p, the carries into the
-// lanes for a step carry-in c are  (p + (g << 1 | c)) ^ p : one 32-bit add
-// resolves a step.  The z' wait in shared memory while the warp's carry-in
-// is found: the steps' (G, P) compose to the warp's, and a block scan of the
+// Each warp owns CRT_SEG consecutive limbs and walks them 128 at a time,
+// lane l on the four limbs seg + 128 s + 4 l + (0..3): the residue loads are
+// one 16-byte vector per prime and the limb stores two 16-byte vectors, all
+// coalesced across the warp.  The neighbour terms (mid and hi of the lane
+// below's top coefficients, and the sum carry of its top limb) come by a
+// rotating shuffle; lane 0 keeps the previous step's lane 31 values, and a
+// prologue of three coefficients starts the segment.  Before carries, limb m
+// is z'_m = lo + mid + hi + (sum carry of limb m-1) mod 2^64; it generates
+// a carry (G) when that wraps and propagates one (P) when z'_m = 2^64 - 1.
+// For G and P bit masks g, p (exclusive per position) the carries into the
+// positions for carry-in c are  (p + (g << 1 | c)) ^ p,  one add: over a
+// lane's four limbs, and over the warp's 32 lanes with the lanes' (G, P) as
+// ballot masks.  The z' wait in shared memory while the warp's carry-in is
+// found: the steps' (G, P) compose to the warp's, and a block scan of the
 // warps plus a decoupled look-back across blocks (block order from an atomic
 // ticket, so every predecessor is already resident) give the block's.
 // ------------------------------------------------------------------------
 #define CRT_T 256
-#ifndef CRT_PER
-#define CRT_PER 16                          // 32-limb steps per warp
+#define CRT_V 4                                 // consecutive limbs per lane and step
+#ifndef CRT_NSTEP
+#define CRT_NSTEP 4                             // steps per warp
 #endif
-#define CRT_SEG (32 * CRT_PER)              // limbs per warp
-#define CRT_BLK ((CRT_T / 32) * CRT_SEG)    // limbs per block
+#define CRT_SEG (32 * CRT_V * CRT_NSTEP)        // limbs per warp
+#ifndef CRT_MINB
+#define CRT_MINB 4                              // blocks per SM (64 registers)
+#endif
+#define CRT_BLK ((CRT_T / 32) * CRT_SEG)        // limbs per block
 #define LB_SPIN_LIMIT (1 << 22)
 #define FLAG_AGG 1u
 #define FLAG_INC 2u
@@ -1231,106 +1237,139 @@ __device__ __forceinline__ uint32_t gp_compose(uint32_t left, uint32_t right) {
     return (gr | (pr & gl)) | ((pr & pl) << 1);
 }
 
+// y + k 2^64 = lo + mid + hi  (k <= 2)
+__device__ __forceinline__ void sum3(uint64_t lo, uint64_t mid, uint32_t hi, uint64_t& y, uint32_t& k) {
+    const uint64_t s1 = lo + mid;
+    k = s1 < lo;
+    y = s1 + hi;
+    k += y < s1;
+}
+
 __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restrict__ R, int64_t L,
                                          int64_t cmin, int64_t cmax, int64_t off,
                                          uint64_t* __restrict__ out, int64_t nout,
                                          uint32_t* flags, uint32_t* err) {
-    __shared__ uint64_t s_z[CRT_BLK];                    // limbs before carries
-    __shared__ uint32_t s_gp[CRT_T / 32][CRT_PER][2];    // per warp and step: g, p
+    __shared__ ulonglong2 s_z[CRT_BLK / 2];              // limbs before carries
+    __shared__ uint32_t s_gp[CRT_T / 32][CRT_NSTEP][2];  // per warp and step: g, p
     __shared__ uint32_t s_warp[CRT_T / 32];
     __shared__ uint32_t s_cin;
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int src1 = (lane + 31) & 31, src2 = (lane + 30) & 31;
+    const int src1 = (lane + 31) & 31;
     const int64_t seg = (int64_t)bid * CRT_BLK + (int64_t)wid * CRT_SEG;
-    uint64_t* zs = s_z + wid * CRT_SEG;
-    // residues of limb m's coefficient j = m + off; zero outside [cmin, cmax],
-    // which Garner maps to lo = mid = hi = 0
-    auto fetch = [&](int64_t m, uint32_t (&r)[SBG_NP]) {
+    ulonglong2* zs = s_z + wid * (CRT_SEG / 2);         // unit (2 s + half) * 32 + lane
+    // residues of the coefficients j = m + off of limbs m .. m+3; zero outside
+    // [cmin, cmax], which Garner maps to lo = mid = hi = 0
+    auto fetch4 = [&](int64_t m, uint32_t (&r)[CRT_V][SBG_NP]) {
         const int64_t j = m + off;
-        const bool in = j >= cmin && j <= cmax;
+        if (((j & 3) == 0) && j >= cmin && j + 3 <= cmax) {
 #pragma unroll
-        for (int q = 0; q < SBG_NP; ++q) r[q] = in ? __ldg(&R[(size_t)q * L + j]) : 0u;
-    };
-    uint64_t lo, mid;
-    uint32_t hi;
-    // prologue: lanes 29..31 rebuild the coefficients of limbs seg-3 .. seg-1
-    // for the first step's neighbour terms and the sum carry of limb seg-1
-    uint64_t c_mid;             // lane 0: mid of the limb below the step
-    uint32_t c_hi;              // lanes 0, 1: hi two limbs below
-    uint32_t c_kk;              // lane 0: sum carry of the limb below
-    {
-        uint32_t r[SBG_NP];
-        if (lane >= 29) {
-            fetch(seg - 32 + lane, r);
-            garner(r, lo, mid, hi);
+            for (int q = 0; q < SBG_NP; ++q) {
+                const uint4 v = __ldg(reinterpret_cast<const uint4*>(R + (size_t)q * L + j));
+                r[0][q] = v.x;
+                r[1][q] = v.y;
+                r[2][q] = v.z;
+                r[3][q] = v.w;
+            }
         } else {
-            lo = 0;
-            mid = 0;
-            hi = 0;
+#pragma unroll
+            for (int k = 0; k < CRT_V; ++k) {
+                const bool in = j + k >= cmin && j + k <= cmax;
+#pragma unroll
+                for (int q = 0; q < SBG_NP; ++q) r[k][q] = in ? __ldg(&R[(size_t)q * L + j + k]) : 0u;
+            }
         }
-        const uint64_t mid1 = __shfl_sync(FULL, mid, src1);
-        const uint32_t hi2 = __shfl_sync(FULL, hi, src2);
-        const uint64_t s1 = lo + mid1;
-        uint32_t k = s1 < lo;
-        const uint64_t y = s1 + hi2;
-        k += y < s1;
-        c_mid = mid1;
-        c_hi = hi2;
-        c_kk = __shfl_sync(FULL, k, src1);
-        if (seg - 1 < 0) c_kk = 0;      // limb -1 carries nothing into limb 0
+    };
+    // what lane 0 takes from below: mid and hi of the limb below, hi two
+    // below, the sum carry of the limb below.  Prologue: lanes 29..31 rebuild
+    // the coefficients of limbs seg-3 .. seg-1.
+    uint64_t c_mid3;
+    uint32_t c_hi2, c_hi3, c_k3;
+    {
+        uint64_t lo = 0, mid = 0;
+        uint32_t hi = 0;
+        if (lane >= 29) {
+            uint32_t r[SBG_NP];
+            const int64_t j = seg - 32 + lane + off;
+            const bool in = j >= cmin && j <= cmax;
+#pragma unroll
+            for (int q = 0; q < SBG_NP; ++q) r[q] = in ? __ldg(&R[(size_t)q * L + j]) : 0u;
+            garner(r, lo, mid, hi);
+        }
+        uint64_t y;
+        uint32_t k;
+        sum3(lo, __shfl_up_sync(FULL, mid, 1), __shfl_up_sync(FULL, hi, 2), y, k);
+        c_mid3 = __shfl_sync(FULL, mid, 31);
+        c_hi2 = __shfl_sync(FULL, hi, 30);
+        c_hi3 = __shfl_sync(FULL, hi, 31);
+        c_k3 = __shfl_sync(FULL, k, 31);
+        if (seg - 1 < 0) c_k3 = 0;      // limb -1 carries nothing into limb 0
     }
     uint32_t wG = 0, wP = 1;            // the warp's (G, P) so far: identity
-    uint64_t zv = 0;                    // the spill limb nout, before carries
-    uint32_t vbad = 0;                  //   and what it must not carry out
-    uint32_t r0[SBG_NP], r1[SBG_NP];    // residues two steps ahead
-    fetch(seg + lane, r0);
-    fetch(seg + 32 + lane, r1);
-#pragma unroll 2
-    for (int s = 0; s < CRT_PER; ++s) {
-        const int64_t m = seg + 32 * s + lane;
-        uint32_t rc[SBG_NP];
+    uint32_t bits = 0;                  // per step: 4 G bits, 4 P bits
+    uint64_t zv = 0;                    // the spill limb nout, before carries,
+    uint32_t vbad = 0;                  //   what it must not carry out,
+    int vpos = -1;                      //   and where it sits (4 s + k)
 #pragma unroll
-        for (int q = 0; q < SBG_NP; ++q) {
-            rc[q] = r0[q];
-            r0[q] = r1[q];
-        }
-        if (s + 2 < CRT_PER) fetch(m + 64, r1);
-        garner(rc, lo, mid, hi);
-        uint64_t mid1 = __shfl_sync(FULL, mid, src1);
-        uint32_t hi2 = __shfl_sync(FULL, hi, src2);
-        const uint64_t n_mid = mid1;    // lane 0: this step's lane 31
-        const uint32_t n_hi = hi2;      // lanes 0, 1: this step's lanes 30, 31
-        if (lane == 0) mid1 = c_mid;
-        if (lane < 2) hi2 = c_hi;
-        c_mid = n_mid;
-        c_hi = n_hi;
-        const uint64_t s1 = lo + mid1;
-        uint32_t k = s1 < lo;
-        const uint64_t y = s1 + hi2;
-        k += y < s1;
-        uint32_t kkp = __shfl_sync(FULL, k, src1);
-        const uint32_t n_kk = kkp;
-        if (lane == 0) kkp = c_kk;
-        c_kk = n_kk;
-        const uint64_t z = y + kkp;
-        uint32_t G = z < y, P = z == ~0ull;
-        if (m < nout) {
-            zs[32 * s + lane] = z;
-        } else {
-            if (m == nout) {            // must end zero with no carry beyond it
-                zv = z;
-                vbad = G | k;
+    for (int s = 0; s < CRT_NSTEP; ++s) {
+        const int64_t m0 = seg + 128 * s + 4 * lane;
+        uint32_t r[CRT_V][SBG_NP];
+        fetch4(m0, r);
+        // top coefficients first: the lane above needs them
+        uint64_t lo3, mid3, lo2, mid2;
+        uint32_t hi3, hi2;
+        garner(r[3], lo3, mid3, hi3);
+        garner(r[2], lo2, mid2, hi2);
+        const uint64_t n_mid3 = __shfl_sync(FULL, mid3, src1);
+        const uint32_t n_hi2 = __shfl_sync(FULL, hi2, src1);
+        const uint32_t n_hi3 = __shfl_sync(FULL, hi3, src1);
+        const uint64_t b_mid3 = lane == 0 ? c_mid3 : n_mid3;
+        const uint32_t b_hi2 = lane == 0 ? c_hi2 : n_hi2;
+        const uint32_t b_hi3 = lane == 0 ? c_hi3 : n_hi3;
+        c_mid3 = n_mid3;                // lane 0: this step's lane 31
+        c_hi2 = n_hi2;
+        c_hi3 = n_hi3;
+        uint64_t lo0, mid0, lo1, mid1;
+        uint32_t hi0, hi1;
+        garner(r[0], lo0, mid0, hi0);
+        garner(r[1], lo1, mid1, hi1);
+        uint64_t y[CRT_V];
+        uint32_t kk[CRT_V];
+        sum3(lo0, b_mid3, b_hi2, y[0], kk[0]);
+        sum3(lo1, mid0, b_hi3, y[1], kk[1]);
+        sum3(lo2, mid1, hi0, y[2], kk[2]);
+        sum3(lo3, mid2, hi1, y[3], kk[3]);
+        const uint32_t n_k3 = __shfl_sync(FULL, kk[3], src1);
+        const uint32_t b_k3 = lane == 0 ? c_k3 : n_k3;
+        c_k3 = n_k3;
+        uint64_t z[CRT_V];
+        uint32_t gb = 0, pb = 0;
+#pragma unroll
+        for (int k = 0; k < CRT_V; ++k) {
+            z[k] = y[k] + (k == 0 ? b_k3 : kk[k - 1]);
+            uint32_t G = z[k] < y[k], P = z[k] == ~0ull;
+            if (m0 + k >= nout) {
+                if (m0 + k == nout) {   // must end zero with no carry beyond it
+                    zv = z[k];
+                    vbad = G | kk[k];
+                    vpos = CRT_V * s + k;
+                }
+                G = 0;
+                P = 0;
             }
-            G = 0;
-            P = 0;
+            gb |= G << k;
+            pb |= P << k;
         }
-        const uint32_t g = __ballot_sync(FULL, G), p = __ballot_sync(FULL, P);
+        zs[(2 * s) * 32 + lane] = make_ulonglong2(z[0], z[1]);
+        zs[(2 * s + 1) * 32 + lane] = make_ulonglong2(z[2], z[3]);
+        bits |= (gb | (pb << 4)) << (8 * s);
+        // the lane's (G, P) over its limbs, then the warp's for the step
+        const uint32_t lG = (pb + (gb << 1)) >> CRT_V, lP = pb == (1u << CRT_V) - 1u;
+        const uint32_t g = __ballot_sync(FULL, lG), p = __ballot_sync(FULL, lP);
         if (lane == 0) {
             s_gp[wid][s][0] = g;
             s_gp[wid][s][1] = p;
         }
-        // the step's own (G, P): carry out with carry-in 0; all lanes propagate
         const uint32_t sG = (uint32_t)(((uint64_t)p + (g << 1)) >> 32) | (g >> 31);
         const uint32_t sP = p == FULL;
         wG = sG | (sP & wG);
@@ -1400,28 +1439,42 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
         }
     }
     __syncthreads();
-    // warp carry-in, then each step's carries from its g, p masks
+    // warp carry-in, then each step's carries: into the lanes from the g, p
+    // masks, into each lane's limbs from its own bits
     const uint32_t wpre = (wid > 0) ? s_warp[wid - 1] : 2u;
     uint32_t cin = (wpre & 1u) | ((wpre >> 1) & s_cin);
-#pragma unroll 4
-    for (int s = 0; s < CRT_PER; ++s) {
-        const int64_t m = seg + 32 * s + lane;
+    const bool al16 = (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+#pragma unroll
+    for (int s = 0; s < CRT_NSTEP; ++s) {
         const uint32_t g = s_gp[wid][s][0], p = s_gp[wid][s][1];
         const uint64_t sum = (uint64_t)p + ((g << 1) | cin);
         const uint32_t c = (((uint32_t)sum ^ p) >> lane) & 1u;
-        if (m < nout) {
-            out[m] = zs[32 * s + lane] + c;
-        } else if (m == nout) {
-            const uint64_t zf = zv + c;
+        cin = (uint32_t)(sum >> 32) | (g >> 31);
+        const uint32_t gb = (bits >> (8 * s)) & 15u, pb = (bits >> (8 * s + 4)) & 15u;
+        const uint32_t cm = (pb + ((gb << 1) | c)) ^ pb;
+        const ulonglong2 z01 = zs[(2 * s) * 32 + lane], z23 = zs[(2 * s + 1) * 32 + lane];
+        const uint64_t z0 = z01.x + (cm & 1u), z1 = z01.y + ((cm >> 1) & 1u);
+        const uint64_t z2 = z23.x + ((cm >> 2) & 1u), z3 = z23.y + ((cm >> 3) & 1u);
+        const int64_t m0 = seg + 128 * s + 4 * lane;
+        if (al16 && m0 + 3 < nout) {
+            *reinterpret_cast<ulonglong2*>(out + m0) = make_ulonglong2(z0, z1);
+            *reinterpret_cast<ulonglong2*>(out + m0 + 2) = make_ulonglong2(z2, z3);
+        } else {
+            if (m0 < nout) out[m0] = z0;
+            if (m0 + 1 < nout) out[m0 + 1] = z1;
+            if (m0 + 2 < nout) out[m0 + 2] = z2;
+            if (m0 + 3 < nout) out[m0 + 3] = z3;
+        }
+        if (vpos >= CRT_V * s && vpos < CRT_V * (s + 1)) {
+            const uint64_t zf = zv + ((cm >> (vpos - CRT_V * s)) & 1u);
             if (vbad | (zf != 0) | (zf < zv)) atomicOr(err, 2u);
         }
-        cin = (uint32_t)(sum >> 32) | (g >> 31);
     }
 }
 
 // Block order comes from an atomic ticket (flags[0]), not blockIdx, so every
 // block's look-back predecessors were scheduled before it.
-__global__ void __launch_bounds__(CRT_T) k_crt_carry(const uint32_t* __restrict__ R, int64_t L,
+__global__ void __launch_bounds__(CRT_T, CRT_MINB) k_crt_carry(const uint32_t* __restrict__ R, int64_t L,
                                                      int64_t cmin, int64_t cmax, int64_t off,
                                                      uint64_t* __restrict__ out, int64_t nout,
                                                      uint32_t* flags, uint32_t* err) {
@@ -1433,7 +1486,7 @@ __global__ void __launch_bounds__(CRT_T) k_crt_carry(const uint32_t* __restrict_
 
 // batched: blocks_per_job CTAs per job (enough for the longest output of the
 // launch); each takes a ticket on its own job's counter, surplus ones exit.
-__global__ void __launch_bounds__(CRT_T) k_crt_carry_b(const JobDesc* __restrict__ jobs, int64_t L,
+__global__ void __launch_bounds__(CRT_T, CRT_MINB) k_crt_carry_b(const JobDesc* __restrict__ jobs, int64_t L,
                                                        int blocks_per_job, uint32_t* err) {
     __shared__ uint32_t s_bid;
     const JobDesc& J = jobs[blockIdx.x / blocks_per_job];
