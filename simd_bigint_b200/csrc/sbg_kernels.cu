@@ -207,17 +207,21 @@ __device__ __forceinline__ int padded_at(int i0, int t) {
     }
 }
 
+// Operand limbs and residue rows stream through a CTA once: they are loaded
+// L2-only (ld.global.cg) so that they do not evict the twiddle tables, which
+// every pass re-reads, from L1.
+//
 // two limbs of row n (columns c, c+1) -> residues; zero beyond xn
 __device__ __forceinline__ void load_limb_pair(const uint64_t* __restrict__ X, int64_t xn, int64_t n,
                                                bool al16, const PrimeConst& pc, uint32_t& x,
                                                uint32_t& y) {
     if (al16 && n + 1 < xn) {
-        ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(X + n));
+        ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(X + n));
         x = limb_residue(v.x, pc);
         y = limb_residue(v.y, pc);
     } else {
-        x = n < xn ? limb_residue(__ldg(&X[n]), pc) : 0u;
-        y = n + 1 < xn ? limb_residue(__ldg(&X[n + 1]), pc) : 0u;
+        x = n < xn ? limb_residue(__ldcg(&X[n]), pc) : 0u;
+        y = n + 1 < xn ? limb_residue(__ldcg(&X[n + 1]), pc) : 0u;
     }
 }
 
@@ -274,7 +278,7 @@ __device__ __forceinline__ void col_pass_pair(uint32_t* sm, const uint64_t* __re
 #pragma unroll
                 for (int t = 0; t < R; ++t) {
                     const int64_t n = n0 + ((int64_t)(ST * t) << SBG_ROW_LG);
-                    uint2 v = *reinterpret_cast<const uint2*>(Y + n);
+                    uint2 v = __ldcg(reinterpret_cast<const uint2*>(Y + n));
                     x[t] = v.x;
                     y[t] = v.y;
                 }
@@ -313,7 +317,7 @@ __device__ __forceinline__ void col_pass_pair(uint32_t* sm, const uint64_t* __re
 
 __device__ __forceinline__ uint32_t load_limb(const uint64_t* __restrict__ X, int64_t xn, int64_t n,
                                               const PrimeConst& pc) {
-    return n < xn ? limb_residue(__ldg(&X[n]), pc) : 0u;
+    return n < xn ? limb_residue(__ldcg(&X[n]), pc) : 0u;
 }
 
 // Pass K of the lane-per-column mapping (a warp = 32 adjacent columns of one
@@ -355,7 +359,7 @@ __device__ __forceinline__ void col_pass_lane(uint32_t* sm, const uint64_t* __re
                 if constexpr (FWD)
                     x[t] = load_limb(X, xn, n, pc);
                 else
-                    x[t] = Y[n];
+                    x[t] = __ldcg(&Y[n]);
             }
         } else {
             const uint32_t* s0 = sm + col * LD + i0;
@@ -1031,8 +1035,8 @@ __device__ __forceinline__ void row_body(int q, int row, uint32_t* __restrict__ 
 #pragma unroll
         for (int t = 0; t < 16; ++t) {
             uint2 s = s_f[t];
-            xa[t] = mul_shoup(mul_shoup(Ar[tid + 256 * t], s.x, s.y, p), bf, bfs, p);
-            if (!sq) xb[t] = mul_shoup(mul_shoup(__ldg(&Br[tid + 256 * t]), s.x, s.y, p), bf, bfs, p);
+            xa[t] = mul_shoup(mul_shoup(__ldcg(&Ar[tid + 256 * t]), s.x, s.y, p), bf, bfs, p);
+            if (!sq) xb[t] = mul_shoup(mul_shoup(__ldcg(&Br[tid + 256 * t]), s.x, s.y, p), bf, bfs, p);
         }
         if (sq) {
             dif_regs<16>(xa, tf, tid, 256, 12, p);
