@@ -249,21 +249,15 @@ __device__ __forceinline__ void col_pass_pair(uint32_t* sm, const uint64_t* __re
     for (int it = 0; it < ITER; ++it) {
         const int gid = threadIdx.x + it * COL_THREADS;
         if (TOTAL < COL_THREADS && gid >= TOTAL) break;
-        // passes that touch global memory put the column pairs of a row
-        // fastest (a warp covers W/2 pairs x 64/W rows: few row pieces per
-        // access); shared-memory-only passes put consecutive groups fastest
-        int j0, blk, cp;
-        if constexpr (SRC_G || DST_G) {
-            cp = gid & ((1 << (LGW - 1)) - 1);
-            const int rest = gid >> (LGW - 1);
-            j0 = rest & (ST - 1);
-            blk = rest >> LGST;
-        } else {
-            j0 = gid & (ST - 1);
-            const int rest = gid >> LGST;
-            blk = rest & ((1 << (LGS - LGM)) - 1);
-            cp = rest >> (LGS - LGM);
-        }
+        // column pairs of a row fastest: a warp covers W/2 pairs x 64/W rows,
+        // few row pieces per global access, and in the planes (stride
+        // padded length + 32/W) its accesses fall in distinct banks for the
+        // radix-16 passes (consecutive groups fastest would put 32
+        // consecutive rows across a padding step: two-way conflicts)
+        const int cp = gid & ((1 << (LGW - 1)) - 1);
+        const int rest = gid >> (LGW - 1);
+        const int j0 = rest & (ST - 1);
+        const int blk = rest >> LGST;
         const int i0 = (blk << LGM) + j0;
         const int g0 = 2 * cp;
         uint32_t x[R], y[R];
