@@ -38,92 +38,87 @@ namespace sbg {
 #define DIV_TILE (DIV_T * DIV_PER)
 
 // ---------------------------------------------------------------------------
-// block-wide multi-limb add / sub with carry scan (one CTA, tiles of 4096)
+// block-wide multi-limb add / sub with carry scan (one CTA, tiles of DIV_TILE)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t gp2(uint32_t left, uint32_t right) {
     uint32_t gl = left & 1, pl = (left >> 1) & 1, gr = right & 1, pr = (right >> 1) & 1;
     return (gr | (pr & gl)) | ((pr & pl) << 1);
 }
 
-// exclusive block scan of (G, P) pairs; returns this thread's prefix and
-// writes the block total to *total (all threads)
-__device__ __forceinline__ uint32_t block_scan_gp(uint32_t gp, uint32_t* total) {
-    __shared__ uint32_t s_w[DIV_T / 32];
-    __shared__ uint32_t s_tot;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t inc = gp;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        uint32_t o = __shfl_up_sync(0xffffffffu, inc, d);
-        if (lane >= d) inc = gp2(o, inc);
-    }
-    if (lane == 31) s_w[wid] = inc;
-    __syncthreads();
-    if (wid == 0) {
-        uint32_t v = s_w[lane];
-        uint32_t iv = v;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            uint32_t o = __shfl_up_sync(0xffffffffu, iv, d);
-            if (lane >= d) iv = gp2(o, iv);
-        }
-        s_w[lane] = iv;
-        if (lane == 31) s_tot = iv;
-    }
-    __syncthreads();
-    uint32_t prev = __shfl_up_sync(0xffffffffu, inc, 1);
-    uint32_t wpre = wid > 0 ? s_w[wid - 1] : 2u;
-    uint32_t excl = lane > 0 ? gp2(wpre, prev) : wpre;
-    *total = s_tot;
-    __syncthreads();
-    return excl;
-}
-
 // z[0..len) = x +/- y (+ cin / - bin), x(i), y(i) limb accessors (0 beyond
 // their length); returns the carry / borrow out.  z may alias x or y limb
-// for limb.
+// for limb (limb i is read and written by the same thread).
+//
+// A warp takes 32 * DIV_PER consecutive limbs of a tile as DIV_PER rows of
+// 32, lane l on limb row * 32 + l, so every load and store is coalesced.
+// Per row, with the lanes' generate (G) and propagate (P) bits as ballot
+// masks g, p, the carries into the 32 limbs for row carry-in c are
+// (p + (g << 1 | c)) ^ p, and the row passes on (p + (g << 1 | c)) >> 32 |
+// g >> 31.  The rows' (G, P) compose to the warp's, and a block scan of the
+// warps' gives each warp its carry-in.
 template <class FX, class FY>
 __device__ uint32_t block_addsub(uint64_t* z, int64_t len, FX x, FY y, bool sub, uint32_t cin) {
+    __shared__ uint32_t s_w[DIV_T / 32];
+    __shared__ uint32_t s_tot;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint32_t carry = cin;
     for (int64_t base = 0; base < len; base += DIV_TILE) {
-        const int64_t i0 = base + (int64_t)threadIdx.x * DIV_PER;
+        const int64_t w0 = base + (int64_t)wid * (32 * DIV_PER) + lane;
         uint64_t s[DIV_PER];
-        uint32_t gmask = 0, pmask = 0;
+        uint32_t g[DIV_PER], p[DIV_PER];
+        uint32_t wG = 0, wP = 1;
 #pragma unroll
         for (int k = 0; k < DIV_PER; ++k) {
-            const int64_t i = i0 + k;
-            uint64_t a = i < len ? x(i) : 0, b = i < len ? y(i) : 0;
+            const int64_t i = w0 + 32 * k;
+            const bool in = i < len;
+            const uint64_t a = in ? x(i) : 0, b = in ? y(i) : 0;
+            uint64_t d;
+            bool G, P;
+            // limbs past len propagate, so the carry out is that of limb len-1
             if (sub) {
-                uint64_t d = a - b;
-                s[k] = d;
-                if (a < b) gmask |= 1u << k;          // borrow generated
-                if (d == 0 && i < len) pmask |= 1u << k;   // borrow propagates
+                d = a - b;
+                G = a < b;                     // borrow generated
+                P = !in || d == 0;             // borrow propagates
             } else {
-                uint64_t d = a + b;
-                s[k] = d;
-                if (d < a) gmask |= 1u << k;
-                if (d == ~0ull && i < len) pmask |= 1u << k;
+                d = a + b;
+                G = d < a;
+                P = !in || d == ~0ull;
             }
+            s[k] = d;
+            g[k] = __ballot_sync(FULL, G);
+            p[k] = __ballot_sync(FULL, P);
+            const uint32_t rG = (uint32_t)(((uint64_t)p[k] + (g[k] << 1)) >> 32) | (g[k] >> 31);
+            const uint32_t rP = p[k] == FULL;
+            wG = rG | (rP & wG);
+            wP = rP & wP;
         }
-        // thread aggregate over its DIV_PER limbs (in order)
-        uint32_t G = 0, P = 1;
+        if (lane == 0) s_w[wid] = wG | (wP << 1);
+        __syncthreads();
+        if (wid == 0) {
+            uint32_t iv = lane < DIV_T / 32 ? s_w[lane] : 2u;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t o = __shfl_up_sync(FULL, iv, d);
+                if (lane >= d) iv = gp2(o, iv);
+            }
+            if (lane < DIV_T / 32) s_w[lane] = iv;     // inclusive warp prefixes
+            if (lane == 31) s_tot = iv;
+        }
+        __syncthreads();
+        const uint32_t wpre = wid > 0 ? s_w[wid - 1] : 2u;
+        uint32_t c = (wpre & 1u) | ((wpre >> 1) & carry);
 #pragma unroll
         for (int k = 0; k < DIV_PER; ++k) {
-            uint32_t g = (gmask >> k) & 1, p = (pmask >> k) & 1;
-            G = g | (p & G);
-            P = p & P;
+            const int64_t i = w0 + 32 * k;
+            const uint64_t sum = (uint64_t)p[k] + ((g[k] << 1) | c);
+            const uint64_t cl = ((uint32_t)sum ^ p[k]) >> lane & 1u;
+            if (i < len) z[i] = sub ? s[k] - cl : s[k] + cl;
+            c = (uint32_t)(sum >> 32) | (g[k] >> 31);
         }
-        uint32_t tot;
-        uint32_t excl = block_scan_gp(G | (P << 1), &tot);
-        uint32_t c = (excl & 1) | (((excl >> 1) & 1) & carry);
-#pragma unroll
-        for (int k = 0; k < DIV_PER; ++k) {
-            const int64_t i = i0 + k;
-            if (i < len) z[i] = sub ? s[k] - c : s[k] + c;
-            uint32_t g = (gmask >> k) & 1, p = (pmask >> k) & 1;
-            c = g | (p & c);
-        }
-        carry = (tot & 1) | (((tot >> 1) & 1) & carry);
+        const uint32_t tot = s_tot;
+        carry = (tot & 1u) | ((tot >> 1) & carry);
+        __syncthreads();                 // s_w, s_tot reused by the next tile
     }
     return carry;
 }
