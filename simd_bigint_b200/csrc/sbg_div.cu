@@ -484,6 +484,35 @@ static int upload(sbg_ctx* c, const std::vector<T>& host, T** dev) {
     return st;
 }
 
+// Batched limb copies, dst[0..n_dst) = src[0..n_src) zero-extended: the
+// padded numerators in, the quotients or reciprocals out -- one launch for a
+// whole batch instead of a copy (and a fill) per division.
+struct CopyDesc {
+    const uint64_t* src;
+    uint64_t* dst;
+    int64_t n_src, n_dst;
+};
+#define COPY_BPD 8          // blocks per descriptor
+__global__ void __launch_bounds__(256) k_copy_pad(const CopyDesc* d) {
+    const CopyDesc D = d[blockIdx.x / COPY_BPD];
+    const int64_t stride = (int64_t)COPY_BPD * blockDim.x;
+    for (int64_t i = (int64_t)(blockIdx.x % COPY_BPD) * blockDim.x + threadIdx.x; i < D.n_dst; i += stride)
+        D.dst[i] = i < D.n_src ? D.src[i] : 0ull;
+}
+static int copy_batch(sbg_ctx* c, const std::vector<CopyDesc>& cp) {
+    for (size_t first = 0; first < cp.size(); first += 4096) {
+        const size_t cnt = std::min<size_t>(4096, cp.size() - first);
+        std::vector<CopyDesc> part(cp.begin() + first, cp.begin() + first + cnt);
+        CopyDesc* dd = nullptr;
+        int rc = upload(c, part, &dd);
+        if (rc) return rc;
+        k_copy_pad<<<(unsigned)(cnt * COPY_BPD), 256, 0, c->stream>>>(dd);
+        c->launches += 1;
+        if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
+    }
+    return SBG_OK;
+}
+
 // Reciprocals (and optionally quotients) of every instance; all scratch set.
 static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quotient) {
     cudaStream_t st = c->stream;
@@ -560,6 +589,7 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
     // final stage: exact reciprocal, or quotient and remainder
     std::vector<DivFix> fx;
     std::vector<sbg_job> jp;
+    std::vector<CopyDesc> cpx;
     for (auto& d : v) {
         DivFix F{};
         F.N = d.N;
@@ -582,11 +612,11 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
             // P = N_hi * V, V = low n limbs of X
             jp.push_back(sbg_job{d.P, d.N + d.n, X, d.n, d.n, SBG_JOB_MUL, 0});
         } else {
-            if (cudaMemcpyAsync(d.Q, X, (d.n + 1) * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-                return SBG_ECUDA;
+            cpx.push_back(CopyDesc{X, d.Q, d.n + 1, d.n + 1});
             jp.push_back(sbg_job{d.P, d.D, X, d.n, d.n + 1, SBG_JOB_MUL, 0});
         }
     }
+    if (!cpx.empty() && (rc = copy_batch(c, cpx))) return rc;
     DivFix* dfx = nullptr;
     if ((rc = upload(c, fx, &dfx))) return rc;
     if ((rc = enqueue_products(c, jp.data(), (int64_t)jp.size(), err))) return rc;
@@ -605,9 +635,10 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
         if ((rc = enqueue_products(c, jq.data(), (int64_t)jq.size(), err))) return rc;
         k_div_fix<<<(int)fx.size(), DIV_T, 0, st>>>(dfx, err);
         if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
-        for (auto& d : v)
-            if (cudaMemcpyAsync(d.Qout, d.Q, d.qlen * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-                return SBG_ECUDA;
+        std::vector<CopyDesc> cq;
+        cq.reserve(v.size());
+        for (auto& d : v) cq.push_back(CopyDesc{d.Q, d.Qout, d.qlen, d.qlen});
+        if ((rc = copy_batch(c, cq))) return rc;
     }
     return SBG_OK;
 }
@@ -687,7 +718,6 @@ extern "C" int sbg_recip(sbg_ctx* c, uint64_t* ip, const uint64_t* dp, int64_t n
 // shapes go through sbg_divrem, which normalises and splits them.
 extern "C" int sbg_divrem_batch(sbg_ctx* c, const sbg_div_job* jobs, int64_t count) {
     if (!c || (count > 0 && !jobs) || count < 0) return SBG_EINVAL;
-    cudaStream_t st = (cudaStream_t)sbg_ctx_get_stream(c);
     size_t total = 0;
     for (int64_t i = 0; i < count; ++i) {
         const sbg_div_job& j = jobs[i];
@@ -701,8 +731,9 @@ extern "C" int sbg_divrem_batch(sbg_ctx* c, const sbg_div_job* jobs, int64_t cou
     int rc = div_scratch(c, total, &scratch);
     if (rc) return rc;
     std::vector<DivInst> v((size_t)count);
+    std::vector<CopyDesc> cn((size_t)count);
     uint64_t* p = scratch;
-    for (int64_t i = 0; i < count && !rc; ++i) {
+    for (int64_t i = 0; i < count; ++i) {
         const sbg_div_job& j = jobs[i];
         DivInst& d = v[i];
         d.D = j.dp;
@@ -710,15 +741,14 @@ extern "C" int sbg_divrem_batch(sbg_ctx* c, const sbg_div_job* jobs, int64_t cou
         d.Qout = j.qp;
         d.Rout = j.rp;
         d.qlen = j.nn - j.dn + 1;
-        // numerator zero-padded to 2n limbs
+        // numerator zero-padded to 2n limbs (one batched copy below)
         uint64_t* Np = p;
         p += 2 * j.dn + 8;
-        if (cudaMemsetAsync(Np, 0, 2 * j.dn * 8, st) != cudaSuccess ||
-            cudaMemcpyAsync(Np, j.np, j.nn * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-            rc = SBG_ECUDA;
+        cn[i] = CopyDesc{j.np, Np, j.nn, 2 * j.dn};
         d.N = Np;
         carve(d, p);
     }
+    rc = copy_batch(c, cn);
     if (!rc) rc = div_core(c, v, c->derr, true);
     rc = div_finish(c, rc);
     if (getenv("SBG_DEBUG") && rc)
