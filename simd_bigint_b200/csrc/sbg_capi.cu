@@ -221,7 +221,9 @@ int UploadRing::push(const void* src, size_t bytes, cudaStream_t st, void** dev)
         head = 0;
         if (need > cap) {
             release();
-            const size_t nc = std::max(need * 4, (size_t)8 << 20);
+            // 32 MB: a 1024-division batch uploads about 4.5 MB of descriptors,
+            // so the ring wraps (and drains the stream) once every few calls
+            const size_t nc = std::max(need * 4, (size_t)32 << 20);
             if (cudaHostAlloc(&h, nc, 0) != cudaSuccess) return SBG_EALLOC;
             if (cudaMalloc(&d, nc) != cudaSuccess) {
                 cudaFreeHost(h);
