@@ -21,6 +21,7 @@
 // (within 5 of floor(N / D)), R = N - Q0 D, then at most five (R -= D, Q += 1)
 // steps.  The linear steps (borrow/carry chains, compares) run one CTA per
 // division with a block-wide carry scan.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -32,13 +33,74 @@
 #include "sbg_internal.h"
 
 namespace sbg {
+namespace cg = cooperative_groups;
 
 #define DIV_T 1024           // threads of the per-division linear kernels
 #define DIV_PER 8            // limbs per thread per tile
 #define DIV_TILE (DIV_T * DIV_PER)
+// Divisions with n >= DIV_CL_MIN_N run their linear steps on a thread-block
+// cluster of DIV_CL CTAs (one CTA otherwise): limb tiles go to the CTAs in
+// turn, and the cluster-wide carries and decisions are combined through
+// distributed shared memory, so the largest divisions -- the last Newton
+// rounds, where few divisions remain -- spread over DIV_CL SMs.
+#define DIV_CL 8
+#define DIV_CL_MIN_N 32768
+
+// The CTA group of one division: its rank, a barrier over all of its
+// threads (release / acquire: global and shared memory written before it
+// are visible after it), and cross-CTA exchange slots.  Every CTA of a
+// group takes the same path through a kernel, so the slots' parity stays in
+// step; a slot is rewritten only two exchanges later, after a barrier that
+// follows every CTA's reads of it.
+template <int CL>
+struct Grp {
+    long long* slot;        // two words of the kernel's shared memory
+    int par = 0;
+    unsigned rank = 0;
+    __device__ explicit Grp(long long* s) : slot(s) {
+        if constexpr (CL > 1) rank = cg::this_cluster().block_rank();
+    }
+    __device__ void sync() {
+        if constexpr (CL == 1) {
+            __syncthreads();
+        } else {
+            asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+            asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+        }
+    }
+    // publish this CTA's value (uniform in the CTA), then value k of CTA k
+    __device__ const long long* publish(long long v) {
+        long long* s = slot + par;
+        if (threadIdx.x == 0) *s = v;
+        sync();
+        par ^= 1;
+        return s;
+    }
+    __device__ long long peer(const long long* s, int k) const {
+        if constexpr (CL == 1) {
+            return *s;
+        } else {
+            return *cg::this_cluster().map_shared_rank(s, k);
+        }
+    }
+    __device__ long long max_all(long long v) {
+        if constexpr (CL == 1) return v;
+        const long long* s = publish(v);
+        long long r = peer(s, 0);
+        for (int k = 1; k < CL; ++k) r = max(r, peer(s, k));
+        return r;
+    }
+    __device__ long long min_all(long long v) {
+        if constexpr (CL == 1) return v;
+        const long long* s = publish(v);
+        long long r = peer(s, 0);
+        for (int k = 1; k < CL; ++k) r = min(r, peer(s, k));
+        return r;
+    }
+};
 
 // ---------------------------------------------------------------------------
-// block-wide multi-limb add / sub with carry scan (one CTA, tiles of DIV_TILE)
+// group-wide multi-limb add / sub with carry scan
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t gp2(uint32_t left, uint32_t right) {
     uint32_t gl = left & 1, pl = (left >> 1) & 1, gr = right & 1, pr = (right >> 1) & 1;
@@ -49,22 +111,24 @@ __device__ __forceinline__ uint32_t gp2(uint32_t left, uint32_t right) {
 // their length); returns the carry / borrow out.  z may alias x or y limb
 // for limb (limb i is read and written by the same thread).
 //
-// A warp takes 32 * DIV_PER consecutive limbs of a tile as DIV_PER rows of
-// 32, lane l on limb row * 32 + l, so every load and store is coalesced.
-// Per row, with the lanes' generate (G) and propagate (P) bits as ballot
-// masks g, p, the carries into the 32 limbs for row carry-in c are
-// (p + (g << 1 | c)) ^ p, and the row passes on (p + (g << 1 | c)) >> 32 |
-// g >> 31.  The rows' (G, P) compose to the warp's, and a block scan of the
-// warps' gives each warp its carry-in.
-template <class FX, class FY>
-__device__ uint32_t block_addsub(uint64_t* z, int64_t len, FX x, FY y, bool sub, uint32_t cin) {
+// A tile holds CL * DIV_TILE limbs, DIV_TILE per CTA.  A warp takes 32 *
+// DIV_PER consecutive limbs as DIV_PER rows of 32, lane l on limb row * 32
+// + l, so every load and store is coalesced.  Per row, with the lanes'
+// generate (G) and propagate (P) bits as ballot masks g, p, the carries into
+// the 32 limbs for row carry-in c are (p + (g << 1 | c)) ^ p, and the row
+// passes on (p + (g << 1 | c)) >> 32 | g >> 31.  The rows' (G, P) compose to
+// the warp's, a block scan of the warps' gives the CTA's, and the CTAs'
+// aggregates, composed in rank order, give each CTA its carry-in.
+template <int CL, class FX, class FY>
+__device__ uint32_t block_addsub(Grp<CL>& grp, uint64_t* z, int64_t len, FX x, FY y, bool sub,
+                                 uint32_t cin) {
     __shared__ uint32_t s_w[DIV_T / 32];
     __shared__ uint32_t s_tot;
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint32_t carry = cin;
-    for (int64_t base = 0; base < len; base += DIV_TILE) {
-        const int64_t w0 = base + (int64_t)wid * (32 * DIV_PER) + lane;
+    for (int64_t base = 0; base < len; base += (int64_t)CL * DIV_TILE) {
+        const int64_t w0 = base + (int64_t)grp.rank * DIV_TILE + (int64_t)wid * (32 * DIV_PER) + lane;
         uint64_t s[DIV_PER];
         uint32_t g[DIV_PER], p[DIV_PER];
         uint32_t wG = 0, wP = 1;
@@ -106,8 +170,23 @@ __device__ uint32_t block_addsub(uint64_t* z, int64_t len, FX x, FY y, bool sub,
             if (lane == 31) s_tot = iv;
         }
         __syncthreads();
+        uint32_t cta_cin = carry, next;
+        if constexpr (CL == 1) {
+            const uint32_t tot = s_tot;
+            next = (tot & 1u) | ((tot >> 1) & carry);
+        } else {
+            const long long* sl = grp.publish(s_tot);
+            uint32_t pre = 2u, all = 2u;
+            for (int k = 0; k < CL; ++k) {
+                const uint32_t v = (uint32_t)grp.peer(sl, k);
+                if (k < (int)grp.rank) pre = gp2(pre, v);
+                all = gp2(all, v);
+            }
+            cta_cin = (pre & 1u) | ((pre >> 1) & carry);
+            next = (all & 1u) | ((all >> 1) & carry);
+        }
         const uint32_t wpre = wid > 0 ? s_w[wid - 1] : 2u;
-        uint32_t c = (wpre & 1u) | ((wpre >> 1) & carry);
+        uint32_t c = (wpre & 1u) | ((wpre >> 1) & cta_cin);
 #pragma unroll
         for (int k = 0; k < DIV_PER; ++k) {
             const int64_t i = w0 + 32 * k;
@@ -116,26 +195,25 @@ __device__ uint32_t block_addsub(uint64_t* z, int64_t len, FX x, FY y, bool sub,
             if (i < len) z[i] = sub ? s[k] - cl : s[k] + cl;
             c = (uint32_t)(sum >> 32) | (g[k] >> 31);
         }
-        const uint32_t tot = s_tot;
-        carry = (tot & 1u) | ((tot >> 1) & carry);
+        carry = next;
         __syncthreads();                 // s_w, s_tot reused by the next tile
     }
     return carry;
 }
 
-// sign of x - y over len limbs: -1, 0, 1 (block-uniform).  Walks down from
-// the top one block-width at a time and stops at the first chunk holding a
-// difference (the top chunk, unless the operands agree there).
-template <class FX, class FY>
-__device__ int block_cmp(int64_t len, FX x, FY y) {
+// sign of x - y over len limbs: -1, 0, 1 (group-uniform).  Walks down from
+// the top CL * DIV_T limbs at a time and stops at the first window holding a
+// difference (the top one, unless the operands agree there).
+template <int CL, class FX, class FY>
+__device__ int block_cmp(Grp<CL>& grp, int64_t len, FX x, FY y) {
     __shared__ long long s_hi;
-    for (int64_t top = len; top > 0; top -= DIV_T) {
+    for (int64_t top = len; top > 0; top -= (int64_t)CL * DIV_T) {
         if (threadIdx.x == 0) s_hi = -1;
         __syncthreads();
-        const int64_t i = top - 1 - threadIdx.x;
+        const int64_t i = top - 1 - (int64_t)grp.rank * DIV_T - threadIdx.x;
         if (i >= 0 && x(i) != y(i)) atomicMax(&s_hi, (long long)i);
         __syncthreads();
-        const long long hi = s_hi;
+        const long long hi = grp.max_all(s_hi);
         __syncthreads();
         if (hi >= 0) return x(hi) > y(hi) ? 1 : -1;
     }
@@ -144,20 +222,21 @@ __device__ int block_cmp(int64_t len, FX x, FY y) {
 
 // z[0..len) += 1 (inc) or -= 1 in place: the carry / borrow ripples only
 // through the low limbs equal to ~0 / 0, so the pass stops at the first
-// limb that absorbs it (found one block-width at a time)
-__device__ bool block_step1(uint64_t* z, int64_t len, bool inc) {
+// limb that absorbs it (found CL * DIV_T limbs at a time).  The caller puts
+// a group barrier between this and any read of z by another CTA.
+template <int CL>
+__device__ bool block_step1(Grp<CL>& grp, uint64_t* z, int64_t len, bool inc) {
     __shared__ long long s_lo;
     const uint64_t ripple = inc ? ~0ull : 0ull;
-    for (int64_t base = 0; base < len; base += DIV_T) {
+    for (int64_t base = 0; base < len; base += (int64_t)CL * DIV_T) {
         if (threadIdx.x == 0) s_lo = len;
         __syncthreads();
-        const int64_t i = base + threadIdx.x;
+        const int64_t i = base + (int64_t)grp.rank * DIV_T + threadIdx.x;
         const bool stop = i < len && z[i] != ripple;
         if (stop) atomicMin(&s_lo, (long long)i);
         __syncthreads();
-        const long long lo = s_lo;
-        __syncthreads();
-        // limbs below lo (within this chunk) ripple; limb lo absorbs
+        const long long lo = grp.min_all(s_lo);
+        // limbs below lo (within this window) ripple; limb lo absorbs
         if (i < len && i < lo) z[i] = inc ? 0ull : ~0ull;
         if (i == lo) z[i] = inc ? z[i] + 1 : z[i] - 1;
         __syncthreads();
@@ -165,6 +244,10 @@ __device__ bool block_step1(uint64_t* z, int64_t len, bool inc) {
     }
     return true;                        // rippled out of the top limb
 }
+
+// a flag over the group: any (OR) or every (AND) CTA's
+template <int CL>
+__device__ bool grp_any(Grp<CL>& grp, bool v) { return grp.max_all(v ? 1 : 0) != 0; }
 
 // ---------------------------------------------------------------------------
 // per-division descriptors
@@ -251,47 +334,60 @@ __global__ void k_recip_base(const uint64_t* const* A, const int64_t* m, uint64_
 // T = B^(n+h) + E' if E' < B^L / 2, else B^(n+h) - (B^L - 1 - E').  The
 // product itself is the cyclic convolution of length L (the FFT form of the
 // middle product), carried into L + 3 limbs and folded here.
+//
+// Every linear kernel runs CL CTAs per division (descriptor blockIdx.x / CL);
+// limb-parallel loops spread over the group, and a group barrier separates
+// phases that read what another CTA wrote.
+#define GRP_LOOP(i, n) for (int64_t i = (int64_t)grp.rank * DIV_T + threadIdx.x; i < (n); i += (int64_t)CL * DIV_T)
+
+template <int CL>
 __global__ void __launch_bounds__(DIV_T) k_recip_wrap(const RecipStep* st, uint32_t* err) {
-    const RecipStep S = st[blockIdx.x];
-    if (S.L == 0) return;
+    __shared__ long long s_slot[2];
+    Grp<CL> grp(s_slot);
+    const RecipStep S = st[blockIdx.x / CL];
+    if (S.L == 0) return;                   // the whole group returns
     const int64_t n = S.n, h = S.h, L = S.L, sft = n + h - L;   // 0 <= sft < L
     uint64_t* C = S.C;
     // fold: C mod (B^L - 1) = C[0..L) + C[L..L+3), end-around carry
-    const uint32_t c = block_addsub(C, L, [&](int64_t i) { return C[i]; },
+    const uint32_t c = block_addsub(grp, C, L, [&](int64_t i) { return C[i]; },
                                     [&](int64_t i) { return i < 3 ? C[L + i] : 0ull; }, false, 0);
-    __syncthreads();
-    if (c && block_step1(C, L, true)) {     // B^L = 1 again: the value is 1
-        if (threadIdx.x == 0) C[0] = 1;
+    grp.sync();
+    if (c && block_step1(grp, C, L, true)) {    // B^L = 1 again: the value is 1
+        if (grp.rank == 0 && threadIdx.x == 0) C[0] = 1;
     }
-    __syncthreads();
+    grp.sync();
     // E' = C - B^sft  (a borrow out means C < B^sft: E' = C - B^sft + B^L - 1)
-    const uint32_t b = block_addsub(C, L, [&](int64_t i) { return C[i]; },
+    const uint32_t b = block_addsub(grp, C, L, [&](int64_t i) { return C[i]; },
                                     [&](int64_t i) { return i == sft ? 1ull : 0ull; }, true, 0);
-    __syncthreads();
-    if (b) block_step1(C, L, false);
-    __syncthreads();
+    grp.sync();
+    if (b) block_step1(grp, C, L, false);
+    grp.sync();
     const bool neg = (C[L - 1] >> 63) != 0;
     // |E| < 2 B^n: limbs n+1 .. L-1 of E' are 0 (E >= 0) or ~0 (E < 0)
     if (threadIdx.x == 0 && L - 1 > n && C[L - 1] != (neg ? ~0ull : 0ull)) atomicOr(err, 128u);
     uint64_t* T = S.T;
     const int64_t tl = n + h + 1;
     if (!neg) {
-        for (int64_t i = threadIdx.x; i < tl; i += DIV_T)
-            T[i] = i < L ? C[i] : (i == n + h ? 1ull : 0ull);
+        GRP_LOOP(i, tl) T[i] = i < L ? C[i] : (i == n + h ? 1ull : 0ull);
     } else {
         // T = B^(n+h) - |E| = (E' + 1) on the low L limbs, ~0 up to n+h-1, 0 on top
-        block_addsub(T, L, [&](int64_t i) { return C[i]; }, [&](int64_t i) { return 0ull; }, false, 1);
-        for (int64_t i = L + threadIdx.x; i < tl; i += DIV_T) T[i] = i == n + h ? 0ull : ~0ull;
+        block_addsub(grp, T, L, [&](int64_t i) { return C[i]; }, [&](int64_t i) { return 0ull; }, false, 1);
+        for (int64_t i = L + (int64_t)grp.rank * DIV_T + threadIdx.x; i < tl; i += (int64_t)CL * DIV_T)
+            T[i] = i == n + h ? 0ull : ~0ull;
     }
+    if constexpr (CL > 1) grp.sync();       // peers may still read this CTA's slots
 }
 
 // step 1: correct X_h while T >= B^(n+h); T_m = limbs l..n of B^(n+h) - T
+template <int CL>
 __global__ void __launch_bounds__(DIV_T) k_recip_step1(const RecipStep* st, uint32_t* err) {
-    const RecipStep S = st[blockIdx.x];
+    __shared__ long long s_slot[2];
+    Grp<CL> grp(s_slot);
+    const RecipStep S = st[blockIdx.x / CL];
     const int64_t n = S.n, h = S.h, l = n - h, tl = n + h + 1;
     // T - B^(n+h) < A_lo * X_h < 2 B^n <= 4 A: at most four corrections
     for (int it = 0; it < 6; ++it) {
-        __syncthreads();
+        grp.sync();
         if (S.T[n + h] == 0) break;
         if (it == 5) {
             if (threadIdx.x == 0) atomicOr(err, 16u);
@@ -299,145 +395,161 @@ __global__ void __launch_bounds__(DIV_T) k_recip_step1(const RecipStep* st, uint
         }
         const uint64_t* A = S.A;
         uint64_t* T = S.T;
-        block_addsub(T, tl, [&](int64_t i) { return T[i]; },
+        block_addsub(grp, T, tl, [&](int64_t i) { return T[i]; },
                      [&](int64_t i) { return i < n ? A[i] : 0ull; }, true, 0);
-        block_step1(S.Xh, h + 1, false);
+        block_step1(grp, S.Xh, h + 1, false);
     }
-    __syncthreads();
+    grp.sync();
     // B^(n+h) - T = (~T + 1) on the low n+1 limbs; the +1 reaches limb l only
     // when the limbs below l are all zero
     const uint64_t* T = S.T;
     __shared__ int s_nz;
     if (threadIdx.x == 0) s_nz = 0;
     __syncthreads();
-    for (int64_t i = threadIdx.x; i < l; i += DIV_T)
-        if (T[i] != 0) s_nz = 1;
+    GRP_LOOP(i, l) if (T[i] != 0) s_nz = 1;
     __syncthreads();
-    const uint32_t cin = s_nz ? 0u : 1u;
+    const uint32_t cin = grp_any(grp, s_nz != 0) ? 0u : 1u;
     uint64_t* TM = S.TM;
-    block_addsub(TM, h + 1, [&](int64_t i) { return ~T[l + i]; },
+    block_addsub(grp, TM, h + 1, [&](int64_t i) { return ~T[l + i]; },
                  [&](int64_t i) { return 0ull; }, false, cin);
+    if constexpr (CL > 1) grp.sync();
 }
 
 // step 2: X = X_h * B^l + floor(U / B^(2h-l))
+template <int CL>
 __global__ void __launch_bounds__(DIV_T) k_recip_step2(const RecipStep* st) {
-    const RecipStep S = st[blockIdx.x];
+    __shared__ long long s_slot[2];
+    Grp<CL> grp(s_slot);
+    const RecipStep S = st[blockIdx.x / CL];
     const int64_t n = S.n, h = S.h, l = n - h, sh = 2 * h - l;
     const uint64_t* U = S.U;
     const uint64_t* Xh = S.Xh;
     uint64_t* X = S.X;
     // U' = U >> sh limbs has l + 2 limbs (U has 2h + 2)
-    block_addsub(X, n + 1,
+    block_addsub(grp, X, n + 1,
                  [&](int64_t i) {
                      const int64_t k = sh + i;
                      return k < 2 * h + 2 ? U[k] : 0ull;
                  },
                  [&](int64_t i) { return i >= l ? Xh[i - l] : 0ull; }, false, 0);
+    if constexpr (CL > 1) grp.sync();
 }
 
 // Q0 = N_hi + floor(P / B^n), P = N_hi * V (2n limbs)
+template <int CL>
 __global__ void __launch_bounds__(DIV_T) k_div_q0(const DivFix* df) {
-    const DivFix F = df[blockIdx.x];
+    __shared__ long long s_slot[2];
+    Grp<CL> grp(s_slot);
+    const DivFix F = df[blockIdx.x / CL];
     const int64_t n = F.n;
     const uint64_t* Nh = F.N + n;
     const uint64_t* P = F.P;
-    block_addsub(F.Q, n + 1, [&](int64_t i) { return i < n ? Nh[i] : 0ull; },
+    block_addsub(grp, F.Q, n + 1, [&](int64_t i) { return i < n ? Nh[i] : 0ull; },
                  [&](int64_t i) { return i < n ? P[n + i] : 0ull; }, false, 0);
+    if constexpr (CL > 1) grp.sync();
 }
 
 // R = (N - Q0 D) on n+1 limbs, then while R >= D: R -= D, Q += 1.  With a
 // wrapped product (L >= n + 3): 0 <= R < 6 D < B^(n+1) is the residue of
 // N - C mod (B^L - 1), N folded to L limbs, C = Q0 D mod (B^L - 1).
+template <int CL>
 __global__ void __launch_bounds__(DIV_T) k_div_fix(const DivFix* df, uint32_t* err) {
-    const DivFix F = df[blockIdx.x];
+    __shared__ long long s_slot[2];
+    Grp<CL> grp(s_slot);
+    const DivFix F = df[blockIdx.x / CL];
     const int64_t n = F.n;
     const uint64_t* N = F.N;
     uint64_t* P = F.P;
     const uint64_t* D = F.D;
     uint64_t* Rw = F.Rw;
     if (F.L == 0) {
-        block_addsub(Rw, n + 1, [&](int64_t i) { return N[i]; }, [&](int64_t i) { return P[i]; }, true,
-                     0);
+        block_addsub(grp, Rw, n + 1, [&](int64_t i) { return N[i]; }, [&](int64_t i) { return P[i]; },
+                     true, 0);
     } else {
         const int64_t L = F.L;
         // C = P[0..L) + P[L..L+3), end-around
-        uint32_t c = block_addsub(P, L, [&](int64_t i) { return P[i]; },
+        uint32_t c = block_addsub(grp, P, L, [&](int64_t i) { return P[i]; },
                                   [&](int64_t i) { return i < 3 ? P[L + i] : 0ull; }, false, 0);
-        __syncthreads();
-        if (c && block_step1(P, L, true)) {
-            if (threadIdx.x == 0) P[0] = 1;
+        grp.sync();
+        if (c && block_step1(grp, P, L, true)) {
+            if (grp.rank == 0 && threadIdx.x == 0) P[0] = 1;
         }
-        __syncthreads();
+        grp.sync();
         // N_lo - C (a borrow out adds B^L = 1 + (B^L - 1): take 1 back) ...
-        const uint32_t b1 = block_addsub(P, L, [&](int64_t i) { return N[i]; },
+        const uint32_t b1 = block_addsub(grp, P, L, [&](int64_t i) { return N[i]; },
                                          [&](int64_t i) { return P[i]; }, true, 0);
-        __syncthreads();
+        grp.sync();
         // ... + N_hi (limbs L .. 2n-1; a carry out is B^L = 1 + (B^L - 1): give 1)
-        const uint32_t c2 = block_addsub(P, L, [&](int64_t i) { return P[i]; },
+        const uint32_t c2 = block_addsub(grp, P, L, [&](int64_t i) { return P[i]; },
                                          [&](int64_t i) { return L + i < 2 * n ? N[L + i] : 0ull; }, false, 0);
-        __syncthreads();
+        grp.sync();
         if (c2 && !b1) {
-            if (block_step1(P, L, true) && threadIdx.x == 0) P[0] = 1;
+            if (block_step1(grp, P, L, true) && grp.rank == 0 && threadIdx.x == 0) P[0] = 1;
         } else if (b1 && !c2) {
-            block_step1(P, L, false);
+            block_step1(grp, P, L, false);
+        }
+        grp.sync();
+        // the value is R, or R + (B^L - 1) when R = 0 and the sum came out all ones
+        __shared__ int s_hi, s_ones;
+        if (threadIdx.x == 0) {
+            s_hi = 0;
+            s_ones = 1;
         }
         __syncthreads();
-        // the value is R, or R + (B^L - 1) when R = 0 and the sum came out all ones
-        __shared__ int s_hi;
-        if (threadIdx.x == 0) s_hi = 0;
-        __syncthreads();
-        for (int64_t i = n + 1 + threadIdx.x; i < L; i += DIV_T)
+        for (int64_t i = n + 1 + (int64_t)grp.rank * DIV_T + threadIdx.x; i < L; i += (int64_t)CL * DIV_T)
             if (P[i] != 0) s_hi = 1;
         __syncthreads();
-        if (s_hi) {
-            __shared__ int s_ones;
-            if (threadIdx.x == 0) s_ones = 1;
+        if (grp_any(grp, s_hi != 0)) {
+            GRP_LOOP(i, L) if (P[i] != ~0ull) s_ones = 0;
             __syncthreads();
-            for (int64_t i = threadIdx.x; i < L; i += DIV_T)
-                if (P[i] != ~0ull) s_ones = 0;
-            __syncthreads();
-            if (!s_ones && threadIdx.x == 0) atomicOr(err, 256u);
-            for (int64_t i = threadIdx.x; i <= n; i += DIV_T) Rw[i] = 0;
+            if (grp_any(grp, s_ones == 0) && threadIdx.x == 0) atomicOr(err, 256u);
+            GRP_LOOP(i, n + 1) Rw[i] = 0;
         } else {
-            for (int64_t i = threadIdx.x; i <= n; i += DIV_T) Rw[i] = P[i];
+            GRP_LOOP(i, n + 1) Rw[i] = P[i];
         }
     }
     for (int it = 0; it < 8; ++it) {
-        __syncthreads();
-        int c = block_cmp(n + 1, [&](int64_t i) { return Rw[i]; },
+        grp.sync();
+        int c = block_cmp(grp, n + 1, [&](int64_t i) { return Rw[i]; },
                           [&](int64_t i) { return i < n ? D[i] : 0ull; });
         if (c < 0) break;
         if (it == 7) {
             if (threadIdx.x == 0) atomicOr(err, 32u);
             break;
         }
-        block_addsub(Rw, n + 1, [&](int64_t i) { return Rw[i]; },
+        block_addsub(grp, Rw, n + 1, [&](int64_t i) { return Rw[i]; },
                      [&](int64_t i) { return i < n ? D[i] : 0ull; }, true, 0);
-        block_step1(F.Q, n + 1, true);
+        block_step1(grp, F.Q, n + 1, true);
     }
-    __syncthreads();
-    for (int64_t i = threadIdx.x; i < n; i += DIV_T) F.R[i] = Rw[i];
+    grp.sync();
+    GRP_LOOP(i, n) F.R[i] = Rw[i];
+    if constexpr (CL > 1) grp.sync();
 }
 
 // recip output: V = X - B^n, +1 when B^2n - 1 - D X >= D (X exact in {V, V+1}),
 // computed from P = D * X (2n+1 limbs): R = complement of P's low n+1 limbs
+template <int CL>
 __global__ void __launch_bounds__(DIV_T) k_recip_final(const DivFix* df, uint32_t* err) {
-    const DivFix F = df[blockIdx.x];
+    __shared__ long long s_slot[2];
+    Grp<CL> grp(s_slot);
+    const DivFix F = df[blockIdx.x / CL];
     const int64_t n = F.n;
     const uint64_t* P = F.P;
     const uint64_t* D = F.D;
     uint64_t* Rw = F.Rw;
-    for (int64_t i = threadIdx.x; i <= n; i += DIV_T) Rw[i] = ~P[i];
-    __syncthreads();
-    int c = block_cmp(n + 1, [&](int64_t i) { return Rw[i]; },
+    GRP_LOOP(i, n + 1) Rw[i] = ~P[i];
+    grp.sync();
+    int c = block_cmp(grp, n + 1, [&](int64_t i) { return Rw[i]; },
                       [&](int64_t i) { return i < n ? D[i] : 0ull; });
     // Q holds X (n+1 limbs); V = X (+1) low n limbs
     uint64_t* Q = F.Q;
-    if (c >= 0) block_step1(Q, n + 1, true);
-    __syncthreads();
+    if (c >= 0) block_step1(grp, Q, n + 1, true);
+    grp.sync();
     if (threadIdx.x == 0 && Q[n] != 1) atomicOr(err, 64u);
-    for (int64_t i = threadIdx.x; i < n; i += DIV_T) F.R[i] = Q[i];
+    GRP_LOOP(i, n) F.R[i] = Q[i];
+    if constexpr (CL > 1) grp.sync();
 }
+#undef GRP_LOOP
 
 }  // namespace sbg
 
@@ -513,6 +625,33 @@ static int copy_batch(sbg_ctx* c, const std::vector<CopyDesc>& cp) {
     return SBG_OK;
 }
 
+// One linear step over a descriptor list ordered single-CTA divisions
+// first ([0, ns)), clustered ones after ([ns, ns + nb)): a launch per part.
+template <class D, class... KA, class... A>
+static int launch_lin(sbg_ctx* c, void (*k1)(const D*, KA...), void (*kc)(const D*, KA...), const D* d,
+                      int ns, int nb, A... a) {
+    if (ns > 0) {
+        k1<<<ns, DIV_T, 0, c->stream>>>(d, a...);
+        c->launches += 1;
+    }
+    if (nb > 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)nb * DIV_CL);
+        cfg.blockDim = dim3(DIV_T);
+        cfg.stream = c->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = DIV_CL;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        if (cudaLaunchKernelEx(&cfg, kc, d + ns, a...) != cudaSuccess) return SBG_ECUDA;
+        c->launches += 1;
+    }
+    return cudaGetLastError() == cudaSuccess ? SBG_OK : SBG_ECUDA;
+}
+
 // Reciprocals (and optionally quotients) of every instance; all scratch set.
 static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quotient) {
     cudaStream_t st = c->stream;
@@ -545,7 +684,7 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
     }
     for (int r = 1; r <= maxd && !rc; ++r) {
         std::vector<sbg_job> jt, ju;
-        std::vector<RecipStep> steps;
+        std::vector<RecipStep> steps, big;       // single-CTA divisions, clustered ones
         for (auto& d : v) {
             const int depth = (int)d.sz.size() - 1;
             if (depth < r) continue;
@@ -570,24 +709,26 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
             } else {
                 jt.push_back(sbg_job{S.T, S.A, S.Xh, n, h + 1, SBG_JOB_MUL, 0});
             }
-            steps.push_back(S);
+            (n >= DIV_CL_MIN_N ? big : steps).push_back(S);
             ju.push_back(sbg_job{d.U, S.TM, S.Xh, h + 1, h + 1, SBG_JOB_MUL, 0});
         }
-        if (steps.empty()) continue;
+        const int ns = (int)steps.size(), nb = (int)big.size();
+        if (ns + nb == 0) continue;
+        steps.insert(steps.end(), big.begin(), big.end());
         RecipStep* dsteps = nullptr;
         if ((rc = upload(c, steps, &dsteps))) break;
         if ((rc = enqueue_products(c, jt.data(), (int64_t)jt.size(), err))) break;
-        k_recip_wrap<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps, err);
-        k_recip_step1<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps, err);
-        c->launches += 3;                      // wrap, step1 and step2
-        if (cudaGetLastError() != cudaSuccess) { rc = SBG_ECUDA; break; }
+        if ((rc = launch_lin(c, k_recip_wrap<1>, k_recip_wrap<DIV_CL>, (const RecipStep*)dsteps, ns, nb, err)))
+            break;
+        if ((rc = launch_lin(c, k_recip_step1<1>, k_recip_step1<DIV_CL>, (const RecipStep*)dsteps, ns, nb, err)))
+            break;
         if ((rc = enqueue_products(c, ju.data(), (int64_t)ju.size(), err))) break;
-        k_recip_step2<<<(int)steps.size(), DIV_T, 0, st>>>(dsteps);
-        if (cudaGetLastError() != cudaSuccess) { rc = SBG_ECUDA; break; }
+        if ((rc = launch_lin(c, k_recip_step2<1>, k_recip_step2<DIV_CL>, (const RecipStep*)dsteps, ns, nb)))
+            break;
     }
     if (rc) return rc;
     // final stage: exact reciprocal, or quotient and remainder
-    std::vector<DivFix> fx;
+    std::vector<DivFix> fx, fxb;             // single-CTA divisions, clustered ones
     std::vector<sbg_job> jp;
     std::vector<CopyDesc> cpx;
     for (auto& d : v) {
@@ -606,7 +747,7 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
         F.R = quotient ? d.Rout : d.Qout;
         F.Rw = d.Rw;
         F.n = d.n;
-        fx.push_back(F);
+        (d.n >= DIV_CL_MIN_N ? fxb : fx).push_back(F);
         uint64_t* X = d.X[0];
         if (quotient) {
             // P = N_hi * V, V = low n limbs of X
@@ -617,24 +758,22 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
         }
     }
     if (!cpx.empty() && (rc = copy_batch(c, cpx))) return rc;
+    const int fs = (int)fx.size(), fb = (int)fxb.size();
+    fx.insert(fx.end(), fxb.begin(), fxb.end());
     DivFix* dfx = nullptr;
     if ((rc = upload(c, fx, &dfx))) return rc;
     if ((rc = enqueue_products(c, jp.data(), (int64_t)jp.size(), err))) return rc;
     if (!quotient) {
-        k_recip_final<<<(int)fx.size(), DIV_T, 0, st>>>(dfx, err);
-        c->launches += 1;
-        if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
+        if ((rc = launch_lin(c, k_recip_final<1>, k_recip_final<DIV_CL>, (const DivFix*)dfx, fs, fb, err)))
+            return rc;
     } else {
-        k_div_q0<<<(int)fx.size(), DIV_T, 0, st>>>(dfx);
-        c->launches += 2;                      // q0 and fix
-        if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
+        if ((rc = launch_lin(c, k_div_q0<1>, k_div_q0<DIV_CL>, (const DivFix*)dfx, fs, fb))) return rc;
         std::vector<sbg_job> jq;
         for (auto& d : v)
             jq.push_back(d.wrapq >= 0 ? sbg_job{d.P, d.Q, d.D, d.n + 1, d.n, SBG_JOB_CYCLIC, d.wrapq}
                                       : sbg_job{d.P, d.Q, d.D, d.n + 1, d.n, SBG_JOB_MUL, 0});
         if ((rc = enqueue_products(c, jq.data(), (int64_t)jq.size(), err))) return rc;
-        k_div_fix<<<(int)fx.size(), DIV_T, 0, st>>>(dfx, err);
-        if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
+        if ((rc = launch_lin(c, k_div_fix<1>, k_div_fix<DIV_CL>, (const DivFix*)dfx, fs, fb, err))) return rc;
         std::vector<CopyDesc> cq;
         cq.reserve(v.size());
         for (auto& d : v) cq.push_back(CopyDesc{d.Q, d.Qout, d.qlen, d.qlen});

@@ -142,3 +142,31 @@ def test_divrem_many_in_flight(ctx):
             assert (O.mod_u64(Q, p) * O.mod_u64(D, p) + O.mod_u64(R, p)) % p == O.mod_u64(N, p)
         hi = np.nonzero(R != D)[0]
         assert len(hi) and R[hi[-1]] < D[hi[-1]]
+
+
+def test_cluster_sized_divisions_extreme_carries(ctx):
+    """Divisions large enough for the clustered linear steps (n >= 32768),
+    with the carry-heaviest operands: an all-ones numerator over all-ones and
+    minimal (B^n / 2) divisors, checked as Q D + R = N with 0 <= R < D."""
+    n = 40000
+    ones = O.pattern(2 * n, "ones")
+    for D in (O.pattern(n, "ones"),
+              np.concatenate([np.zeros(n - 1, np.uint64), np.array([1 << 63], np.uint64)])):
+        q, r = _divrem(ctx, ones, D)
+        Nv, Dv, Qv, Rv = O.to_int(ones), O.to_int(D), O.to_int(q), O.to_int(r)
+        assert Qv * Dv + Rv == Nv and 0 <= Rv < Dv
+
+
+def test_cluster_sized_recip_exact(ctx):
+    """The exact reciprocal at a clustered size: V = floor((B^2n - 1) / D) - B^n
+    holds iff 0 <= B^2n - 1 - D (V + B^n) < D."""
+    import torch
+    rng = np.random.default_rng(406)
+    n = 40000
+    D = rng.integers(0, 2**64, n, dtype=np.uint64)
+    D[-1] |= np.uint64(1 << 63)
+    i = torch.empty(n, dtype=torch.int64, device="cuda")
+    ctx.recip(i, _dev(D))
+    Dv, Vv = O.to_int(D), O.to_int(_host(i))
+    rem = (1 << (128 * n)) - 1 - Dv * (Vv + (1 << (64 * n)))
+    assert 0 <= rem < Dv
