@@ -212,6 +212,15 @@ static int batch_launch(sbg_batch* b, KTimer* kt) {
 
 namespace sbg {
 
+// Descriptor uploads are pulled by a kernel from the ring's page-locked
+// host buffer (device-addressable), not copied by a DMA engine: a caller's
+// large host<->device copies queued on the copy engines would otherwise
+// delay every batch's small descriptor upload behind them.
+__global__ void k_ring_pull(uint4* __restrict__ dst, const uint4* __restrict__ src, size_t n16) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
 int UploadRing::push(const void* src, size_t bytes, cudaStream_t st, void** dev) {
     const size_t need = (bytes + 255) & ~(size_t)255;
     if (need > cap || head + need > cap) {
@@ -224,7 +233,12 @@ int UploadRing::push(const void* src, size_t bytes, cudaStream_t st, void** dev)
             // 32 MB: a 1024-division batch uploads about 4.5 MB of descriptors,
             // so the ring wraps (and drains the stream) once every few calls
             const size_t nc = std::max(need * 4, (size_t)32 << 20);
-            if (cudaHostAlloc(&h, nc, 0) != cudaSuccess) return SBG_EALLOC;
+            if (cudaHostAlloc(&h, nc, cudaHostAllocMapped) != cudaSuccess) return SBG_EALLOC;
+            if (cudaHostGetDevicePointer((void**)&hd, h, 0) != cudaSuccess) {
+                cudaFreeHost(h);
+                h = nullptr;
+                return SBG_EALLOC;
+            }
             if (cudaMalloc(&d, nc) != cudaSuccess) {
                 cudaFreeHost(h);
                 h = nullptr;
@@ -234,8 +248,13 @@ int UploadRing::push(const void* src, size_t bytes, cudaStream_t st, void** dev)
         }
     }
     std::memcpy(h + head, src, bytes);
-    if (bytes && cudaMemcpyAsync(d + head, h + head, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
-        return SBG_ECUDA;
+    if (bytes) {
+        const size_t n16 = need / 16;      // the whole 256-byte-rounded block
+        const unsigned blocks = (unsigned)std::min<size_t>((n16 + 255) / 256, 64);
+        k_ring_pull<<<blocks, 256, 0, st>>>((uint4*)(d + head), (const uint4*)(hd + head), n16);
+        if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
+        ++pulls;
+    }
     *dev = d + head;
     head += need;
     last = st;
@@ -246,6 +265,7 @@ void UploadRing::release() {
     if (h) cudaFreeHost(h);
     if (d) cudaFree(d);
     h = nullptr;
+    hd = nullptr;
     d = nullptr;
     cap = head = 0;
 }
@@ -658,7 +678,7 @@ int sbg_batch_run(sbg_batch* b) {
     return batch_launch(b, c->timer);
 }
 
-int64_t sbg_ctx_launches(sbg_ctx* c) { return c ? c->launches.load() : 0; }
+int64_t sbg_ctx_launches(sbg_ctx* c) { return c ? c->launches.load() + c->ring.pulls : 0; }
 
 // For every size class k where a 3 * 2^k transform could replace 2^(k+2),
 // time one full product (an = bn = 3 * 2^(k-1), the largest of the class)

@@ -43,6 +43,21 @@ static int host_slot_reserve(sbg_ctx* c, sbg_ctx::HostSlot& h, size_t limbs) {
     return SBG_OK;
 }
 
+// Copies in 8 MB pieces: with an upload and a download running at once, the
+// two copy engines interleave pieces of this size more evenly on PCIe than
+// whole 100 MB transfers (measured on B200, 268 MB each way: 5.54 ms in
+// 8 MB pieces against 5.83 ms whole; 4.84 ms for one direction alone).
+#define HOST_COPY_PIECE ((size_t)8 << 20)
+static cudaError_t copy_pieces(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind,
+                               cudaStream_t st) {
+    for (size_t o = 0; o < bytes; o += HOST_COPY_PIECE) {
+        const size_t len = bytes - o < HOST_COPY_PIECE ? bytes - o : HOST_COPY_PIECE;
+        cudaError_t e = cudaMemcpyAsync((char*)dst + o, (const char*)src + o, len, kind, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 static int host_product(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, const uint64_t* bp,
                         int64_t bn, int sq) {
     if (!c || !rp || !ap || an <= 0 || (!sq && (!bp || bn <= 0))) return SBG_EINVAL;
@@ -60,8 +75,8 @@ static int host_product(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an
     // the slot's operands are free once its previous product has run, its
     // result buffer once that result has been downloaded
     if (cudaStreamWaitEvent(c->s_in, h.comp_done, 0) != cudaSuccess ||
-        cudaMemcpyAsync(da, ap, (size_t)an * 8, cudaMemcpyHostToDevice, c->s_in) != cudaSuccess ||
-        (!sq && cudaMemcpyAsync(db, bp, (size_t)bn * 8, cudaMemcpyHostToDevice, c->s_in) != cudaSuccess) ||
+        copy_pieces(da, ap, (size_t)an * 8, cudaMemcpyHostToDevice, c->s_in) != cudaSuccess ||
+        (!sq && copy_pieces(db, bp, (size_t)bn * 8, cudaMemcpyHostToDevice, c->s_in) != cudaSuccess) ||
         cudaEventRecord(h.in_done, c->s_in) != cudaSuccess ||
         cudaStreamWaitEvent(c->stream, h.in_done, 0) != cudaSuccess ||
         cudaStreamWaitEvent(c->stream, h.out_done, 0) != cudaSuccess)
@@ -70,7 +85,7 @@ static int host_product(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an
     if (st) return st;
     if (cudaEventRecord(h.comp_done, c->stream) != cudaSuccess ||
         cudaStreamWaitEvent(c->s_out, h.comp_done, 0) != cudaSuccess ||
-        cudaMemcpyAsync(rp, dr, (size_t)nout * 8, cudaMemcpyDeviceToHost, c->s_out) != cudaSuccess ||
+        copy_pieces(rp, dr, (size_t)nout * 8, cudaMemcpyDeviceToHost, c->s_out) != cudaSuccess ||
         cudaEventRecord(h.out_done, c->s_out) != cudaSuccess)
         return SBG_ECUDA;
     return SBG_OK;

@@ -224,9 +224,11 @@ struct EventTimer : KTimer {
 // first synchronises the streams of earlier pushes, so no copy or kernel
 // still reading the reused bytes is in flight.  One host thread at a time.
 struct UploadRing {
-    uint8_t* h = nullptr;
+    uint8_t* h = nullptr;           // page-locked host buffer
+    uint8_t* hd = nullptr;          //   its device address
     uint8_t* d = nullptr;
     size_t cap = 0, head = 0;
+    int64_t pulls = 0;              // copy kernels launched (k_ring_pull)
     cudaStream_t last = nullptr;
     int push(const void* src, size_t bytes, cudaStream_t st, void** dev);
     void release();
