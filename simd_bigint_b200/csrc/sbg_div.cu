@@ -107,98 +107,167 @@ __device__ __forceinline__ uint32_t gp2(uint32_t left, uint32_t right) {
     return (gr | (pr & gl)) | ((pr & pl) << 1);
 }
 
-// z[0..len) = x +/- y (+ cin / - bin), x(i), y(i) limb accessors (0 beyond
-// their length); returns the carry / borrow out.  z may alias x or y limb
-// for limb (limb i is read and written by the same thread).
-//
-// A tile holds CL * DIV_TILE limbs, DIV_TILE per CTA.  A warp takes 32 *
-// DIV_PER consecutive limbs as DIV_PER rows of 32, lane l on limb row * 32
-// + l, so every load and store is coalesced.  Per row, with the lanes'
-// generate (G) and propagate (P) bits as ballot masks g, p, the carries into
-// the 32 limbs for row carry-in c are (p + (g << 1 | c)) ^ p, and the row
-// passes on (p + (g << 1 | c)) >> 32 | g >> 31.  The rows' (G, P) compose to
-// the warp's, a block scan of the warps' gives the CTA's, and the CTAs'
+// Carries of one tile: the rows' generate / propagate masks g[k], p[k]
+// (lane l = limb k * 32 + l of this warp's rows) and the group's carry into
+// the tile give cm[k], the carries into every limb as a lane mask; returns
+// the carry out of the tile (group-uniform).  Per row, with carry-in c, the
+// carries into the 32 limbs are (p + (g << 1 | c)) ^ p and the row passes on
+// (p + (g << 1 | c)) >> 32 | g >> 31.  The rows' (G, P) compose to the
+// warp's, a block scan of the warps' gives the CTA's, and the CTAs'
 // aggregates, composed in rank order, give each CTA its carry-in.
-template <int CL, class FX, class FY>
-__device__ uint32_t block_addsub(Grp<CL>& grp, uint64_t* z, int64_t len, FX x, FY y, bool sub,
-                                 uint32_t cin) {
+template <int CL, int R>
+__device__ uint32_t tile_carries(Grp<CL>& grp, const uint32_t (&g)[R], const uint32_t (&p)[R],
+                                 uint32_t carry, uint32_t (&cm)[R]) {
     __shared__ uint32_t s_w[DIV_T / 32];
     __shared__ uint32_t s_tot;
     constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t wG = 0, wP = 1;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const uint32_t rG = (uint32_t)(((uint64_t)p[k] + (g[k] << 1)) >> 32) | (g[k] >> 31);
+        const uint32_t rP = p[k] == FULL;
+        wG = rG | (rP & wG);
+        wP = rP & wP;
+    }
+    if (lane == 0) s_w[wid] = wG | (wP << 1);
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t iv = lane < DIV_T / 32 ? s_w[lane] : 2u;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(FULL, iv, d);
+            if (lane >= d) iv = gp2(o, iv);
+        }
+        if (lane < DIV_T / 32) s_w[lane] = iv;     // inclusive warp prefixes
+        if (lane == 31) s_tot = iv;
+    }
+    __syncthreads();
+    uint32_t cta_cin = carry, next;
+    if constexpr (CL == 1) {
+        const uint32_t tot = s_tot;
+        next = (tot & 1u) | ((tot >> 1) & carry);
+    } else {
+        const long long* sl = grp.publish(s_tot);
+        uint32_t pre = 2u, all = 2u;
+        for (int k = 0; k < CL; ++k) {
+            const uint32_t v = (uint32_t)grp.peer(sl, k);
+            if (k < (int)grp.rank) pre = gp2(pre, v);
+            all = gp2(all, v);
+        }
+        cta_cin = (pre & 1u) | ((pre >> 1) & carry);
+        next = (all & 1u) | ((all >> 1) & carry);
+    }
+    const uint32_t wpre = wid > 0 ? s_w[wid - 1] : 2u;
+    uint32_t c = (wpre & 1u) | ((wpre >> 1) & cta_cin);
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const uint64_t sum = (uint64_t)p[k] + ((g[k] << 1) | c);
+        cm[k] = (uint32_t)sum ^ p[k];
+        c = (uint32_t)(sum >> 32) | (g[k] >> 31);
+    }
+    __syncthreads();                 // s_w, s_tot reused by the next tile
+    return next;
+}
+
+// One row of an add (sub = false) or subtract chain: d = a +/- b, its
+// generate / propagate masks over the warp; limbs past the length (!in)
+// propagate, so a chain's carry out is that of its last limb.
+__device__ __forceinline__ void chain_row(uint64_t a, uint64_t b, bool in, bool sub, uint64_t& d,
+                                          uint32_t& g, uint32_t& p) {
+    constexpr unsigned FULL = 0xffffffffu;
+    bool G, P;
+    if (sub) {
+        d = a - b;
+        G = a < b;                     // borrow generated
+        P = !in || d == 0;             // borrow propagates
+    } else {
+        d = a + b;
+        G = d < a;
+        P = !in || d == ~0ull;
+    }
+    g = __ballot_sync(FULL, G);
+    p = __ballot_sync(FULL, P);
+}
+
+// z[0..len) = x +/- y (+ cin / - bin), x(i), y(i) limb accessors (0 beyond
+// their length); returns the carry / borrow out.  z may alias x or y limb
+// for limb (limb i is read and written by the same thread).  A tile holds
+// CL * DIV_TILE limbs, DIV_TILE per CTA; a warp takes 32 * DIV_PER
+// consecutive limbs as DIV_PER rows of 32, lane l on limb row * 32 + l, so
+// every load and store is coalesced.
+template <int CL, class FX, class FY>
+__device__ uint32_t block_addsub(Grp<CL>& grp, uint64_t* z, int64_t len, FX x, FY y, bool sub,
+                                 uint32_t cin) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint32_t carry = cin;
     for (int64_t base = 0; base < len; base += (int64_t)CL * DIV_TILE) {
         const int64_t w0 = base + (int64_t)grp.rank * DIV_TILE + (int64_t)wid * (32 * DIV_PER) + lane;
         uint64_t s[DIV_PER];
-        uint32_t g[DIV_PER], p[DIV_PER];
-        uint32_t wG = 0, wP = 1;
+        uint32_t g[DIV_PER], p[DIV_PER], cm[DIV_PER];
 #pragma unroll
         for (int k = 0; k < DIV_PER; ++k) {
             const int64_t i = w0 + 32 * k;
             const bool in = i < len;
-            const uint64_t a = in ? x(i) : 0, b = in ? y(i) : 0;
-            uint64_t d;
-            bool G, P;
-            // limbs past len propagate, so the carry out is that of limb len-1
-            if (sub) {
-                d = a - b;
-                G = a < b;                     // borrow generated
-                P = !in || d == 0;             // borrow propagates
-            } else {
-                d = a + b;
-                G = d < a;
-                P = !in || d == ~0ull;
-            }
-            s[k] = d;
-            g[k] = __ballot_sync(FULL, G);
-            p[k] = __ballot_sync(FULL, P);
-            const uint32_t rG = (uint32_t)(((uint64_t)p[k] + (g[k] << 1)) >> 32) | (g[k] >> 31);
-            const uint32_t rP = p[k] == FULL;
-            wG = rG | (rP & wG);
-            wP = rP & wP;
+            chain_row(in ? x(i) : 0, in ? y(i) : 0, in, sub, s[k], g[k], p[k]);
         }
-        if (lane == 0) s_w[wid] = wG | (wP << 1);
-        __syncthreads();
-        if (wid == 0) {
-            uint32_t iv = lane < DIV_T / 32 ? s_w[lane] : 2u;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint32_t o = __shfl_up_sync(FULL, iv, d);
-                if (lane >= d) iv = gp2(o, iv);
-            }
-            if (lane < DIV_T / 32) s_w[lane] = iv;     // inclusive warp prefixes
-            if (lane == 31) s_tot = iv;
-        }
-        __syncthreads();
-        uint32_t cta_cin = carry, next;
-        if constexpr (CL == 1) {
-            const uint32_t tot = s_tot;
-            next = (tot & 1u) | ((tot >> 1) & carry);
-        } else {
-            const long long* sl = grp.publish(s_tot);
-            uint32_t pre = 2u, all = 2u;
-            for (int k = 0; k < CL; ++k) {
-                const uint32_t v = (uint32_t)grp.peer(sl, k);
-                if (k < (int)grp.rank) pre = gp2(pre, v);
-                all = gp2(all, v);
-            }
-            cta_cin = (pre & 1u) | ((pre >> 1) & carry);
-            next = (all & 1u) | ((all >> 1) & carry);
-        }
-        const uint32_t wpre = wid > 0 ? s_w[wid - 1] : 2u;
-        uint32_t c = (wpre & 1u) | ((wpre >> 1) & cta_cin);
+        carry = tile_carries(grp, g, p, carry, cm);
 #pragma unroll
         for (int k = 0; k < DIV_PER; ++k) {
             const int64_t i = w0 + 32 * k;
-            const uint64_t sum = (uint64_t)p[k] + ((g[k] << 1) | c);
-            const uint64_t cl = ((uint32_t)sum ^ p[k]) >> lane & 1u;
+            const uint64_t cl = (cm[k] >> lane) & 1u;
             if (i < len) z[i] = sub ? s[k] - cl : s[k] + cl;
-            c = (uint32_t)(sum >> 32) | (g[k] >> 31);
         }
-        carry = next;
-        __syncthreads();                 // s_w, s_tot reused by the next tile
     }
     return carry;
+}
+
+// The three chains of the division's end-around remainder in one pass:
+// F = C_lo + C_hi (C_hi = P[L .. L+3) at limbs 0..2), G = N_lo - F,
+// H = G + N_hi (N_hi = N[L .. n2)), H into P[0 .. L).  Returns the carry
+// outs c, b, c2 in bits 0, 1, 2: the value N - C = H + (c2 - b - c) B^L.
+// Each row's limbs go through the chains in order, every chain's carries
+// resolved per tile before the next chain reads its digits.
+#define FOLD_PER 4
+template <int CL>
+__device__ uint32_t block_fold3(Grp<CL>& grp, uint64_t* P, int64_t L, const uint64_t* N, int64_t n2) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    constexpr int64_t TILE = (int64_t)DIV_T * FOLD_PER;
+    uint32_t ca = 0, cb = 0, cc = 0;
+    for (int64_t base = 0; base < L; base += (int64_t)CL * TILE) {
+        const int64_t w0 = base + (int64_t)grp.rank * TILE + (int64_t)wid * (32 * FOLD_PER) + lane;
+        uint64_t v[FOLD_PER], nl[FOLD_PER], nh[FOLD_PER];
+        uint32_t g[FOLD_PER], p[FOLD_PER], cm[FOLD_PER];
+#pragma unroll
+        for (int k = 0; k < FOLD_PER; ++k) {
+            const int64_t i = w0 + 32 * k;
+            const bool in = i < L;
+            nl[k] = in ? N[i] : 0;
+            nh[k] = (in && L + i < n2) ? N[L + i] : 0;
+            chain_row(in ? P[i] : 0, (in && i < 3) ? P[L + i] : 0, in, false, v[k], g[k], p[k]);
+        }
+        ca = tile_carries(grp, g, p, ca, cm);
+#pragma unroll
+        for (int k = 0; k < FOLD_PER; ++k) {
+            const int64_t i = w0 + 32 * k;
+            const bool in = i < L;          // limbs past L hold 0 in every chain
+            chain_row(nl[k], in ? v[k] + ((cm[k] >> lane) & 1u) : 0, in, true, v[k], g[k], p[k]);
+        }
+        cb = tile_carries(grp, g, p, cb, cm);
+#pragma unroll
+        for (int k = 0; k < FOLD_PER; ++k) {
+            const int64_t i = w0 + 32 * k;
+            const bool in = i < L;
+            chain_row(in ? v[k] - ((cm[k] >> lane) & 1u) : 0, nh[k], in, false, v[k], g[k], p[k]);
+        }
+        cc = tile_carries(grp, g, p, cc, cm);
+#pragma unroll
+        for (int k = 0; k < FOLD_PER; ++k) {
+            const int64_t i = w0 + 32 * k;
+            if (i < L) P[i] = v[k] + ((cm[k] >> lane) & 1u);
+        }
+    }
+    return ca | (cb << 1) | (cc << 2);
 }
 
 // sign of x - y over len limbs: -1, 0, 1 (group-uniform).  Walks down from
@@ -467,28 +536,24 @@ __global__ void __launch_bounds__(DIV_T) k_div_fix(const DivFix* df, uint32_t* e
                      true, 0);
     } else {
         const int64_t L = F.L;
-        // C = P[0..L) + P[L..L+3), end-around
-        uint32_t c = block_addsub(grp, P, L, [&](int64_t i) { return P[i]; },
-                                  [&](int64_t i) { return i < 3 ? P[L + i] : 0ull; }, false, 0);
+        // H = (N_lo - (C_lo + C_hi)) + N_hi in one pass; N - C = H + d B^L
+        // with d = c2 - b - c, and B^L = 1 modulo B^L - 1
+        const uint32_t cs = block_fold3(grp, P, L, N, 2 * n);
+        const int d = (int)((cs >> 2) & 1u) - (int)((cs >> 1) & 1u) - (int)(cs & 1u);
         grp.sync();
-        if (c && block_step1(grp, P, L, true)) {
-            if (grp.rank == 0 && threadIdx.x == 0) P[0] = 1;
-        }
-        grp.sync();
-        // N_lo - C (a borrow out adds B^L = 1 + (B^L - 1): take 1 back) ...
-        const uint32_t b1 = block_addsub(grp, P, L, [&](int64_t i) { return N[i]; },
-                                         [&](int64_t i) { return P[i]; }, true, 0);
-        grp.sync();
-        // ... + N_hi (limbs L .. 2n-1; a carry out is B^L = 1 + (B^L - 1): give 1)
-        const uint32_t c2 = block_addsub(grp, P, L, [&](int64_t i) { return P[i]; },
-                                         [&](int64_t i) { return L + i < 2 * n ? N[L + i] : 0ull; }, false, 0);
-        grp.sync();
-        if (c2 && !b1) {
+        if (d > 0) {
+            // H + 1; wrapping past B^L - 1 leaves B^L = 1
             if (block_step1(grp, P, L, true) && grp.rank == 0 && threadIdx.x == 0) P[0] = 1;
-        } else if (b1 && !c2) {
-            block_step1(grp, P, L, false);
+            grp.sync();
         }
-        grp.sync();
+        for (int k = 0; k < -d; ++k) {
+            // H - 1; wrapping below 0 leaves B^L - 1, which is one more than -1
+            if (block_step1(grp, P, L, false)) {
+                grp.sync();
+                block_step1(grp, P, L, false);
+            }
+            grp.sync();
+        }
         // the value is R, or R + (B^L - 1) when R = 0 and the sum came out all ones
         __shared__ int s_hi, s_ones;
         if (threadIdx.x == 0) {
