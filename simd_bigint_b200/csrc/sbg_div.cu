@@ -454,7 +454,43 @@ __global__ void __launch_bounds__(DIV_T) k_recip_step1(const RecipStep* st, uint
     Grp<CL> grp(s_slot);
     const RecipStep S = st[blockIdx.x / CL];
     const int64_t n = S.n, h = S.h, l = n - h, tl = n + h + 1;
-    // T - B^(n+h) < A_lo * X_h < 2 B^n <= 4 A: at most four corrections
+    grp.sync();
+    if (S.T[n + h] != 0) {
+        // T >= B^(n+h): E = T - B^(n+h) < 2 B^n <= 4 A sits in T's low n+1
+        // limbs.  With k the number of corrections (the least k with
+        // k A > E), B^(n+h) - (T - k A) = W = k A - E in (0, A], so T_m is
+        // limbs l..n of W: W = A - E, then + A while W <= 0 -- n-limb passes
+        // instead of k passes over T's n+h+1 limbs.
+        const uint64_t* A = S.A;
+        uint64_t* T = S.T;
+        uint32_t neg = block_addsub(grp, T, n + 1, [&](int64_t i) { return i < n ? A[i] : 0ull; },
+                                    [&](int64_t i) { return T[i]; }, true, 0);
+        int k = 1;
+        for (;;) {
+            grp.sync();
+            // W > 0: no borrow left and some limb nonzero
+            if (!neg && block_cmp(grp, n + 1, [&](int64_t i) { return T[i]; },
+                                  [&](int64_t i) { return 0ull; }) > 0)
+                break;
+            if (k == 4) {
+                if (threadIdx.x == 0) atomicOr(err, 16u);
+                break;
+            }
+            const uint32_t c = block_addsub(grp, T, n + 1, [&](int64_t i) { return T[i]; },
+                                            [&](int64_t i) { return i < n ? A[i] : 0ull; }, false, 0);
+            neg = neg & (c ^ 1u);       // a carry out of the n+1 limbs ends the wrap
+            ++k;
+        }
+        for (int j = 0; j < k; ++j) {
+            block_step1(grp, S.Xh, h + 1, false);
+            grp.sync();
+        }
+        uint64_t* TM = S.TM;
+        GRP_LOOP(i, h + 1) TM[i] = T[l + i];
+        if constexpr (CL > 1) grp.sync();
+        return;
+    }
+    // T < B^(n+h) (the loop below keeps its correction path as a guard)
     for (int it = 0; it < 6; ++it) {
         grp.sync();
         if (S.T[n + h] == 0) break;
