@@ -425,9 +425,9 @@ __global__ void __launch_bounds__(DIV_T) k_recip_wrap(const RecipStep* st, uint3
         if (grp.rank == 0 && threadIdx.x == 0) C[0] = 1;
     }
     grp.sync();
-    // E' = C - B^sft  (a borrow out means C < B^sft: E' = C - B^sft + B^L - 1)
-    const uint32_t b = block_addsub(grp, C, L, [&](int64_t i) { return C[i]; },
-                                    [&](int64_t i) { return i == sft ? 1ull : 0ull; }, true, 0);
+    // E' = C - B^sft: a borrow rippling up from limb sft, over the zero limbs
+    // only (a borrow out of the top means C < B^sft: E' = C - B^sft + B^L - 1)
+    const bool b = block_step1(grp, C + sft, L - sft, false);
     grp.sync();
     if (b) block_step1(grp, C, L, false);
     grp.sync();
@@ -439,8 +439,11 @@ __global__ void __launch_bounds__(DIV_T) k_recip_wrap(const RecipStep* st, uint3
     if (!neg) {
         GRP_LOOP(i, tl) T[i] = i < L ? C[i] : (i == n + h ? 1ull : 0ull);
     } else {
-        // T = B^(n+h) - |E| = (E' + 1) on the low L limbs, ~0 up to n+h-1, 0 on top
-        block_addsub(grp, T, L, [&](int64_t i) { return C[i]; }, [&](int64_t i) { return 0ull; }, false, 1);
+        // T = B^(n+h) - |E| = (E' + 1) on the low L limbs, ~0 up to n+h-1, 0 on
+        // top: a copy, then the +1 ripple (E' < B^L - 1, so it stops inside)
+        GRP_LOOP(i, L) T[i] = C[i];
+        grp.sync();
+        block_step1(grp, T, L, true);
         for (int64_t i = L + (int64_t)grp.rank * DIV_T + threadIdx.x; i < tl; i += (int64_t)CL * DIV_T)
             T[i] = i == n + h ? 0ull : ~0ull;
     }
