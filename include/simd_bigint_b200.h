@@ -246,8 +246,8 @@ int sbg_nt_sqr(uint64_t *rp, const uint64_t *ap, ptrdiff_t an);
  *                 const uint64_t *dp, uint64_t dn64, uint64_t *qn64_out,
  *                 uint64_t *rn64_out)        -- reference include/divrem.h:218,
  *                                               include/dc_div.h:154 (divrem_u64_dc)
- * Same arguments: qp gets nn-dn+1 limbs, rp gets dn limbs, *qn/*rn the
- * trimmed lengths (>= 1).  Any divisor with a nonzero top limb, any
+ * Same arguments: qp gets nn-dn+1 limbs, rp gets dn limbs, *qn64_out and
+ * *rn64_out the trimmed lengths (>= 1). Any divisor with a nonzero top limb, any
  * nn >= dn (normalised and split into 2dn/dn Newton steps).  Returns 1 on
  * success, 0 on failure (the reference's version returns void). */
 int sbg_divrem_u64(uint64_t *qp, uint64_t *rp, const uint64_t *np, uint64_t nn64,
