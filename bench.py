@@ -663,10 +663,13 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
     torch.cuda.synchronize()
     l0 = ctx.launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # batches queued back to back (sbg_divrem_batch_async): the host prepares
+    # the next batch while the device runs this one; one wait at the end
     e0.record(stream)
     for _ in range(steps):
-        ctx.divrem_batch(jobs)
+        ctx.divrem_batch_async(jobs)
     e1.record(stream)
+    ctx.divrem_wait()
     torch.cuda.synchronize()
     launches = ctx.launches() - l0
     dt = barrier_max(pg, e0.elapsed_time(e1) * 1e-3, dev) / steps
@@ -697,7 +700,7 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
         sets.append((d_in, d_out, ej))
     s_in = torch.cuda.Stream(device=dev)
     s_out = torch.cuda.Stream(device=dev)
-    ev = [{k: torch.cuda.Event() for k in ("in", "out")} for _ in range(2)]
+    ev = [{k: torch.cuda.Event() for k in ("in", "comp", "out")} for _ in range(2)]
     for e in ev:
         for x in e.values():
             x.record(stream)
@@ -708,6 +711,7 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
 
     def upload(i):
         d_in = sets[i & 1][0]
+        s_in.wait_event(ev[i & 1]["comp"])     # the division that last read this set
         with torch.cuda.stream(s_in):
             for o in range(0, ni, piece):
                 d_in[o:o + piece].copy_(h_in[o:o + piece], non_blocking=True)
@@ -717,13 +721,12 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
         d_in, d_out, ej = sets[i & 1]
         e = ev[i & 1]
         if i + 1 < last:
-            upload(i + 1)                       # that set's previous call has returned
+            upload(i + 1)
         stream.wait_event(e["in"])
         stream.wait_event(e["out"])             # its previous download is done
-        ctx.divrem_batch(ej)
-        done = torch.cuda.Event()
-        done.record(stream)
-        s_out.wait_event(done)
+        ctx.divrem_batch_async(ej)
+        e["comp"].record(stream)
+        s_out.wait_event(e["comp"])
         with torch.cuda.stream(s_out):
             for o in range(0, no, piece):
                 h_out[o:o + piece].copy_(d_out[o:o + piece], non_blocking=True)
@@ -732,11 +735,13 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
     upload(0)
     for i in range(2):
         e2e_step(i, 2)
+    ctx.divrem_wait()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     upload(0)
     for i in range(steps):
         e2e_step(i, steps)
+    ctx.divrem_wait()
     torch.cuda.synchronize()
     e2e_s = barrier_max(pg, time.perf_counter() - t0, dev) / steps
     ov = h_out.numpy().view(np.uint64)
@@ -762,8 +767,8 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
         "bit_exact": bool(exact),
         "e2e": {"value": round(total * ws / e2e_s / 1e6, 2), "unit": "Mlimb/s",
                 "h2d_bytes_per_step": int(ni * 8), "d2h_bytes_per_step": int(no * 8),
-                "entry": "sbg_divrem_batch between pinned host copies of all N, D in and Q, R out; two "
-                         "buffer sets alternate so the copies overlap the neighbouring steps' divisions"},
+                "entry": "sbg_divrem_batch_async between pinned host copies of all N, D in and Q, R out; "
+                         "two buffer sets alternate so the copies overlap the neighbouring steps' divisions"},
         "gpu_launches": int(launches), "roofline": None, "clocks": clk,
     }
     ctx.close()

@@ -174,6 +174,15 @@ typedef struct {
     int64_t nn, dn;        /* dn <= nn <= 2 dn */
 } sbg_div_job;
 int sbg_divrem_batch(sbg_ctx *ctx, const sbg_div_job *jobs, int64_t count);
+/* sbg_divrem_batch_async: the same batch queued on the context's stream
+ * without waiting (argument errors are returned at once); the host can
+ * prepare the next batch while the device runs this one.  Consecutive
+ * batches on one context run in order.  Device errors of every queued batch
+ * accumulate until sbg_divrem_wait, which waits for the stream and returns
+ * (and clears) them; a synchronous sbg_divrem_batch clears them too, so wait
+ * before mixing the two.  Operands and results must stay valid until then. */
+int sbg_divrem_batch_async(sbg_ctx *ctx, const sbg_div_job *jobs, int64_t count);
+int sbg_divrem_wait(sbg_ctx *ctx);
 
 /* ---- serving loop -------------------------------------------------------------
  * Continuous batching of independent requests with admission by HBM

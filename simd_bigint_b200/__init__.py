@@ -106,6 +106,10 @@ def lib(build_if_missing: bool = False):
         L.sbg_divrem.restype = C.c_int
         L.sbg_divrem_batch.argtypes = [_vp, _vp, _i64]
         L.sbg_divrem_batch.restype = C.c_int
+        L.sbg_divrem_batch_async.argtypes = [_vp, _vp, _i64]
+        L.sbg_divrem_batch_async.restype = C.c_int
+        L.sbg_divrem_wait.argtypes = [_vp]
+        L.sbg_divrem_wait.restype = C.c_int
         L.sbg_divrem_u64.argtypes = [_vp, _vp, _vp, C.c_uint64, _vp, C.c_uint64,
                                      C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         L.sbg_divrem_u64.restype = C.c_int
@@ -264,12 +268,27 @@ class Context:
         _check(self._L.sbg_divrem(self.handle, _dptr(q), _dptr(r), _dptr(n_), nn, _dptr(d), dn),
                "sbg_divrem")
 
-    def divrem_batch(self, jobs: list[tuple]):
-        """jobs: (q_ptr, r_ptr, n_ptr, d_ptr, nn, dn) raw device addresses."""
+    @staticmethod
+    def _div_jobs(jobs: list[tuple]):
         arr = (DivJob * max(1, len(jobs)))()
         for i, (q, r, n_, d, nn, dn) in enumerate(jobs):
             arr[i].qp, arr[i].rp, arr[i].np, arr[i].dp, arr[i].nn, arr[i].dn = q, r, n_, d, nn, dn
+        return arr
+
+    def divrem_batch(self, jobs: list[tuple]):
+        """jobs: (q_ptr, r_ptr, n_ptr, d_ptr, nn, dn) raw device addresses."""
+        arr = self._div_jobs(jobs)
         _check(self._L.sbg_divrem_batch(self.handle, C.cast(arr, _vp), len(jobs)), "sbg_divrem_batch")
+
+    def divrem_batch_async(self, jobs: list[tuple]):
+        """sbg_divrem_batch_async: queue the batch and return; results are
+        ready, and device errors reported, after divrem_wait()."""
+        arr = self._div_jobs(jobs)
+        _check(self._L.sbg_divrem_batch_async(self.handle, C.cast(arr, _vp), len(jobs)),
+               "sbg_divrem_batch_async")
+
+    def divrem_wait(self):
+        _check(self._L.sbg_divrem_wait(self.handle), "sbg_divrem_wait")
 
     def mulmid(self, r, a, b, an: int | None = None, bn: int | None = None):
         an = a.numel() if an is None else an

@@ -887,7 +887,7 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
 }
 
 // grow-only division scratch of the context (and its error word, cleared)
-static int div_scratch(sbg_ctx* c, size_t limbs, uint64_t** scratch) {
+static int div_scratch(sbg_ctx* c, size_t limbs, uint64_t** scratch, bool clear_err = true) {
     if (limbs > c->dscr_cap) {
         if (cudaStreamSynchronize(c->stream) != cudaSuccess) return SBG_ECUDA;
         cudaFree(c->dscr);
@@ -897,8 +897,11 @@ static int div_scratch(sbg_ctx* c, size_t limbs, uint64_t** scratch) {
         if (cudaMalloc(&c->dscr, nl * 8) != cudaSuccess) return SBG_EALLOC;
         c->dscr_cap = nl;
     }
-    if (!c->derr && cudaMalloc(&c->derr, 4) != cudaSuccess) return SBG_EALLOC;
-    if (cudaMemsetAsync(c->derr, 0, 4, c->stream) != cudaSuccess) return SBG_ECUDA;
+    if (!c->derr) {
+        if (cudaMalloc(&c->derr, 4) != cudaSuccess) return SBG_EALLOC;
+        clear_err = true;               // a fresh word starts at zero
+    }
+    if (clear_err && cudaMemsetAsync(c->derr, 0, 4, c->stream) != cudaSuccess) return SBG_ECUDA;
     *scratch = c->dscr;
     return SBG_OK;
 }
@@ -958,8 +961,12 @@ extern "C" int sbg_recip(sbg_ctx* c, uint64_t* ip, const uint64_t* dp, int64_t n
 
 // Batched division: every job has a normalised divisor (top bit set) and
 // nn <= 2 dn (the configurations of the reference's Newton division); other
-// shapes go through sbg_divrem, which normalises and splits them.
-extern "C" int sbg_divrem_batch(sbg_ctx* c, const sbg_div_job* jobs, int64_t count) {
+// shapes go through sbg_divrem, which normalises and splits them.  Queues the
+// whole batch on the context's stream; keep_err leaves the error word of
+// earlier queued batches in place (the asynchronous entry).
+static int divrem_enqueue(sbg_ctx* c, const sbg_div_job* jobs, int64_t count, bool keep_err,
+                          bool* queued) {
+    *queued = false;
     if (!c || (count > 0 && !jobs) || count < 0) return SBG_EINVAL;
     size_t total = 0;
     for (int64_t i = 0; i < count; ++i) {
@@ -971,8 +978,9 @@ extern "C" int sbg_divrem_batch(sbg_ctx* c, const sbg_div_job* jobs, int64_t cou
     }
     if (cudaSetDevice(c->device) != cudaSuccess) return SBG_ECUDA;
     uint64_t* scratch = nullptr;
-    int rc = div_scratch(c, total, &scratch);
+    int rc = div_scratch(c, total, &scratch, !keep_err);
     if (rc) return rc;
+    *queued = true;
     std::vector<DivInst> v((size_t)count);
     std::vector<CopyDesc> cn((size_t)count);
     uint64_t* p = scratch;
@@ -993,11 +1001,37 @@ extern "C" int sbg_divrem_batch(sbg_ctx* c, const sbg_div_job* jobs, int64_t cou
     }
     rc = copy_batch(c, cn);
     if (!rc) rc = div_core(c, v, c->derr, true);
+    return rc;
+}
+
+extern "C" int sbg_divrem_batch(sbg_ctx* c, const sbg_div_job* jobs, int64_t count) {
+    bool queued = false;
+    int rc = divrem_enqueue(c, jobs, count, false, &queued);
+    if (!queued) return rc;             // argument errors: nothing was queued
     rc = div_finish(c, rc);
     if (getenv("SBG_DEBUG") && rc)
         fprintf(stderr, "sbg_divrem_batch: status %d (count %lld, first dn %lld nn %lld)\n", rc,
                 (long long)count, count ? (long long)jobs[0].dn : 0LL,
                 count ? (long long)jobs[0].nn : 0LL);
+    return rc;
+}
+
+// The same batch queued without waiting: consecutive batches on one context
+// follow each other on its stream (scratch, descriptor ring and padded
+// numerators are reused in stream order), so the host prepares the next
+// batch while the device runs this one.  Device errors accumulate until
+// sbg_divrem_wait.
+extern "C" int sbg_divrem_batch_async(sbg_ctx* c, const sbg_div_job* jobs, int64_t count) {
+    bool queued = false;
+    return divrem_enqueue(c, jobs, count, true, &queued);
+}
+
+extern "C" int sbg_divrem_wait(sbg_ctx* c) {
+    if (!c) return SBG_EINVAL;
+    if (cudaSetDevice(c->device) != cudaSuccess) return SBG_ECUDA;
+    if (!c->derr) return cudaStreamSynchronize(c->stream) == cudaSuccess ? SBG_OK : SBG_ECUDA;
+    const int rc = div_finish(c, SBG_OK);
+    if (cudaMemsetAsync(c->derr, 0, 4, c->stream) != cudaSuccess) return rc ? rc : SBG_ECUDA;
     return rc;
 }
 

@@ -170,3 +170,38 @@ def test_cluster_sized_recip_exact(ctx):
     Dv, Vv = O.to_int(D), O.to_int(_host(i))
     rem = (1 << (128 * n)) - 1 - Dv * (Vv + (1 << (64 * n)))
     assert 0 <= rem < Dv
+
+
+def test_async_batches_back_to_back_match_sync(ctx):
+    """sbg_divrem_batch_async: three batches queued without waiting (the
+    scratch, descriptor ring and padded numerators reused in stream order),
+    one sbg_divrem_wait, then every quotient and remainder equals the
+    synchronous sbg_divrem_batch on the same inputs."""
+    import torch
+    rng = np.random.default_rng(407)
+    batches = [[700, 1500, 3000], [40000, 513], [9000, 2048, 33000, 600]]
+    keep = []
+    for ns in batches:
+        jobs, held = [], []
+        for n in ns:
+            N = rng.integers(0, 2**64, 2 * n, dtype=np.uint64)
+            D = rng.integers(0, 2**64, n, dtype=np.uint64)
+            D[-1] |= np.uint64(1 << 63)
+            tN, tD = _dev(N), _dev(D)
+            q = torch.full((n + 1,), -1, dtype=torch.int64, device="cuda")
+            r = torch.full((n,), -1, dtype=torch.int64, device="cuda")
+            jobs.append((q.data_ptr(), r.data_ptr(), tN.data_ptr(), tD.data_ptr(), 2 * n, n))
+            held.append((tN, tD, q, r, n))
+        ctx.divrem_batch_async(jobs)
+        keep.append(held)
+    ctx.divrem_wait()
+    for held in keep:
+        sync_jobs, outs = [], []
+        for tN, tD, q, r, n in held:
+            q2 = torch.empty(n + 1, dtype=torch.int64, device="cuda")
+            r2 = torch.empty(n, dtype=torch.int64, device="cuda")
+            sync_jobs.append((q2.data_ptr(), r2.data_ptr(), tN.data_ptr(), tD.data_ptr(), 2 * n, n))
+            outs.append((q, r, q2, r2))
+        ctx.divrem_batch(sync_jobs)
+        for q, r, q2, r2 in outs:
+            assert torch.equal(q, q2) and torch.equal(r, r2)
