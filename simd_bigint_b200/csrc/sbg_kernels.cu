@@ -1308,7 +1308,9 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
     uint64_t zv = 0;                    // the spill limb nout, before carries,
     uint32_t vbad = 0;                  //   what it must not carry out,
     int vpos = -1;                      //   and where it sits (4 s + k)
-#pragma unroll
+    // a runtime loop: each step holds four Garner reconstructions, and
+    // unrolling the steps quadruples the code the warps fetch
+#pragma unroll 1
     for (int s = 0; s < CRT_NSTEP; ++s) {
         const int64_t m0 = seg + 128 * s + 4 * lane;
         uint32_t r[CRT_V][SBG_NP];
