@@ -221,6 +221,120 @@ def product_ok(a: np.ndarray, b: np.ndarray, r: np.ndarray) -> bool:
     return (a1 * b1) % M61 == r1 and (a2 * b2) % M64 == r2 and low
 
 
+def _is_prime(n: int) -> bool:
+    """Miller-Rabin with the first twelve prime bases (deterministic below 3.3e24)."""
+    if n < 2:
+        return False
+    small = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37)
+    for p in small:
+        if n % p == 0:
+            return n == p
+    d, s = n - 1, 0
+    while d % 2 == 0:
+        d //= 2
+        s += 1
+    for a in small:
+        x = pow(a, d, n)
+        if x in (1, n - 1):
+            continue
+        for _ in range(s - 1):
+            x = x * x % n
+            if x == n - 1:
+                break
+        else:
+            return False
+    return True
+
+
+# the transform primes: an error that is a multiple of their product would be
+# invisible modulo any of them, so the spot check never draws them
+NTT_PRIMES = (1107296257, 1711276033, 1811939329, 2013265921, 2113929217)
+
+
+def random_primes(seed: int, k: int = 4, bits: int = 31) -> list[int]:
+    """k distinct random primes of `bits` bits drawn from `seed` (logged with
+    the result, so a failing check can be replayed)."""
+    import random
+    rnd = random.Random(seed)
+    out: list[int] = []
+    while len(out) < k:
+        c = rnd.getrandbits(bits) | (1 << (bits - 1)) | 1
+        if c not in out and c not in NTT_PRIMES and _is_prime(c):
+            out.append(c)
+    return out
+
+
+def limbs_mod(a: np.ndarray, q: int, block: int = 4096) -> int:
+    """A mod q for a little-endian u64 limb array and a prime q < 2^31, in
+    numpy: limb i weighs 2^(64 i) mod q, split as w_small[i mod block] *
+    w_big[i / block]; every product stays below 2^62."""
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    n = a.size
+    if n == 0:
+        return 0
+    Q = np.uint64(q)
+    x = ((a >> np.uint64(32)) % Q * np.uint64(pow(2, 32, q)) + (a & np.uint64(0xFFFFFFFF)) % Q) % Q
+    rows = -(-n // block)
+    b = pow(2, 64, q)
+    w_small = np.empty(block, dtype=np.uint64)
+    v = 1
+    for i in range(block):
+        w_small[i] = v
+        v = v * b % q
+    big = pow(2, 64 * block, q)
+    w_big = np.empty(rows, dtype=np.uint64)
+    v = 1
+    for j in range(rows):
+        w_big[j] = v
+        v = v * big % q
+    xp = np.zeros(rows * block, dtype=np.uint64)
+    xp[:n] = x
+    t = (xp.reshape(rows, block) * w_small[None, :]) % Q
+    srow = t.sum(axis=1, dtype=np.uint64) % Q
+    return int(((srow * w_big) % Q).sum(dtype=np.uint64)) % q
+
+
+def spot_check_primes(a: np.ndarray, b: np.ndarray, r: np.ndarray, primes: list[int]) -> bool:
+    """(A mod q)(B mod q) == R mod q for every q in `primes`."""
+    return all(limbs_mod(a, q) * limbs_mod(b, q) % q == limbs_mod(r, q) for q in primes)
+
+
+GOLDEN_FILE = ROOT / "tests" / "golden" / "golden.json"
+
+
+def golden_sha256(op: str, an: int, bn: int, seed: int = 42) -> str | None:
+    """The reference's own product digest for these operands (xorshift64
+    stream from `seed`), from the committed golden vectors made by the
+    unmodified reference; None where none was generated."""
+    try:
+        g = json.loads(GOLDEN_FILE.read_text())
+    except (OSError, ValueError):
+        return None
+    for e in g.get("mul", []):
+        if (e["op"], e["an"], e["bn"], e["pattern"], e["seed"]) == (op, an, bn, "xs", seed):
+            return e["sha256"]
+    return None
+
+
+def sha256_limbs(x: np.ndarray) -> str:
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(x, dtype="<u8").tobytes()).hexdigest()
+
+
+XS_SEED = 42          # the single-product workloads' operands: xorshift64 from 42
+
+
+def xs_inputs(op: str, an: int, bn: int, seed: int = XS_SEED):
+    """Operands of the single-product workloads: the xorshift64 stream of the
+    reference's test batteries (a first, b continues the stream; sqr uses a),
+    the inputs the golden digests were made from.  Every output of the
+    generator is nonzero, so the top limbs are."""
+    from simd_bigint_b200.workloads import xorshift64_limbs
+    a, st = xorshift64_limbs(an, seed)
+    b = a if op == "sqr" else xorshift64_limbs(bn, st)[0]
+    return a, b
+
+
 def make_inputs(an: int, bn: int, seed: int):
     rng = np.random.default_rng(seed)
     a = rng.integers(0, 2**64, size=an, dtype=np.uint64)
@@ -250,11 +364,13 @@ def cpu_threads_for(an: int, bn: int, want: int | None = None, cap: int = 64) ->
 
 def _cpu_worker(op, an, bn, seed, steps, warmup, barrier, queue):
     """One baseline process: its own inputs, its own reference plan (built in
-    the warm-up), then `steps` timed products between barriers."""
+    the warm-up), then `steps` timed products between barriers.  seed None:
+    the GPU arm's own operands (xorshift64 from 42), and the process reports
+    the sha256 of its product so the two arms can be compared bit for bit."""
     try:
         from oracle import oracle as O
         use_ref = O.ref_available()
-        a, b = make_inputs(an, bn, seed)
+        a, b = xs_inputs(op, an, bn) if seed is None else make_inputs(an, bn, seed)
         f = (lambda: O.ref_sqr(a)) if (use_ref and op == "sqr") else \
             (lambda: O.ref_mul(a, b)) if use_ref else \
             (lambda: O.port_sqr(a)) if op == "sqr" else (lambda: O.port_mul(a, b))
@@ -263,12 +379,13 @@ def _cpu_worker(op, an, bn, seed, steps, warmup, barrier, queue):
             f()
         plan_s = time.time() - t0
         times = []
+        r = None
         for _ in range(steps):
             barrier.wait(timeout=3600)
             t = time.perf_counter()
-            f()
+            r = f()
             times.append(time.perf_counter() - t)
-        queue.put(("ok", plan_s, times))
+        queue.put(("ok", plan_s, times, sha256_limbs(r) if (seed is None and r is not None) else None))
     except Exception as e:  # reported to the parent
         try:
             barrier.abort()
@@ -294,7 +411,8 @@ def cpu_run(op: str, an: int, bn: int, procs: int, steps: int, warmup: int, seed
     ctx = mp.get_context("spawn")
     barrier = ctx.Barrier(procs)
     queue = ctx.Queue()
-    ps = [ctx.Process(target=_cpu_worker, args=(op, an, bn, seed + i, steps, warmup, barrier, queue))
+    ps = [ctx.Process(target=_cpu_worker,
+                      args=(op, an, bn, None if i == 0 else seed + i, steps, warmup, barrier, queue))
           for i in range(procs)]
     for p in ps:
         p.start()
@@ -311,8 +429,9 @@ def cpu_run(op: str, an: int, bn: int, procs: int, steps: int, warmup: int, seed
     step = statistics.median(step_times)
     cpu = O.host_cpu()
     isa = [f for f in O.REF_ISA if f in cpu["flags"]]
+    digests = [r[3] for r in res if len(r) > 3 and r[3]]
     return {"value": procs * (an + bn) / step / 1e6, "unit": "Mlimb/s", "cores": procs,
-            "kind": kind, "step_s": step,
+            "kind": kind, "step_s": step, "sha256_xs42": digests[0] if digests else None,
             "sample": f"{procs} single-threaded process(es) x one {op} {an}x{bn} per step, median of "
                       f"{steps} steps (step = slowest process) after {max(1, warmup)} warm-up "
                       f"(plan build {plan_s:.1f}s, excluded)",
@@ -1069,7 +1188,9 @@ def run_ours(args, ws, rank, local, pg) -> dict | None:
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     op, an, bn = WORKLOADS[args.workload]
-    a, b = make_inputs(an, bn, 1000 + rank)
+    # every rank multiplies the reference batteries' operands (xorshift64 from
+    # 42): the same inputs the committed reference digests were made from
+    a, b = xs_inputs(op, an, bn)
     ta = torch.from_numpy(a.view(np.int64)).to(dev)
     tb = torch.from_numpy(b.view(np.int64)).to(dev)
     tr = torch.empty(an + bn, dtype=torch.int64, device=dev)
@@ -1090,9 +1211,21 @@ def run_ours(args, ws, rank, local, pg) -> dict | None:
     for _ in range(args.warmup):
         step()
     ctx.sync()
-    # bit-exactness of what is timed: spot check of the warm-up product
+    # bit-exactness of what is timed: the warm-up product against the
+    # reference's own digest for these operands, plus the modular checks
+    # (2^61-1, 2^64-1, the low limb, and random primes from a logged seed)
     got = tr.cpu().numpy().view(np.uint64)
-    exact = product_ok(a, a if op == "sqr" else b, got)
+    bb = a if op == "sqr" else b
+    spot_seed = args.spot_seed if args.spot_seed is not None else int.from_bytes(os.urandom(4), "little")
+    primes = random_primes(spot_seed)
+    want_sha = golden_sha256(op, an, bn)
+    got_sha = sha256_limbs(got)
+    parity = {"reference_sha256": want_sha, "sha256": got_sha,
+              "reference_match": (got_sha == want_sha) if want_sha else None,
+              "modular_2p61m1_2p64m1": product_ok(a, bb, got),
+              "spot_seed": spot_seed, "spot_primes": primes,
+              "spot_ok": spot_check_primes(a, bb, got, primes)}
+    exact = bool(parity["modular_2p61m1_2p64m1"] and parity["spot_ok"] and parity["reference_match"] is not False)
 
     # ---- device-timed region (operands resident in HBM) ----
     if pg is not None:
@@ -1199,6 +1332,7 @@ def run_ours(args, ws, rank, local, pg) -> dict | None:
                    "an": an, "bn": bn, "parallelism": f"replicas x{ws} (no collective)",
                    "l2": "operands + 1.3 GB workspace exceed the 126 MB L2; no flush needed"},
         "bit_exact": bool(exact),
+        "parity": parity,
         "e2e": {"value": round(e2e_val, 2), "unit": "Mlimb/s", "h2d_bytes_per_step": 8 * (an + (0 if op == "sqr" else bn)),
                 "d2h_bytes_per_step": 8 * (an + bn),
                 "entry": "sbg_mul_host/sbg_sqr_host on pinned host buffers, steps queued back to back, "
@@ -1242,7 +1376,12 @@ def reference_line(args, op: str, an: int, bn: int) -> dict:
         metric, unit = "product Mlimb/s", "Mlimb/s"
         cfg = {"workload": f"{op} {an} x {bn} limbs, one product per step per GPU", "an": an, "bn": bn}
     cfg["parallelism"] = f"{r['cores']} host processes"
-    return {"metric": metric, "value": round(r["value"], 3), "unit": unit,
+    extra = {}
+    if r.get("sha256_xs42"):
+        want = golden_sha256(op, an, bn)
+        extra["parity"] = {"sha256": r["sha256_xs42"], "golden_sha256": want,
+                           "golden_match": (r["sha256_xs42"] == want) if want else None}
+    return {**extra, "metric": metric, "value": round(r["value"], 3), "unit": unit,
             "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": round(r["step_s"] * 1e3, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic: seeded uniform u64 limbs", "config": cfg, "impl": "reference",
@@ -1267,6 +1406,8 @@ def main():
     ap.add_argument("--len3-mask", type=lambda x: int(x, 0), default=None,
                     help="serve: 3*2^k length classes to use (bit k; default: the library's)")
     ap.add_argument("--cpu-requests", type=int, default=640, help="serve: CPU baseline sample")
+    ap.add_argument("--spot-seed", type=int, default=None,
+                    help="seed of the random spot-check primes (default: drawn and logged)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local, pg = (1, 0, 0, None)
@@ -1307,6 +1448,11 @@ def main():
                 res["cpu_baseline"] = cpu_run_serve(args.cpu_requests, cpu_threads_for(1 << 20, 1 << 20, cap=32))
             else:
                 res["cpu_baseline"] = cpu_bounded(op, an, bn)
+                # the reference's product of the same operands, bit for bit
+                ref_sha = res["cpu_baseline"].get("sha256_xs42")
+                if ref_sha and "parity" in res:
+                    res["parity"]["cpu_reference_match"] = ref_sha == res["parity"]["sha256"]
+                    res["bit_exact"] = bool(res["bit_exact"] and res["parity"]["cpu_reference_match"])
         except Exception as e:  # recorded, not fatal
             res["cpu_baseline"] = {"value": None, "unit": "Mlimb/s", "error": str(e)}
     print(json.dumps(res), flush=True)

@@ -279,6 +279,13 @@ int sbg_divrem_u64(uint64_t *qp, uint64_t *rp, const uint64_t *np, uint64_t nn64
 int sbg_mul_noalloc(uint64_t *rp, const uint64_t *ap, int64_t an, const uint64_t *bp, int64_t bn,
                     void *stream);
 int64_t sbg_noalloc_max_limbs(void);
+/* Waits for `stream`, then returns the status of the device-side checks of
+ * the sbg_mul_noalloc calls made on the current device since the last
+ * sbg_noalloc_status (SBG_OK, SBG_ETIMEOUT: the carry scan's bounded wait
+ * expired, SBG_ESPILL: the spill check failed), and clears it.  Errors
+ * accumulate until read, so an earlier queued call's error is not hidden by
+ * a later clean call.  Allocates nothing.  No counterpart in the reference. */
+int sbg_noalloc_status(void *stream);
 
 /* ---- diagnostics ---------------------------------------------------------- */
 

@@ -22,6 +22,18 @@
 // fully rewritten before they are read).  Calls that overlap on the GPU --
 // on different streams, or from several host threads -- race on the scratch;
 // callers must order them (one stream, or events).
+//
+// Errors found on the device (the carry look-back's bounded wait expiring,
+// the spill check) set bits in an error word inside the scratch.  They
+// accumulate over calls until sbg_noalloc_status reads them: it waits for the
+// caller's stream, returns the status the bits map to and zeroes the word, so
+// a later call's clean run cannot hide an earlier queued call's error.
+//
+// The set-up state (symbol addresses, tables, constants) is kept per device
+// for the life of the process; a cudaDeviceReset after the first call on a
+// device is not supported (the addresses and tables would be stale).  The
+// first calls on different devices run their set-up concurrently (one lock
+// per device).
 #include <cuda_runtime.h>
 #include <mutex>
 
@@ -77,11 +89,12 @@ struct NoallocDev {
     uint2* tw_i = nullptr;
 };
 
-static std::mutex g_na_mu;
-static NoallocDev g_na[64];
+#define SBG_NOALLOC_MAX_DEV 64
+static std::mutex g_na_mu[SBG_NOALLOC_MAX_DEV];
+static NoallocDev g_na[SBG_NOALLOC_MAX_DEV];
 
 static cudaError_t noalloc_setup(int dev, cudaStream_t st, NoallocDev** out) {
-    std::lock_guard<std::mutex> g(g_na_mu);
+    std::lock_guard<std::mutex> g(g_na_mu[dev]);
     NoallocDev* d = &g_na[dev];
     if (!d->ready) {
         cudaError_t e = cudaGetSymbolAddress((void**)&d->scratch, g_scratch);
@@ -123,7 +136,7 @@ extern "C" int sbg_mul_noalloc(uint64_t* rp, const uint64_t* ap, int64_t an, con
     if (!rp || !ap || !bp || an <= 0 || bn <= 0) return SBG_EINVAL;
     if (an + bn > SBG_NOALLOC_MAX_LIMBS) return SBG_EBAND;   // beyond the static scratch
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SBG_ENODEV;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= SBG_NOALLOC_MAX_DEV) return SBG_ENODEV;
     cudaStream_t st = (cudaStream_t)stream;
     NoallocDev* d = nullptr;
     if (noalloc_setup(dev, st, &d) != cudaSuccess) return SBG_ECUDA;
@@ -144,4 +157,26 @@ extern "C" int sbg_mul_noalloc(uint64_t* rp, const uint64_t* ap, int64_t an, con
         cudaSuccess)
         return SBG_ECUDA;
     return SBG_OK;
+}
+
+extern "C" int sbg_noalloc_status(void* stream) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= SBG_NOALLOC_MAX_DEV) return SBG_ENODEV;
+    NoallocDev* d = &g_na[dev];
+    {
+        std::lock_guard<std::mutex> g(g_na_mu[dev]);
+        if (!d->ready) return SBG_OK;           // no call has run on this device
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    uint32_t* err = d->scratch + SBG_NOALLOC_RES_WORDS + SBG_NOALLOC_FLAG_WORDS;
+    uint32_t h = 0;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return SBG_ECUDA;
+    if (cudaMemcpy(&h, err, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return SBG_ECUDA;
+    if (!h) return SBG_OK;
+    if (cudaMemsetAsync(err, 0, sizeof(uint32_t), st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return SBG_ECUDA;
+    if (h & 1u) return SBG_ETIMEOUT;
+    if (h & 2u) return SBG_ESPILL;
+    return SBG_ECUDA;
 }

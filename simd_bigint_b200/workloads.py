@@ -34,6 +34,76 @@ def division_shapes(count: int = 1024, seed: int = 4242, lo: int = 512,
     return [int(math.exp(rng.uniform(math.log(lo), math.log(hi)))) for _ in range(count)]
 
 
+_M64 = (1 << 64) - 1
+
+
+def _xs_step_int(s: int) -> int:
+    s ^= (s << 13) & _M64
+    s ^= s >> 7
+    s ^= (s << 17) & _M64
+    return s
+
+
+def _xs_jump(k: int) -> list[int]:
+    """Columns of the GF(2) matrix of k xorshift64 steps (the generator is
+    linear over GF(2)^64): column i is the image of the unit state 1 << i."""
+    cols = [_xs_step_int(1 << i) for i in range(64)]          # one step
+    acc = [1 << i for i in range(64)]                          # identity
+
+    def apply(m, v):
+        r = 0
+        i = 0
+        while v:
+            if v & 1:
+                r ^= m[i]
+            v >>= 1
+            i += 1
+        return r
+
+    while k:
+        if k & 1:
+            acc = [apply(cols, c) for c in acc]
+        cols = [apply(cols, c) for c in cols]
+        k >>= 1
+    return acc
+
+
+def xorshift64_limbs(n: int, state: int = 42, lanes: int = 4096) -> tuple[np.ndarray, int]:
+    """n consecutive outputs of the xorshift64 generator (state ^= state << 13,
+    ^= state >> 7, ^= state << 17; each output is the new state), the stream
+    the reference's test batteries draw their operands from, and the state
+    after them (to continue the stream for a second operand).  Vectorised:
+    `lanes` independent starting points are found by jumping the linear
+    generator ahead, then all lanes step together."""
+    if n <= 0:
+        return np.zeros(0, dtype=np.uint64), state
+    lanes = max(1, min(lanes, n))
+    chunk = -(-n // lanes)
+    jump = _xs_jump(chunk)
+    starts = []
+    s = state
+    for _ in range(lanes):
+        starts.append(s)
+        r = 0
+        v, i = s, 0
+        while v:
+            if v & 1:
+                r ^= jump[i]
+            v >>= 1
+            i += 1
+        s = r
+    st = np.array(starts, dtype=np.uint64)
+    out = np.empty((lanes, chunk), dtype=np.uint64)
+    a, b, c = np.uint64(13), np.uint64(7), np.uint64(17)
+    for i in range(chunk):
+        st ^= st << a
+        st ^= st >> b
+        st ^= st << c
+        out[:, i] = st
+    flat = out.reshape(-1)[:n].copy()
+    return flat, int(flat[-1])
+
+
 def fill_limbs(n: int, rng: np.random.Generator, top_bit: bool = False) -> np.ndarray:
     x = rng.integers(0, 2**64, size=n, dtype=np.uint64)
     if n:

@@ -3,6 +3,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import os
 from pathlib import Path
 
 import numpy as np
@@ -11,9 +12,48 @@ from oracle import oracle as O
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "golden.json"
 
-# the reference batteries' spot-check idea: random 61-bit primes
-SPOT_PRIMES = [2305843009213693951, 2305843009213693921, 2305843009213693907,
-               2305843009213693669]
+def _is_prime(n: int) -> bool:
+    """Miller-Rabin with the first twelve prime bases (deterministic below 3.3e24)."""
+    if n < 2:
+        return False
+    small = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37)
+    for p in small:
+        if n % p == 0:
+            return n == p
+    d, s = n - 1, 0
+    while d % 2 == 0:
+        d //= 2
+        s += 1
+    for a in small:
+        x = pow(a, d, n)
+        if x in (1, n - 1):
+            continue
+        for _ in range(s - 1):
+            x = x * x % n
+            if x == n - 1:
+                break
+        else:
+            return False
+    return True
+
+
+def random_primes(seed: int, k: int = 4, bits: int = 61) -> list[int]:
+    """k distinct random primes of `bits` bits drawn from `seed`."""
+    import random
+    rnd = random.Random(seed)
+    out: list[int] = []
+    while len(out) < k:
+        c = rnd.getrandbits(bits) | (1 << (bits - 1)) | 1
+        if c not in out and _is_prime(c):
+            out.append(c)
+    return out
+
+
+# The modular spot check draws fresh random 61-bit primes in every session,
+# from a seed that is logged (and replayable through SBG_SPOT_SEED).
+SPOT_SEED = int(os.environ.get("SBG_SPOT_SEED") or int.from_bytes(os.urandom(4), "little"))
+SPOT_PRIMES = random_primes(SPOT_SEED)
+print(f"[spot check] seed {SPOT_SEED}: primes {SPOT_PRIMES}")
 
 
 def golden() -> dict:

@@ -3,7 +3,7 @@ reference (oracle/_ref/libsbref.so, built by `make -C oracle ref` from the
 reference's own sources).  Run in a container that has the reference and an
 AVX-512 IFMA host:
 
-    python tests/golden/gen_golden.py
+    python tests/golden/gen_golden.py [--missing]
 
 Inputs are regenerated from their description (xorshift64 seed or a fixed
 fill pattern, see golden_inputs()), so the file stores only the shape, the
@@ -39,8 +39,15 @@ MUL_CASES = [
     ("sqr", 80, 80, "xs", 5), ("sqr", 4096, 4096, "ones", 0),
     ("sqr", 65536, 65536, "weyl_a", 0), ("sqr", 1 << 20, 1 << 20, "xs", 9),
     ("sqr", 1 << 21, 1 << 21, "ones", 0),
+    # the large single-product configurations, on the same xorshift64 stream
+    # (seed 42) that bench.py multiplies: 2^24 x 2^24, sqr 2^24, 2^24 x 2^20
+    ("mul", 1 << 24, 1 << 24, "xs", 42),
+    ("sqr", 1 << 24, 1 << 24, "xs", 42),
+    ("mul", 1 << 24, 1 << 20, "xs", 42),
+    ("sqr", 1 << 22, 1 << 22, "xs", 42),
 ]
-DIV_CASES = [(1024, 512, 21), (2000, 1000, 22), (8192, 4096, 23), (131072, 65536, 24)]
+DIV_CASES = [(1024, 512, 21), (2000, 1000, 22), (8192, 4096, 23), (131072, 65536, 24),
+             (524288, 262144, 25)]                   # the top divisor size of the division batch
 
 
 def golden_inputs(op: str, an: int, bn: int, pat: str, seed: int):
@@ -70,17 +77,30 @@ def summary(x: np.ndarray) -> dict:
 
 
 def main():
+    """Writes golden.json.  With --missing, entries already in the file are
+    kept and only cases not yet present are computed (a reference product at
+    2^24 limbs costs minutes including its plan build on a slow host)."""
     if not O.ref_available():
         raise SystemExit("reference oracle not available (make -C oracle ref; AVX-512 IFMA host)")
+    keep = "--missing" in sys.argv[1:] and (HERE / "golden.json").exists()
+    old = json.loads((HERE / "golden.json").read_text()) if keep else {"mul": [], "div": []}
+    have_mul = {(e["op"], e["an"], e["bn"], e["pattern"], e["seed"]): e for e in old["mul"]}
+    have_div = {(e["nn"], e["dn"], e["seed"]): e for e in old["div"]}
     out = {"generator": "tests/golden/gen_golden.py", "source": "reference nt_mul / nt_sqr / divrem_u64_dc",
            "mul": [], "div": []}
     for op, an, bn, pat, seed in MUL_CASES:
+        if (op, an, bn, pat, seed) in have_mul:
+            out["mul"].append(have_mul[(op, an, bn, pat, seed)])
+            continue
         t = time.time()
         a, b = golden_inputs(op, an, bn, pat, seed)
         r = O.ref_sqr(a) if op == "sqr" else O.ref_mul(a, b)
         out["mul"].append({"op": op, "an": an, "bn": bn, "pattern": pat, "seed": seed, **summary(r)})
         print(op, an, bn, pat, f"{time.time() - t:.2f}s", flush=True)
     for n2, n, seed in DIV_CASES:
+        if (n2, n, seed) in have_div:
+            out["div"].append(have_div[(n2, n, seed)])
+            continue
         a, d = div_inputs(n, seed)
         q, r = O.ref_divrem(a, d)
         out["div"].append({"nn": n2, "dn": n, "seed": seed, "q": summary(q), "r": summary(r)})

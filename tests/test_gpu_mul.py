@@ -7,8 +7,11 @@ all-0xFF / sparse / Weyl patterns at the caps, random shapes, squaring.
 Ground truth is the reference's own output (golden vectors generated by the
 unmodified reference, tests/golden/gen_golden.py) or, where no golden exists,
 our C restatement of the reference algorithm (oracle/port.c) and Python big
-integers; at 2^24 limbs, where a CPU product takes seconds, the closed form
-of the all-0xFF square and the random-prime modular spot check stand in.
+integers.  The large single-product configurations (2^24 x 2^24, sqr 2^24,
+2^24 x 2^20, 2^22 x 2^22) are golden vectors of the reference's own nt_mul /
+nt_sqr on its batteries' xorshift64 operands; on top of them the closed form
+of the all-0xFF square and a modular spot check with random 61-bit primes
+(drawn per session from a logged seed) cover other operands at that size.
 Every comparison is bit-exact.
 """
 import numpy as np
