@@ -1054,7 +1054,8 @@ def run_serve(args, ws, rank, local, pg) -> dict | None:
     sops = serve_operands(sreqs, pool, seed=78 + rank)
     slimbs = sum(serve_out_limbs(k, an, bn) for k, an, bn in sreqs)
     skinds = np.array([k for k, _, _ in sreqs])
-    for j, f in enumerate(SERVE_FRACS if n_sweep else ()):
+    fracs = getattr(args, "serve_fracs", SERVE_FRACS)
+    for j, f in enumerate(fracs if n_sweep else ()):
         # offered load: fraction f of the measured capacity, in requests of this stream
         rate = f * capacity * (limbs / n_main) / (slimbs / n_sweep)
         arr = poisson_arrivals(n_sweep, rate, seed=300 + j)
@@ -1086,7 +1087,7 @@ def run_serve(args, ws, rank, local, pg) -> dict | None:
         "config": {"workload": f"serving: {n_main} mul/sqr/reciprocal requests (50/30/20%), sizes log-uniform "
                                "[32, 2^20] limbs, 70% balanced / 30% unbalanced (ratio up to 16), seed 2025; "
                                "submitted as one burst (sbg_server_submit_many, saturation), then a Poisson arrival-rate sweep of "
-                               f"{n_sweep} requests at {list(SERVE_FRACS)} of that capacity",
+                               f"{n_sweep} requests at {list(fracs)} of that capacity",
                    "requests": n_main, "parallelism": f"replicas x{ws}",
                    "server": {"arena_gb": args.arena_gb, "slots": args.slots, "max_batch": 256,
                               "batch_lg_points": args.batch_lg_points or 26},
@@ -1348,6 +1349,40 @@ def run_ours(args, ws, rank, local, pg) -> dict | None:
     return result
 
 
+def run_extras(args, ws, rank, local, pg) -> dict:
+    """The metric's other parts, measured compactly beside the single-product
+    line: the mixed-size batch (batched vs one product per launch over the
+    same 4096 products) and one serving point (Poisson arrivals at 60% of a
+    measured capacity, p50 / p99 latency)."""
+    import copy
+    out = {}
+    ab = copy.copy(args)
+    ab.steps, ab.warmup = 5, 3
+    b = run_batch(ab, ws, rank, local, pg)
+    if b is not None:
+        out["batch4096"] = {
+            "metric": b["metric"], "value": b["value"], "unit": b["unit"], "ms_per_step": b["ms_per_step"],
+            "one_per_launch": b["one_per_launch"], "bit_exact": b["bit_exact"],
+            "e2e": {"value": b["e2e"]["value"], "unit": b["e2e"]["unit"]},
+            "gpu_launches_per_step": round(b["gpu_launches"] / ab.steps, 1),
+            "engine": b.get("engine"), "config": b["config"]["workload"], "steps": ab.steps}
+    asv = copy.copy(args)
+    asv.requests, asv.sweep_requests, asv.serve_fracs = 20000, 6000, (0.6,)
+    asv.warmup = 3
+    sv = run_serve(asv, ws, rank, local, pg)
+    if sv is not None:
+        pt = sv["sweep"][0] if sv["sweep"] else {}
+        out["serve"] = {
+            "capacity_req_s": sv["value"], "served_mlimb_s": sv["served_mlimb_s"],
+            "requests_at_saturation": asv.requests,
+            "at_60pct_load": {"offered_req_s": pt.get("offered_req_s"), "requests": asv.sweep_requests,
+                              "p50_ms": pt.get("p50_ms"), "p99_ms": pt.get("p99_ms"),
+                              "by_kind": pt.get("by_kind")},
+            "bit_exact": sv["bit_exact"], "checked_results": sv["checked_results"],
+            "config": "serving stream (seed 2025): mul/sqr/reciprocal 50/30/20%, sizes log-uniform [32, 2^20]"}
+    return out
+
+
 def reference_line(args, op: str, an: int, bn: int) -> dict:
     """The reference arm: the reference's own CPU code on a bounded sample of
     the same workload, reported in the same metric, unit and config as ours."""
@@ -1398,6 +1433,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="mul2p24")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="single-product workloads: skip the compact batch and serving measurements")
     ap.add_argument("--requests", type=int, default=200000, help="serve: requests at saturation")
     ap.add_argument("--sweep-requests", type=int, default=20000, help="serve: requests per sweep point")
     ap.add_argument("--arena-gb", type=int, default=16, help="serve: server arena (GiB)")
@@ -1429,6 +1466,10 @@ def main():
         res = run_serve(args, ws, rank, local, pg)
     else:
         res = run_ours(args, ws, rank, local, pg)
+        if not args.no_extras:
+            extras = run_extras(args, ws, rank, local, pg)
+            if res is not None:
+                res.update(extras)
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()

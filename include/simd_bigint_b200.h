@@ -46,7 +46,8 @@ enum {
     SBG_ETIMEOUT = 5,  /* a bounded device-side wait expired                   */
     SBG_ESPILL = 6,    /* the product spilled past its top limb (internal)     */
     SBG_EADMIT = 7,    /* serving: request rejected by admission control       */
-    SBG_ENODEV = 8     /* no CUDA device / library built without device code  */
+    SBG_ENODEV = 8,    /* no CUDA device / library built without device code  */
+    SBG_ECANCELED = 9  /* serving: request cancelled before it was launched    */
 };
 
 typedef struct sbg_ctx sbg_ctx;
@@ -107,6 +108,27 @@ int sbg_sqr(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an);
  * include/mulmid.h:5-18 (the reference has no library implementation). */
 int sbg_mulmid(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an, const uint64_t *bp,
                int64_t bn);
+
+/* ---- u52 redundant-digit boundary -------------------------------------------
+ * Radix-2^52 digits in 64-bit lanes, the form the reference keeps inside its
+ * multiply and division code, converted on the device so that code holding
+ * such digits can use the GPU multiply without converting on the host.  All
+ * pointers are device memory; work is queued on the context's stream.
+ *
+ * sbg_u52_from_u64: dp[i] = bits [52 i, 52 i + 52) of {ap, an}, i < n52
+ * (digits beyond the number are zero; the reference's u52_from_u64 writes
+ * ceil(bitlength / 52) of them -- include/u64cvt.h:42).
+ * sbg_u64_from_u52: rp[0 .. rn) = (sum_i dp[i] 2^(52 i)) mod 2^(64 rn) for
+ * redundant digits -- unsigned lanes (is_signed = 0, the reference's
+ * u64_from_u52_canon, include/canon.h:324) or two's-complement signed lanes
+ * (is_signed = 1, u64_from_u52_canonneg, include/canon.h:303).
+ * sbg_mul_u52: rp[0 .. an52 + bn52) = the canonical digits of the product
+ * of two canonical digit arrays (each digit < 2^52). */
+int sbg_u52_from_u64(sbg_ctx *ctx, uint64_t *dp, int64_t n52, const uint64_t *ap, int64_t an);
+int sbg_u64_from_u52(sbg_ctx *ctx, uint64_t *rp, int64_t rn, const uint64_t *dp, int64_t n52,
+                     int is_signed);
+int sbg_mul_u52(sbg_ctx *ctx, uint64_t *rp, const uint64_t *ap, int64_t an52, const uint64_t *bp,
+                int64_t bn52);
 
 /* ---- host-pointer entries, stream-ordered ---------------------------------
  * The product of HOST operands into a HOST result, queued and returned at
@@ -234,6 +256,10 @@ int sbg_server_submit_many(sbg_server *srv, const sbg_request *reqs, int64_t cou
 int sbg_server_poll(sbg_server *srv, sbg_completion *out, int max, int *n, int wait_ms);
 /* Frees a completed request's result buffer. */
 int sbg_server_release(sbg_server *srv, uint64_t ticket);
+/* Cancels a request that is still queued: it completes at once with status
+ * SBG_ECANCELED and no result.  SBG_EINVAL when the ticket is unknown or the
+ * request has already been launched or completed (it then runs to the end). */
+int sbg_server_cancel(sbg_server *srv, uint64_t ticket);
 int sbg_server_stats(sbg_server *srv, int64_t *pending, int64_t *completed, int64_t *batches,
                      size_t *arena_used);
 /* Kernel launches queued by the server so far (multiply batches and reciprocals). */
@@ -286,6 +312,24 @@ int64_t sbg_noalloc_max_limbs(void);
  * accumulate until read, so an earlier queued call's error is not hidden by
  * a later clean call.  Allocates nothing.  No counterpart in the reference. */
 int sbg_noalloc_status(void *stream);
+
+/* ---- test hooks (error paths) ------------------------------------------------
+ * For tests of the failure paths without faulting the GPU; no counterpart in
+ * the reference.  sbg_debug_inject sets, for the current device, test hooks
+ * of the CRT + carry kernel that change data or withhold a flag (0 = off):
+ *   SBG_INJECT_WITHHOLD  the first block of each carry scan never publishes
+ *                        its look-back flag, and the look-back's bounded wait
+ *                        is shortened, so the next block's wait runs out:
+ *                        the product is wrong and the status SBG_ETIMEOUT;
+ *   SBG_INJECT_TOP       the top coefficient's first residue is altered
+ *                        before Garner: the product spills, SBG_ESPILL;
+ *   SBG_INJECT_MID       a middle coefficient's residue is altered: a wrong
+ *                        product that no device check sees (for host checks).
+ * sbg_debug_fail_allocs(n): the next n device allocations of contexts
+ * (workspace, plan tables) fail as an out-of-memory device would (SBG_EALLOC). */
+enum { SBG_INJECT_WITHHOLD = 1, SBG_INJECT_TOP = 2, SBG_INJECT_MID = 4 };
+int sbg_debug_inject(uint32_t mask);
+void sbg_debug_fail_allocs(int n);
 
 /* ---- diagnostics ---------------------------------------------------------- */
 

@@ -106,6 +106,10 @@ def ref():
             getattr(lib, name).restype = None
         lib.sbref_mul_router.argtypes = [C.c_int, _u64p, _u64p, u64, _u64p, u64]
         lib.sbref_mul_router.restype = C.c_int
+        lib.sbref_u52_from_u64.argtypes = [_u64p, _u64p, u64]
+        lib.sbref_u52_from_u64.restype = u64
+        lib.sbref_u64_from_u52.argtypes = [_u64p, u64, _u64p, u64, C.c_int]
+        lib.sbref_u64_from_u52.restype = None
         lib.sbref_run_threads.argtypes = [C.c_void_p, i64, C.c_int]
         lib.sbref_run_threads.restype = C.c_int
         _ref = lib
@@ -251,6 +255,67 @@ def ref_divrem(n: np.ndarray, d: np.ndarray, dc: bool = True) -> tuple[np.ndarra
 class Job(C.Structure):
     _fields_ = [("kind", C.c_int32), ("pad", C.c_int32), ("r", C.c_void_p), ("r2", C.c_void_p),
                 ("a", C.c_void_p), ("b", C.c_void_p), ("an", C.c_uint64), ("bn", C.c_uint64)]
+
+
+# ------------------------------------------------ u52 redundant digits --
+M52 = (1 << 52) - 1
+
+
+def _digits_of(v: int, n: int, out: list) -> None:
+    """Appends the n low radix-2^52 digits of v >= 0 (divide and conquer, so
+    long numbers cost O(bits log n) instead of O(bits n))."""
+    if n <= 64:
+        for i in range(n):
+            out.append((v >> (52 * i)) & M52)
+        return
+    h = n // 2
+    _digits_of(v & ((1 << (52 * h)) - 1), h, out)
+    _digits_of(v >> (52 * h), n - h, out)
+
+
+def _value_of(d: list, lo: int, hi: int) -> int:
+    """sum_{lo <= i < hi} d[i] 2^(52 (i - lo)) for any integer lanes."""
+    if hi - lo <= 64:
+        v = 0
+        for i in range(hi - 1, lo - 1, -1):
+            v = (v << 52) + d[i]
+        return v
+    m = (lo + hi) // 2
+    return _value_of(d, lo, m) + (_value_of(d, m, hi) << (52 * (m - lo)))
+
+
+def u52_from_u64(a: np.ndarray) -> np.ndarray:
+    """Canonical radix-2^52 digits of {a}: ceil(bitlength / 52) of them (the
+    reference's u52_from_u64, include/u64cvt.h:42-58), by Python integers."""
+    v = to_int(np.ascontiguousarray(a, dtype=np.uint64))
+    n52 = (v.bit_length() + 51) // 52
+    out: list = []
+    _digits_of(v, n52, out)
+    return np.array(out, dtype=np.uint64)
+
+
+def u64_from_u52(d: np.ndarray, out_limbs: int, signed: bool = False) -> np.ndarray:
+    """sum_i d[i] 2^(52 i) mod 2^(64 out_limbs) for redundant digits: unsigned
+    64-bit lanes, or two's-complement signed lanes (the reference's
+    u64_from_u52_canon / _canonneg, include/canon.h:303-324)."""
+    lanes = np.asarray(d, dtype=np.uint64)
+    vals = (lanes.view(np.int64) if signed else lanes).tolist()
+    v = _value_of(vals, 0, len(vals)) & ((1 << (64 * out_limbs)) - 1)
+    return from_int(v, out_limbs) if out_limbs else np.zeros(0, dtype=np.uint64)
+
+
+def ref_u52_from_u64(a: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    out = np.zeros(len(a) * 64 // 52 + 2, dtype=np.uint64)
+    n = ref().sbref_u52_from_u64(_ptr(out), _ptr(a) if len(a) else _ptr(out), len(a))
+    return out[:n].copy()
+
+
+def ref_u64_from_u52(d: np.ndarray, out_limbs: int, signed: bool = False) -> np.ndarray:
+    d = np.ascontiguousarray(d, dtype=np.uint64)
+    r = np.zeros(max(out_limbs, 1), dtype=np.uint64)
+    ref().sbref_u64_from_u52(_ptr(r), out_limbs, _ptr(d) if len(d) else _ptr(r), len(d), int(signed))
+    return r[:out_limbs]
 
 
 def run_jobs(jobs: list[tuple], threads: int, which: str) -> int:

@@ -18,6 +18,12 @@
  *   sbref_run_threads                -> runs a list of independent jobs on T
  *                                       pthreads (one job at a time per thread),
  *                                       the multi-core CPU baseline.
+ *   sbref_u52_from_u64               -> u52_from_u64           (include/u64cvt.h:42)
+ *   sbref_u64_from_u52               -> u64_from_u52_canon / u64_from_u52_canonneg
+ *                                       (include/canon.h:303-324), the u52
+ *                                       redundant-digit boundary; plain arrays
+ *                                       are copied into the 64-byte aligned,
+ *                                       vector-padded buffers those functions take.
  */
 #define SCRATCH_IMPLEMENTATION
 #include "ntmul.h"
@@ -26,6 +32,8 @@
 
 #include <pthread.h>
 #include <stdatomic.h>
+#include <stdlib.h>
+#include <string.h>
 
 int sbref_nt_mul(uint64_t *rp, const uint64_t *ap, int64_t an,
                  const uint64_t *bp, int64_t bn){
@@ -121,4 +129,35 @@ int sbref_run_threads(sbref_job *jobs, int64_t njobs, int threads){
     for(int t = 0; t < threads; ++t)
         pthread_join(tid[t], NULL);
     return atomic_load(&pool.fails);
+}
+
+/* ---- u52 redundant-digit boundary ----------------------------------------- */
+/* n52 canonical u52 digits of {ap, an} into out (room for an*64/52 + 1
+ * digits); returns n52. */
+uint64_t sbref_u52_from_u64(uint64_t *out, const uint64_t *ap, uint64_t an){
+    const uint64_t cap = (an * 64 + 51) / 52 + 16;
+    uint64_t *buf = aligned_alloc(64, ((cap * 8 + 63) / 64) * 64);
+    if(!buf) return 0;
+    memset(buf, 0, ((cap * 8 + 63) / 64) * 64);
+    const uint64_t n52 = u52_from_u64((pvec)buf, ap, an);
+    memcpy(out, buf, n52 * 8);
+    free(buf);
+    return n52;
+}
+
+/* rp[0 .. out_limbs) = sum_i d[i] 2^(52 i) for n52 redundant digits: each
+ * d[i] an unsigned 64-bit lane (is_signed = 0, u64_from_u52_canon) or a
+ * two's-complement signed lane (is_signed = 1, u64_from_u52_canonneg). */
+void sbref_u64_from_u52(uint64_t *rp, uint64_t out_limbs, const uint64_t *d, uint64_t n52,
+                        int is_signed){
+    const uint64_t need = (out_limbs * 64 + 51) / 52 + 16;
+    const uint64_t cap = (need > n52 ? need : n52) + 16;
+    const size_t bytes = ((cap * 8 + 63) / 64) * 64;
+    uint64_t *buf = aligned_alloc(64, bytes);
+    if(!buf) return;
+    memset(buf, 0, bytes);
+    memcpy(buf, d, n52 * 8);
+    if(is_signed) u64_from_u52_canonneg(rp, (cpvec)buf, out_limbs);
+    else u64_from_u52_canon(rp, (cpvec)buf, out_limbs);
+    free(buf);
 }

@@ -26,7 +26,7 @@ __all__ = [
 
 STATUS = {
     0: "SBG_OK", 1: "SBG_EINVAL", 2: "SBG_EBAND", 3: "SBG_EALLOC", 4: "SBG_ECUDA",
-    5: "SBG_ETIMEOUT", 6: "SBG_ESPILL", 7: "SBG_EADMIT", 8: "SBG_ENODEV",
+    5: "SBG_ETIMEOUT", 6: "SBG_ESPILL", 7: "SBG_EADMIT", 8: "SBG_ENODEV", 9: "SBG_ECANCELED",
 }
 
 _lib = None
@@ -123,6 +123,22 @@ def lib(build_if_missing: bool = False):
         L.sbg_server_poll.restype = C.c_int
         L.sbg_server_release.argtypes = [_vp, C.c_uint64]
         L.sbg_server_release.restype = C.c_int
+        L.sbg_server_cancel.argtypes = [_vp, C.c_uint64]
+        L.sbg_server_cancel.restype = C.c_int
+        L.sbg_debug_inject.argtypes = [C.c_uint32]
+        L.sbg_debug_inject.restype = C.c_int
+        L.sbg_debug_fail_allocs.argtypes = [C.c_int]
+        L.sbg_debug_fail_allocs.restype = None
+        L.sbg_noalloc_status.argtypes = [_vp]
+        L.sbg_noalloc_status.restype = C.c_int
+        L.sbg_mul_noalloc.argtypes = [_vp, _vp, _i64, _vp, _i64, _vp]
+        L.sbg_mul_noalloc.restype = C.c_int
+        L.sbg_u52_from_u64.argtypes = [_vp, _vp, _i64, _vp, _i64]
+        L.sbg_u52_from_u64.restype = C.c_int
+        L.sbg_u64_from_u52.argtypes = [_vp, _vp, _i64, _vp, _i64, C.c_int]
+        L.sbg_u64_from_u52.restype = C.c_int
+        L.sbg_mul_u52.argtypes = [_vp, _vp, _vp, _i64, _vp, _i64]
+        L.sbg_mul_u52.restype = C.c_int
         L.sbg_server_stats.argtypes = [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                        C.POINTER(C.c_int64), C.POINTER(C.c_size_t)]
         L.sbg_server_stats.restype = C.c_int
@@ -295,6 +311,22 @@ class Context:
         bn = b.numel() if bn is None else bn
         _check(self._L.sbg_mulmid(self.handle, _dptr(r), _dptr(a), an, _dptr(b), bn), "sbg_mulmid")
 
+    # ---- u52 redundant-digit boundary (device tensors of 64-bit lanes) ----
+    def u52_from_u64(self, d, a):
+        """d[i] = bits [52 i, 52 i + 52) of a, for i < d.numel()."""
+        _check(self._L.sbg_u52_from_u64(self.handle, _dptr(d), d.numel(), _dptr(a), a.numel()),
+               "sbg_u52_from_u64")
+
+    def u64_from_u52(self, r, d, signed: bool = False):
+        """r = sum_i d[i] 2^(52 i) mod 2^(64 r.numel()), lanes unsigned or signed."""
+        _check(self._L.sbg_u64_from_u52(self.handle, _dptr(r), r.numel(), _dptr(d), d.numel(), int(signed)),
+               "sbg_u64_from_u52")
+
+    def mul_u52(self, r, a, b):
+        """r (a.numel() + b.numel() digits) = the canonical digits of a * b."""
+        _check(self._L.sbg_mul_u52(self.handle, _dptr(r), _dptr(a), a.numel(), _dptr(b), b.numel()),
+               "sbg_mul_u52")
+
 
 JOB_MUL, JOB_SQR, JOB_MULMID = 0, 1, 2
 
@@ -353,6 +385,8 @@ class Batch:
 
 
 REQ_MUL, REQ_SQR, REQ_RECIP = 0, 1, 2
+# test hooks of the CRT kernel (sbg_debug_inject)
+INJECT_WITHHOLD, INJECT_TOP, INJECT_MID = 1, 2, 4
 
 
 class Request(C.Structure):
@@ -432,6 +466,11 @@ class Server:
 
     def release(self, ticket: int):
         _check(self._L.sbg_server_release(self.handle, ticket), "sbg_server_release")
+
+    def cancel(self, ticket: int) -> bool:
+        """Cancels a still-queued request (it completes with SBG_ECANCELED);
+        False when it was already launched or completed."""
+        return self._L.sbg_server_cancel(self.handle, ticket) == 0
 
     def launches(self) -> int:
         """Kernel launches the server has queued so far."""

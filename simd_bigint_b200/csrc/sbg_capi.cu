@@ -5,6 +5,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -26,6 +27,15 @@ int cuda_fail(cudaError_t e, const char* where) {
         cudaError_t e_ = (call);                            \
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
+
+static std::atomic<int> g_fail_allocs{0};
+
+cudaError_t dev_alloc(void** p, size_t bytes) {
+    int n = g_fail_allocs.load();
+    while (n > 0)
+        if (g_fail_allocs.compare_exchange_weak(n, n - 1)) return cudaErrorMemoryAllocation;
+    return cudaMalloc(p, bytes);
+}
 
 int lg_ceil(int64_t n) {
     int l = 0;
@@ -66,14 +76,19 @@ int ensure_plan(sbg_ctx* c, int lgL) {
         np.hi_n = (int)(np.L >> 13);
         size_t lo_b = (size_t)SBG_NP * 8192 * sizeof(uint2);
         size_t hi_b = (size_t)SBG_NP * np.hi_n * sizeof(uint2);
-        CK(cudaMalloc(&np.fs_lo_f, lo_b));
-        CK(cudaMalloc(&np.fs_lo_i, lo_b));
-        CK(cudaMalloc(&np.fs_hi_f, hi_b));
-        CK(cudaMalloc(&np.fs_hi_i, hi_b));
+        const size_t t3_b = np.m3 >= 0 ? (size_t)SBG_NP * (2 << np.m3) * sizeof(uint2) : 0;
+        uint2** bufs[6] = {&np.fs_lo_f, &np.fs_lo_i, &np.fs_hi_f, &np.fs_hi_i, &np.t3_f, &np.t3_i};
+        const size_t sizes[6] = {lo_b, lo_b, hi_b, hi_b, t3_b, t3_b};
+        for (int k = 0; k < 6; ++k) {
+            if (!sizes[k]) continue;
+            cudaError_t e = dev_alloc((void**)bufs[k], sizes[k]);
+            if (e != cudaSuccess) {                 // nothing of the plan is kept
+                for (int j = 0; j < k; ++j)
+                    if (*bufs[j]) cudaFree(*bufs[j]);
+                return cuda_fail(e, "plan tables");
+            }
+        }
         if (np.m3 >= 0) {
-            size_t t3_b = (size_t)SBG_NP * (2 << np.m3) * sizeof(uint2);
-            CK(cudaMalloc(&np.t3_f, t3_b));
-            CK(cudaMalloc(&np.t3_i, t3_b));
             for (int q = 0; q < SBG_NP; ++q) {     // cube roots of unity w_N1^M
                 const uint32_t p = kPrimes[q];
                 const uint32_t w = host_powmod(kGenerators[q], (p - 1) / 3, p);
@@ -99,7 +114,7 @@ static int ensure_ws(sbg_ctx* c, size_t words, size_t flag_words) {
         if (c->ws) cudaFree(c->ws);
         c->ws = nullptr;
         c->ws_cap = 0;
-        CK(cudaMalloc(&c->ws, words * sizeof(uint32_t)));
+        CK(dev_alloc((void**)&c->ws, words * sizeof(uint32_t)));
         c->ws_cap = words;
     }
     if (flag_words > c->flags_cap) {
@@ -108,7 +123,7 @@ static int ensure_ws(sbg_ctx* c, size_t words, size_t flag_words) {
         c->flags = nullptr;
         c->flags_cap = 0;
         size_t fw = flag_words < 4096 ? 4096 : flag_words;
-        CK(cudaMalloc(&c->flags, fw * sizeof(uint32_t)));
+        CK(dev_alloc((void**)&c->flags, fw * sizeof(uint32_t)));
         c->flags_cap = fw;
     }
     return SBG_OK;
@@ -129,6 +144,16 @@ static int run_conv(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, co
     CK(launch_crt_carry(c->ws, lgL, lp, cmin, cmax, off, rp, nout, c->flags, c->err, c->stream,
                         c->timer));
     c->launches += class_launches(lgL);
+    return SBG_OK;
+}
+
+// A plain product of at most SBG_SCHOOL_MAX limbs: one schoolbook warp.
+static int run_school(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, const uint64_t* bp,
+                      int64_t bn) {
+    KT_BEGIN(c->timer, KID_SMALL, c->stream);
+    CK(launch_school(ap, an, bp, bn, rp, c->stream));
+    KT_END(c->timer, KID_SMALL, c->stream);
+    c->launches += 1;
     return SBG_OK;
 }
 
@@ -167,12 +192,12 @@ static int job_shape(const sbg_job& j, uint32_t mask3, int* lgL, int64_t* cmin, 
         case SBG_JOB_MUL:
             if (!j.bp || j.bn <= 0) return SBG_EINVAL;
             if (j.an + j.bn - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
-            *lgL = conv_lg(j.an + j.bn - 1, mask3);
+            *lgL = j.an + j.bn <= SBG_SCHOOL_MAX ? SBG_CODE_SCHOOL : conv_lg(j.an + j.bn - 1, mask3);
             *cmin = 0; *cmax = j.an + j.bn - 2; *off = 0; *nout = j.an + j.bn; *sq = 0;
             return SBG_OK;
         case SBG_JOB_SQR:
             if (2 * j.an - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
-            *lgL = conv_lg(2 * j.an - 1, mask3);
+            *lgL = 2 * j.an <= SBG_SCHOOL_MAX ? SBG_CODE_SCHOOL : conv_lg(2 * j.an - 1, mask3);
             *cmin = 0; *cmax = 2 * j.an - 2; *off = 0; *nout = 2 * j.an; *sq = 1;
             return SBG_OK;
         case SBG_JOB_CYCLIC: {
@@ -378,6 +403,7 @@ const char* sbg_strerror(int status) {
         case SBG_ESPILL: return "product spilled past its top limb";
         case SBG_EADMIT: return "request rejected by admission control";
         case SBG_ENODEV: return "no CUDA device";
+        case SBG_ECANCELED: return "request cancelled before it was launched";
         default: return "unknown status";
     }
 }
@@ -442,6 +468,7 @@ void sbg_ctx_destroy(sbg_ctx* c) {
     cudaFree(c->pw);
     cudaFree(c->dscr);
     cudaFree(c->derr);
+    cudaFree(c->u52buf);
     c->ring.release();
     for (int k = 0; k < SBG_AUX_STREAMS; ++k) {
         if (c->aux[k]) cudaStreamDestroy(c->aux[k]);
@@ -523,6 +550,7 @@ int sbg_mul(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an, const uint
     if (!c || !rp || !ap || !bp || an <= 0 || bn <= 0) return SBG_EINVAL;
     if (an + bn - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
     CK(cudaSetDevice(c->device));
+    if (an + bn <= SBG_SCHOOL_MAX) return run_school(c, rp, ap, an, bp, bn);
     int lgL = conv_lg(an + bn - 1, c->len3_mask);
     return run_conv(c, rp, ap, an, bp, bn, 0, lgL, 0, an + bn - 2, 0, an + bn);
 }
@@ -531,6 +559,7 @@ int sbg_sqr(sbg_ctx* c, uint64_t* rp, const uint64_t* ap, int64_t an) {
     if (!c || !rp || !ap || an <= 0) return SBG_EINVAL;
     if (2 * an - 1 > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
     CK(cudaSetDevice(c->device));
+    if (2 * an <= SBG_SCHOOL_MAX) return run_school(c, rp, ap, an, ap, an);
     int lgL = conv_lg(2 * an - 1, c->len3_mask);
     return run_conv(c, rp, ap, an, ap, an, 1, lgL, 0, 2 * an - 2, 0, 2 * an);
 }
@@ -838,3 +867,8 @@ int sbg_nt_sqr(uint64_t* rp, const uint64_t* ap, ptrdiff_t an) {
 }
 
 }  // extern "C"
+
+// ---- test hooks ---------------------------------------------------------------
+extern "C" int sbg_debug_inject(uint32_t mask) { return cuda_fail(set_inject(mask), "inject"); }
+
+extern "C" void sbg_debug_fail_allocs(int n) { g_fail_allocs.store(n < 0 ? 0 : n); }

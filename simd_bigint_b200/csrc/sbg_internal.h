@@ -23,6 +23,11 @@ namespace sbg {
 // (at k = 20 the columns of 768 rows need the cross-CTA radix-3 exchange,
 // which costs more than the quarter of the points it saves)
 #define SBG_LEN3_DEFAULT 0x00EF0000u
+// Plain products of at most SBG_SCHOOL_MAX limbs (an + bn) run as one
+// schoolbook warp each (sbg_school.cu); in the batch engine they form the
+// length class SBG_CODE_SCHOOL (no transform, no workspace).
+#define SBG_SCHOOL_MAX 128
+#define SBG_CODE_SCHOOL 1
 inline bool code_three(int c) { return c >= SBG_CODE3; }
 inline int code_lg(int c) { return c >= SBG_CODE3 ? c - SBG_CODE3 : c; }
 inline int64_t code_len(int c) { return (int64_t)(c >= SBG_CODE3 ? 3 : 1) << code_lg(c); }
@@ -133,6 +138,11 @@ ShoupPair host_scale(int64_t L, int q);
 
 // ---- launchers (sbg_kernels.cu) ----
 cudaError_t upload_constants(cudaStream_t st);
+// test hooks of the CRT kernel on the current device (SBG_INJECT_* bits)
+cudaError_t set_inject(uint32_t mask);
+// device allocation of the context's workspace and plan tables; fails on
+// purpose while sbg_debug_fail_allocs has failures pending
+cudaError_t dev_alloc(void** p, size_t bytes);
 cudaError_t set_kernel_attributes();
 size_t master_table_entries();
 cudaError_t gen_master_tables(uint2* tw_f, uint2* tw_i, cudaStream_t st);
@@ -152,6 +162,17 @@ cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int6
                              uint32_t* flags, uint32_t* err, cudaStream_t st,
                              KTimer* kt = nullptr);
 size_t carry_flag_words(int64_t nout);
+// schoolbook products (sbg_school.cu): one, or one warp per job of a list
+// (plain products: cmin = off = 0, nout = an + bn <= SBG_SCHOOL_MAX)
+cudaError_t launch_school(const uint64_t* a, int64_t an, const uint64_t* b, int64_t bn,
+                          uint64_t* out, cudaStream_t st);
+cudaError_t launch_school_batch(const JobDesc* djobs, int njobs, cudaStream_t st);
+// u52 boundary (sbg_u52.cu): digits <- limbs; limbs <- redundant digits
+// (scratch: u52_encode_scratch_words(rn) u32)
+cudaError_t launch_u52_decode(uint64_t* d, int64_t n52, const uint64_t* a, int64_t an, cudaStream_t st);
+size_t u52_encode_scratch_words(int64_t rn);
+cudaError_t launch_u52_encode(uint64_t* r, int64_t rn, const uint64_t* d, int64_t n52, int sgn,
+                              uint32_t* scratch, cudaStream_t st);
 int64_t crt_blocks(int64_t nout);
 // All stages of one size class of the batch engine (every job of length
 // 2^lgL); `flags` holds flag_words zero-initialised words, job regions inside.
@@ -246,7 +267,9 @@ struct UploadRing {
 
 // kernel launches of one product (or one length class of a batch): the
 // fused single-CTA transform or the three four-step transforms, then CRT+carry
-inline int class_launches(int lgL) { return lgL <= SBG_SMALL_MAX_LG ? 2 : 4; }
+inline int class_launches(int lgL) {
+    return lgL == SBG_CODE_SCHOOL ? 1 : (lgL <= SBG_SMALL_MAX_LG ? 2 : 4);
+}
 // codes in the order batches launch them: longest transforms first
 inline int64_t code_order_key(int c) { return code_len(c); }
 
@@ -276,6 +299,9 @@ struct sbg_ctx {
     cudaStream_t aux[SBG_AUX_STREAMS] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[SBG_AUX_STREAMS] = {};
+    // u52 boundary scratch (grow-only): packed operands, product, scan words
+    uint64_t* u52buf = nullptr;
+    size_t u52cap = 0;
     // division scratch (grow-only) and its error word
     uint64_t* dscr = nullptr;
     size_t dscr_cap = 0;

@@ -1170,6 +1170,12 @@ __global__ void __launch_bounds__(256, ROW_MINB) k_row12_b(const JobDesc* __rest
 #endif
 #define CRT_BLK ((CRT_T / 32) * CRT_SEG)        // limbs per block
 #define LB_SPIN_LIMIT (1 << 22)
+#define LB_SPIN_LIMIT_TEST (1 << 12)
+
+// Test hooks for the error paths (sbg_debug_inject, 0 = off): they change
+// data or withhold a flag, never an address, so an injected failure shows as
+// an error status and never as a fault or an unbounded wait.
+__device__ uint32_t g_inject;
 #define FLAG_AGG 1u
 #define FLAG_INC 2u
 
@@ -1255,6 +1261,14 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int src1 = (lane + 31) & 31;
     const int64_t seg = (int64_t)bid * CRT_BLK + (int64_t)wid * CRT_SEG;
+    const uint32_t inj = *(volatile uint32_t*)&g_inject;
+    // injected residue corruption: the top coefficient (the product then
+    // spills) or a middle one (a wrong product no device check sees)
+    auto corrupt = [&](int64_t j, uint32_t& r0) {
+        if (((inj & SBG_INJECT_TOP) && j == cmax) ||
+            ((inj & SBG_INJECT_MID) && j == cmin + (cmax - cmin) / 2))
+            r0 ^= 1u;
+    };
     ulonglong2* zs = s_z + wid * (CRT_SEG / 2);         // unit (2 s + half) * 32 + lane
     // residues of the coefficients j = m + off of limbs m .. m+3; zero outside
     // [cmin, cmax], which Garner maps to lo = mid = hi = 0
@@ -1292,6 +1306,7 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
             const bool in = j >= cmin && j <= cmax;
 #pragma unroll
             for (int q = 0; q < SBG_NP; ++q) r[q] = in ? __ldg(&R[(size_t)q * L + j]) : 0u;
+            if (inj && in) corrupt(j, r[0]);
             garner(r, lo, mid, hi);
         }
         uint64_t y;
@@ -1315,6 +1330,11 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
         const int64_t m0 = seg + 128 * s + 4 * lane;
         uint32_t r[CRT_V][SBG_NP];
         fetch4(m0, r);
+        if (inj) {
+#pragma unroll
+            for (int k = 0; k < CRT_V; ++k)
+                if (m0 + off + k >= cmin && m0 + off + k <= cmax) corrupt(m0 + off + k, r[k][0]);
+        }
         // top coefficients first: the lane above needs them
         uint64_t lo3, mid3, lo2, mid2;
         uint32_t hi3, hi2;
@@ -1401,10 +1421,11 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
                 uint32_t gacc = 0, pacc = 1;
                 int64_t jb = (int64_t)bid - 1;
                 int spins = 0;
+                const int limit = (inj & SBG_INJECT_WITHHOLD) ? LB_SPIN_LIMIT_TEST : LB_SPIN_LIMIT;
                 while (true) {
                     uint32_t f = vf[jb];
                     if (f == 0) {
-                        if (++spins > LB_SPIN_LIMIT) {
+                        if (++spins > limit) {
                             atomicOr(err, 1u);
                             cin = 0;
                             break;
@@ -1434,7 +1455,8 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
             }
             uint32_t cout = (agg & 1u) | (((agg >> 1) & 1u) & cin);
             __threadfence();
-            atomicExch(&flags[1 + bid], FLAG_INC | (cout << 2));
+            if (!((inj & SBG_INJECT_WITHHOLD) && bid == 0))     // injected: block 0 stays silent
+                atomicExch(&flags[1 + bid], FLAG_INC | (cout << 2));
             s_cin = cin;
         }
     }
@@ -1552,6 +1574,8 @@ static cudaError_t col3_attr() {
     return e;
 }
 
+cudaError_t set_inject(uint32_t mask) { return cudaMemcpyToSymbol(g_inject, &mask, sizeof(mask)); }
+
 cudaError_t set_kernel_attributes() {
     const int big = 200 * 1024;
     cudaError_t e = cudaSuccess;
@@ -1633,6 +1657,7 @@ cudaError_t gen_len_tables(LenPlan* lp, cudaStream_t st) {
 }
 
 size_t ws_words(int lgL, int sq) {
+    if (lgL == SBG_CODE_SCHOOL) return 0;
     size_t L = (size_t)code_len(lgL);
     return (sq ? 1 : 2) * SBG_NP * L;
 }
@@ -1784,6 +1809,12 @@ cudaError_t launch_batch_class(const JobDesc* djobs, int njobs, int lgL, const L
                                uint32_t* flags, size_t flag_words, uint32_t* err,
                                cudaStream_t st, KTimer* kt) {
     if (njobs <= 0) return cudaSuccess;
+    if (lgL == SBG_CODE_SCHOOL) {
+        KT_BEGIN(kt, KID_BATCH, st);
+        cudaError_t e = launch_school_batch(djobs, njobs, st);
+        KT_END(kt, KID_BATCH, st);
+        return e;
+    }
     ScaleArg sc;
     for (int q = 0; q < SBG_NP; ++q) {
         sc.w[q] = lp->scale[q].w;

@@ -496,7 +496,7 @@ static int prepare(sbg_server* s, const sbg_request* req, SReq& q) {
         if (req->kind == SBG_REQ_MUL && (!req->bp || req->bn <= 0)) return SBG_EINVAL;
         int64_t need = req->kind == SBG_REQ_SQR ? 2 * req->an - 1 : req->an + req->bn - 1;
         if (need > ((int64_t)1 << SBG_MAX_LG)) return SBG_EBAND;
-        q.lgL = conv_lg(need, s->ctx->len3_mask);
+        q.lgL = need + 1 <= SBG_SCHOOL_MAX ? SBG_CODE_SCHOOL : conv_lg(need, s->ctx->len3_mask);
         q.sq = req->kind == SBG_REQ_SQR;
         q.cmin = 0;
         q.cmax = need - 1;
@@ -585,6 +585,32 @@ extern "C" int sbg_server_release(sbg_server* s, uint64_t ticket) {
     s->results.erase(it);
     s->cv_work.notify_all();
     return SBG_OK;
+}
+
+extern "C" int sbg_server_cancel(sbg_server* s, uint64_t ticket) {
+    if (!s) return SBG_EINVAL;
+    std::lock_guard<std::mutex> g(s->mu);
+    for (std::deque<SReq>* fifo : {&s->pending_small, &s->pending_mul, &s->pending_recip}) {
+        for (auto it = fifo->begin(); it != fifo->end(); ++it) {
+            if (it->ticket != ticket) continue;
+            // still queued: it holds no arena block yet, so it completes
+            // without touching the allocators
+            sbg_completion c{};
+            c.ticket = ticket;
+            c.status = SBG_ECANCELED;
+            c.rp = nullptr;
+            c.rn = 0;
+            const double t = now_s();
+            c.latency_s = t - it->t_arrive;
+            c.queue_s = c.latency_s;
+            fifo->erase(it);
+            s->done.push_back(c);
+            s->n_done++;
+            s->cv_done.notify_all();
+            return SBG_OK;
+        }
+    }
+    return SBG_EINVAL;          // unknown, already launched, or already complete
 }
 
 extern "C" int64_t sbg_server_launches(sbg_server* s) {

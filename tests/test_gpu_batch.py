@@ -124,3 +124,28 @@ def test_mul_batch_convenience_and_errors(ctx):
     bad[0].kind, bad[0].rp, bad[0].ap, bad[0].bp, bad[0].an, bad[0].bn = (
         sbg.JOB_MULMID, t.data_ptr(), t.data_ptr(), t.data_ptr(), 3, 5)
     assert sbg.lib().sbg_mul_batch(ctx.handle, C.cast(bad, C.c_void_p), 1) == 1
+
+
+def test_batch_of_small_products_vs_schoolbook(ctx):
+    """The schoolbook class of the batch engine (an + bn <= 128: one warp per
+    product) beside transform classes, checked against the u128 schoolbook."""
+    import simd_bigint_b200 as sbg
+    rng = np.random.default_rng(304)
+    shapes = []
+    for i in range(300):
+        tot = int(rng.integers(2, 140))
+        an = int(rng.integers(1, tot))
+        kind = sbg.JOB_SQR if i % 5 == 0 else sbg.JOB_MUL
+        shapes.append((kind, an, tot - an, "ones" if i % 4 == 0 else "rand"))
+    shapes += [(sbg.JOB_MUL, 5000, 4000, "rand"), (sbg.JOB_MUL, 64, 64, "ones")]
+    jobs, keep = _mixed_jobs(rng, shapes)
+    b = sbg.Batch(ctx, jobs)
+    b.capture()
+    for _ in range(2):
+        b.run()
+        ctx.sync()
+        for (kind, a, bb, ta, tb, tr), (_, _, _, _, an, bn) in zip(keep, jobs):
+            got = tr.cpu().numpy().view(np.uint64)
+            want = O.school_mul(a, a if kind == sbg.JOB_SQR else bb)
+            assert np.array_equal(got, want), (kind, an, bn)
+    b.close()

@@ -216,3 +216,20 @@ def test_cluster_lengths_random_spot_check(ctx, an, bn):
     r = gpu_mul(a, b)
     assert spot_check(a, b, r)
     assert np.array_equal(gpu_mul(b, a), r)
+
+
+def test_school_band_edges_vs_u128_schoolbook(ctx):
+    """Products of at most 128 limbs run as one schoolbook warp: every split
+    of the totals at the band's top, and the all-0xFF carry worst case."""
+    rng = np.random.default_rng(110)
+    for tot in (2, 31, 32, 33, 63, 64, 65, 95, 96, 97, 126, 127, 128, 129, 130):
+        for an in sorted({1, 2, tot // 3, tot // 2, tot - 2, tot - 1}):
+            bn = tot - an
+            if an < 1 or bn < 1:
+                continue
+            for pat in ("rand", "ones"):
+                a, b = O.pattern(an, pat, rng), O.pattern(bn, pat, rng)
+                assert np.array_equal(gpu_mul(a, b), O.school_mul(a, b)), (an, bn, pat)
+    for an in (1, 17, 32, 63, 64, 65):
+        a = O.pattern(an, "ones")
+        assert np.array_equal(gpu_sqr(a), O.school_mul(a, a)), an

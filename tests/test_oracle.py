@@ -97,3 +97,21 @@ def test_ones_square_closed_form():
     for n in (1, 2, 3, 100):
         a = O.pattern(n, "ones")
         assert np.array_equal(O.port_sqr(a), ones_square(n))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference not built / host lacks AVX-512 IFMA")
+def test_u52_restatement_matches_reference():
+    """oracle.py's u52 boundary (Python integers) against the reference's own
+    u52_from_u64 / u64_from_u52_canon / _canonneg."""
+    rng = np.random.default_rng(7)
+    for n in (1, 2, 3, 13, 64, 65, 777):
+        for pat in ("rand", "ones", "sparse"):
+            a = O.pattern(n, pat, rng)
+            assert np.array_equal(O.ref_u52_from_u64(a), O.u52_from_u64(a)), (n, pat)
+    for n52 in (1, 2, 8, 9, 17, 300, 1001):
+        for signed in (False, True):
+            d = (rng.integers(-(1 << 62), 1 << 62, n52).astype(np.int64).view(np.uint64) if signed
+                 else rng.integers(0, 2**64, n52, dtype=np.uint64))
+            d[-min(2, n52):] = rng.integers(0, 1 << 50, min(2, n52), dtype=np.uint64)
+            rn = (52 * n52 + 63) // 64 + 1
+            assert np.array_equal(O.ref_u64_from_u52(d, rn, signed), O.u64_from_u52(d, rn, signed))
