@@ -569,15 +569,35 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
     if pg is not None:
         pg.barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    l0 = ctx.launches()
-    e0.record(stream)
-    for _ in range(args.steps):
-        batch.run()
-    e1.record(stream)
-    ctx.sync()
-    batch_launches = ctx.launches() - l0
-    ms_step = barrier_max(pg, e0.elapsed_time(e1), dev) / args.steps
+
+    def timed_runs():
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.launches()
+        e0.record(stream)
+        for _ in range(args.steps):
+            batch.run()
+        e1.record(stream)
+        ctx.sync()
+        return barrier_max(pg, e0.elapsed_time(e1), dev) / args.steps, ctx.launches() - l0
+
+    ms_step, batch_launches = timed_runs()
+    # the same batch on the other engines: one launch per stage per length
+    # class (captured graph), and the queue with one CTA per item; each
+    # checked against the default engine's products
+    engines = {"persistent_queue": {"ms": round(ms_step, 4), "launches_per_step": batch_launches / args.steps}}
+    for eng, name in ((1, "per_class_graph"), (2, "queue_one_cta_per_item")):
+        batch.set_engine(eng)
+        batch.capture()
+        d_out.fill_(-1)
+        for _ in range(args.warmup):
+            batch.run()
+        ctx.sync()
+        same = bool(np.array_equal(d_out.cpu().numpy().view(np.uint64), got))
+        exact = exact and same
+        ms_e, l_e = timed_runs()
+        engines[name] = {"ms": round(ms_e, 4), "launches_per_step": l_e / args.steps, "same_products": same}
+    batch.set_engine(0)
+    batch.capture()
     # one multiply per launch over the same batch
     L = sbg.lib()
     h = ctx.handle
@@ -660,6 +680,10 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
         "bit_exact": bool(exact),
         "one_per_launch": {"value": round(single, 2), "unit": "Mlimb/s", "ms": round(ms_single, 3),
                            "ratio_batched_vs_single": round(value / ws / single, 2)},
+        "engine": "persistent kernel over a device work-item queue (one launch per batch)",
+        "engines": {k: {**v, "value": round(total / (v["ms"] * 1e-3) / 1e6, 2), "unit": "Mlimb/s",
+                        "ratio_vs_one_per_launch": round(total / (v["ms"] * 1e-3) / 1e6 / single, 2)}
+                    for k, v in engines.items()},
         "e2e": {"value": round(total * ws * args.steps / e2e_s / 1e6, 2), "unit": "Mlimb/s",
                 "h2d_bytes_per_step": int(host_in.nbytes), "d2h_bytes_per_step": int(nr * 8),
                 "entry": "sbg_batch_run (captured graph) between pinned host copies; two buffer sets "
@@ -1365,7 +1389,8 @@ def run_extras(args, ws, rank, local, pg) -> dict:
             "one_per_launch": b["one_per_launch"], "bit_exact": b["bit_exact"],
             "e2e": {"value": b["e2e"]["value"], "unit": b["e2e"]["unit"]},
             "gpu_launches_per_step": round(b["gpu_launches"] / ab.steps, 1),
-            "engine": b.get("engine"), "config": b["config"]["workload"], "steps": ab.steps}
+            "engine": b.get("engine"), "engines": b.get("engines"), "config": b["config"]["workload"],
+            "steps": ab.steps}
     asv = copy.copy(args)
     asv.requests, asv.sweep_requests, asv.serve_fracs = 20000, 6000, (0.6,)
     asv.warmup = 3

@@ -168,6 +168,17 @@ int sbg_batch_capture(sbg_batch *batch);
 int sbg_batch_run(sbg_batch *batch);
 /* Waits for queued runs, then frees. */
 void sbg_batch_destroy(sbg_batch *batch);
+/* Batch engine.  0 (default): ONE persistent kernel whose CTAs take work
+ * items -- (job, stage, tile) -- from a queue in device memory, waiting on
+ * per-job progress counters between a job's stages; it runs the schoolbook,
+ * single-CTA and power-of-two four-step classes up to 2^20 points (longer
+ * and 3 * 2^k classes keep per-class launches beside it).  1: one launch per
+ * stage per length class for every class.  2: the same queue and kernel,
+ * one CTA per item instead of persistent CTAs.  wave_bytes (0: keep the
+ * current, default 48 MB) bounds the transform workspace of the jobs whose
+ * stages the queue interleaves (L2 blocking).  Drops a captured graph:
+ * capture again.  No counterpart in the reference. */
+int sbg_batch_set_engine(sbg_batch *batch, int engine, int64_t wave_bytes);
 /* One-shot batch through the context's reusable product arena (no per-call
  * allocation once it has grown): returns when the products are written. */
 int sbg_mul_batch(sbg_ctx *ctx, const sbg_job *jobs, int64_t count);

@@ -133,6 +133,8 @@ def lib(build_if_missing: bool = False):
         L.sbg_noalloc_status.restype = C.c_int
         L.sbg_mul_noalloc.argtypes = [_vp, _vp, _i64, _vp, _i64, _vp]
         L.sbg_mul_noalloc.restype = C.c_int
+        L.sbg_batch_set_engine.argtypes = [_vp, C.c_int, _i64]
+        L.sbg_batch_set_engine.restype = C.c_int
         L.sbg_u52_from_u64.argtypes = [_vp, _vp, _i64, _vp, _i64]
         L.sbg_u52_from_u64.restype = C.c_int
         L.sbg_u64_from_u52.argtypes = [_vp, _vp, _i64, _vp, _i64, C.c_int]
@@ -368,6 +370,13 @@ class Batch:
 
     def capture(self):
         _check(self._L.sbg_batch_capture(self.handle), "sbg_batch_capture")
+
+    def set_engine(self, engine: int, wave_bytes: int = 0):
+        """0: the persistent kernel over a device work-item queue (default),
+        1: one launch per stage per length class, 2: the queue with one CTA
+        per item.  wave_bytes: the queue's L2 blocking (0: keep).  Drops a
+        captured graph (capture again)."""
+        _check(self._L.sbg_batch_set_engine(self.handle, engine, wave_bytes), "sbg_batch_set_engine")
 
     def run(self):
         _check(self._L.sbg_batch_run(self.handle), "sbg_batch_run")

@@ -183,7 +183,24 @@ struct sbg_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int64_t count = 0;
+    // engine: 0 = the persistent kernel over a work-item queue for the
+    // classes it runs (the others keep per-class launches), 1 = per-class
+    // launches for every class, 2 = the same queue with one CTA per item
+    int engine = 0;
+    std::vector<JobDesc> host_jobs;      // descriptors, in device order
+    std::vector<int> job_code;           // length code of each
+    JobDesc* djobs_all = nullptr;
+    void* pmem = nullptr;                // items, progress state, class table
+    PItem* d_items = nullptr;
+    int nitems = 0;
+    uint32_t* d_state = nullptr;         // queue head + one progress counter per job
+    size_t state_words = 0;
+    PClass* d_cls = nullptr;
+    size_t wave_bytes = (size_t)48 << 20;
+    int grid = 0;
 };
+
+static bool batch_uses_persist(const sbg_batch* b) { return b->engine != 1 && b->nitems > 0; }
 
 static int job_shape(const sbg_job& j, uint32_t mask3, int* lgL, int64_t* cmin, int64_t* cmax,
                      int64_t* off, int64_t* nout, int* sq) {
@@ -220,18 +237,145 @@ static int job_shape(const sbg_job& j, uint32_t mask3, int* lgL, int64_t* cmin, 
 
 static int batch_launch(sbg_batch* b, KTimer* kt) {
     sbg_ctx* c = b->ctx;
+    const bool pers = batch_uses_persist(b);
     CK(cudaEventRecord(b->fork, c->stream));
     for (int k = 0; k < SBG_BATCH_STREAMS; ++k) CK(cudaStreamWaitEvent(b->aux[k], b->fork, 0));
+    int k = 0;
     for (size_t i = 0; i < b->classes.size(); ++i) {
         const auto& cl = b->classes[i];
-        cudaStream_t st = b->aux[i % SBG_BATCH_STREAMS];
+        if (pers && persist_code(cl.lgL)) continue;
+        cudaStream_t st = b->aux[k++ % SBG_BATCH_STREAMS];
         CK(launch_batch_class(cl.djobs, cl.njobs, cl.lgL, &c->plans[cl.lgL], c->tw_f, c->tw_i,
                               cl.max_nout, cl.flags, cl.flag_words, c->err, st, kt));
     }
-    for (int k = 0; k < SBG_BATCH_STREAMS; ++k) {
-        CK(cudaEventRecord(b->join[k], b->aux[k]));
-        CK(cudaStreamWaitEvent(c->stream, b->join[k], 0));
+    if (pers) {
+        CK(cudaMemsetAsync(b->d_state, 0, b->state_words * sizeof(uint32_t), c->stream));
+        for (const auto& cl : b->classes)
+            if (persist_code(cl.lgL) && cl.flag_words)
+                CK(cudaMemsetAsync(cl.flags, 0, cl.flag_words * sizeof(uint32_t), c->stream));
+        KT_BEGIN(kt, KID_BATCH, c->stream);
+        CK(launch_persist(b->d_items, b->nitems, b->djobs_all, b->d_cls, b->d_state, c->tw_f, c->tw_i,
+                          c->err, b->engine == 2 ? 0 : b->grid, c->stream));
+        KT_END(kt, KID_BATCH, c->stream);
     }
+    for (int j = 0; j < SBG_BATCH_STREAMS; ++j) {
+        CK(cudaEventRecord(b->join[j], b->aux[j]));
+        CK(cudaStreamWaitEvent(c->stream, b->join[j], 0));
+    }
+    return SBG_OK;
+}
+
+// kernel launches of one run of the batch
+static int64_t batch_run_launches(const sbg_batch* b) {
+    int64_t n = 0;
+    const bool pers = batch_uses_persist(b);
+    for (const auto& cl : b->classes)
+        if (!(pers && persist_code(cl.lgL))) n += class_launches(cl.lgL);
+    return n + (pers ? 1 : 0);
+}
+
+// The persistent engine's work-item queue: jobs of the classes the
+// persistent kernel runs, cut into waves of about wave_bytes of transform
+// workspace; step t of the queue holds the carry blocks of wave t - 3, the
+// inverse columns of wave t - 2, the rows of wave t - 1 and the forward
+// columns (or single-CTA transforms) of wave t, so that every item comes
+// after the items it waits for and a stage's input is recent in L2.
+static int persist_build(sbg_batch* b) {
+    sbg_ctx* c = b->ctx;
+    struct Wave {
+        std::vector<PItem> s[4];
+    };
+    std::vector<Wave> waves(1);
+    size_t acc = 0;
+    std::vector<int> order;                       // job indices, longest transforms first
+    for (size_t j = 0; j < b->host_jobs.size(); ++j)
+        if (persist_code(b->job_code[j])) order.push_back((int)j);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return code_order_key(b->job_code[x]) > code_order_key(b->job_code[y]);
+    });
+    // schoolbook jobs: groups of up to 8 consecutive descriptors, first wave
+    int sch_first = -1, sch_n = 0;
+    auto flush_school = [&]() {
+        if (sch_n)
+            waves[0].s[0].push_back(PItem{(uint32_t)sch_first, PK_SCHOOL, SBG_CODE_SCHOOL, (uint32_t)sch_n, 0});
+        sch_first = -1;
+        sch_n = 0;
+    };
+    for (int j : order) {
+        const int l = b->job_code[j];
+        const JobDesc& d = b->host_jobs[j];
+        if (l == SBG_CODE_SCHOOL) {
+            if (sch_n == PERSIST_THREADS / 32 || (sch_n && sch_first + sch_n != j)) flush_school();
+            if (!sch_n) sch_first = j;
+            ++sch_n;
+            continue;
+        }
+        const size_t wsb = ws_words(l, d.sq) * 4;
+        if (acc && acc + wsb > b->wave_bytes) {
+            waves.emplace_back();
+            acc = 0;
+        }
+        acc += wsb;
+        Wave& w = waves.back();
+        const uint32_t nb = (uint32_t)crt_blocks(d.nout);
+        const uint16_t lg = (uint16_t)l;
+        if (l <= SBG_SMALL_MAX_LG) {
+            for (uint32_t q = 0; q < SBG_NP; ++q) w.s[0].push_back(PItem{(uint32_t)j, PK_SMALL, lg, q, 0});
+            for (uint32_t k = 0; k < nb; ++k) w.s[1].push_back(PItem{(uint32_t)j, PK_CRT, lg, k, SBG_NP});
+            continue;
+        }
+        const int lgN1 = l - 12;
+        const uint32_t nt = (uint32_t)col_tiles(lgN1);
+        const uint32_t nops = d.sq ? 1 : 2;
+        const uint32_t n_colf = nops * nt * SBG_NP, n_row = (uint32_t)SBG_NP << lgN1, n_coli = nt * SBG_NP;
+        for (uint32_t i = 0; i < n_colf; ++i) w.s[0].push_back(PItem{(uint32_t)j, PK_COLF, lg, i, 0});
+        for (uint32_t i = 0; i < n_row; ++i) w.s[1].push_back(PItem{(uint32_t)j, PK_ROW, lg, i, n_colf});
+        for (uint32_t i = 0; i < n_coli; ++i) w.s[2].push_back(PItem{(uint32_t)j, PK_COLI, lg, i, n_colf + n_row});
+        for (uint32_t k = 0; k < nb; ++k)
+            w.s[3].push_back(PItem{(uint32_t)j, PK_CRT, lg, k, n_colf + n_row + n_coli});
+    }
+    flush_school();
+    std::vector<PItem> q;
+    const int nw = (int)waves.size();
+    for (int t = 0; t < nw + 3; ++t)
+        for (int st = 3; st >= 0; --st) {
+            const int w = t - st;
+            if (w >= 0 && w < nw) q.insert(q.end(), waves[w].s[st].begin(), waves[w].s[st].end());
+        }
+    // class table, items and progress state in one allocation
+    std::vector<PClass> cls(SBG_NCODES + 1);
+    for (int l = 0; l <= SBG_NCODES; ++l) {
+        const LenPlan& lp = c->plans[l];
+        if (lp.lgL != l) continue;
+        cls[l].fsf = FsTables{lp.fs_lo_f, lp.fs_hi_f, lp.hi_n};
+        cls[l].fsi = FsTables{lp.fs_lo_i, lp.fs_hi_i, lp.hi_n};
+        for (int p = 0; p < SBG_NP; ++p) {
+            cls[l].sc.w[p] = lp.scale[p].w;
+            cls[l].sc.ws[p] = lp.scale[p].ws;
+        }
+    }
+    const size_t cls_b = cls.size() * sizeof(PClass);
+    const size_t items_b = q.size() * sizeof(PItem);
+    const size_t state_w = 1 + b->host_jobs.size();
+    const size_t off_items = (cls_b + 255) & ~(size_t)255;
+    const size_t off_state = (off_items + items_b + 255) & ~(size_t)255;
+    const size_t total = off_state + state_w * sizeof(uint32_t);
+    if (b->pmem) {
+        CK(cudaStreamSynchronize(c->stream));
+        cudaFree(b->pmem);
+        b->pmem = nullptr;
+    }
+    CK(cudaMalloc(&b->pmem, total));
+    uint8_t* base = (uint8_t*)b->pmem;
+    b->d_cls = (PClass*)base;
+    b->d_items = (PItem*)(base + off_items);
+    b->d_state = (uint32_t*)(base + off_state);
+    b->state_words = state_w;
+    b->nitems = (int)q.size();
+    CK(cudaMemcpy(b->d_cls, cls.data(), cls_b, cudaMemcpyHostToDevice));
+    if (items_b) CK(cudaMemcpy(b->d_items, q.data(), items_b, cudaMemcpyHostToDevice));
+    b->grid = persist_grid(c->device);
+    if (b->grid <= 0) return SBG_ECUDA;
     return SBG_OK;
 }
 
@@ -581,6 +725,7 @@ void sbg_batch_destroy(sbg_batch* b) {
     }
     if (b->fork) cudaEventDestroy(b->fork);
     cudaFree(b->dmem);
+    cudaFree(b->pmem);
     delete b;
 }
 
@@ -652,6 +797,10 @@ int sbg_batch_create(sbg_ctx* c, const sbg_job* jobs, int64_t count, sbg_batch**
         }
         b->classes.push_back(cl);
     }
+    b->host_jobs = host_all;
+    b->djobs_all = dd;
+    for (int l = 0; l <= SBG_NCODES; ++l)
+        for (size_t k = 0; k < by_lg[l].size(); ++k) b->job_code.push_back(l);
     // largest classes first: they start early on the forked streams
     std::stable_sort(b->classes.begin(), b->classes.end(),
                      [](const sbg_batch::Cls& x, const sbg_batch::Cls& y) {
@@ -666,6 +815,7 @@ int sbg_batch_create(sbg_ctx* c, const sbg_job* jobs, int64_t count, sbg_batch**
             if (!st) st = cuda_fail(cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming), "ev");
         }
         if (!st) st = cuda_fail(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "ev");
+        if (!st) st = persist_build(b);
         if (!st) st = cuda_fail(cudaStreamSynchronize(c->stream), "sync");
     } while (0);
     if (st) {
@@ -699,12 +849,30 @@ int sbg_batch_run(sbg_batch* b) {
     if (!b) return SBG_EINVAL;
     sbg_ctx* c = b->ctx;
     CK(cudaSetDevice(c->device));
-    for (const auto& cl : b->classes) c->launches += class_launches(cl.lgL);
+    c->launches += batch_run_launches(b);
     if (b->exec) {
         CK(cudaGraphLaunch(b->exec, c->stream));
         return SBG_OK;
     }
     return batch_launch(b, c->timer);
+}
+
+int sbg_batch_set_engine(sbg_batch* b, int engine, int64_t wave_bytes) {
+    if (!b || engine < 0 || engine > 2 || wave_bytes < 0) return SBG_EINVAL;
+    CK(cudaSetDevice(b->ctx->device));
+    const bool rebuild = wave_bytes > 0 && (size_t)wave_bytes != b->wave_bytes;
+    if (engine == b->engine && !rebuild) return SBG_OK;
+    CK(cudaStreamSynchronize(b->ctx->stream));
+    if (b->exec) cudaGraphExecDestroy(b->exec);    // the next capture records the new engine
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->engine = engine;
+    if (rebuild) {
+        b->wave_bytes = (size_t)wave_bytes;
+        return persist_build(b);
+    }
+    return SBG_OK;
 }
 
 int64_t sbg_ctx_launches(sbg_ctx* c) { return c ? c->launches.load() + c->ring.pulls : 0; }

@@ -102,6 +102,30 @@ struct JobDesc {
     int32_t pad;
 };
 
+// ---- the persistent batch engine ----
+// One work item of the persistent batch kernel: a stage of one job (or a
+// group of up to 8 schoolbook jobs).  `need` is the value the job's progress
+// counter must reach before the item may start (its earlier stages done).
+enum PKind : uint16_t { PK_SCHOOL = 0, PK_SMALL = 1, PK_COLF = 2, PK_ROW = 3, PK_COLI = 4, PK_CRT = 5 };
+struct PItem {
+    uint32_t job;           // index into the batch's JobDesc array (first job of a group)
+    uint16_t kind;          // PKind
+    uint16_t lg;            // the job's length code
+    uint32_t idx;           // index within the stage (prime, tile, row, carry block; group size)
+    uint32_t need;          // progress-counter value required before starting
+};
+// per length code: four-step twiddle tables and the CRT scale
+struct PClass {
+    FsTables fsf, fsi;
+    ScaleArg sc;
+};
+// length codes the persistent kernel runs: schoolbook, single-CTA, and
+// power-of-two four-step lengths with columns of at most 2^8 rows
+inline bool persist_code(int c) {
+    return c == SBG_CODE_SCHOOL || (c >= 4 && c <= 12) || (c >= 13 && c <= 20);
+}
+#define PERSIST_THREADS 256
+
 // Kernel ids for the optional per-launch event timing (sbg_ctx_kernel_times).
 enum KernelId {
     KID_SMALL = 0,
@@ -167,6 +191,16 @@ size_t carry_flag_words(int64_t nout);
 cudaError_t launch_school(const uint64_t* a, int64_t an, const uint64_t* b, int64_t bn,
                           uint64_t* out, cudaStream_t st);
 cudaError_t launch_school_batch(const JobDesc* djobs, int njobs, cudaStream_t st);
+// the persistent batch kernel over a work-item queue (sbg_kernels.cu); state
+// = {queue head, one progress counter per job}, zeroed before every run;
+// grid > 0: that many persistent CTAs, grid = 0: one CTA per item
+cudaError_t launch_persist(const PItem* items, int nitems, const JobDesc* jobs, const PClass* cls,
+                           uint32_t* state, const uint2* tw_f, const uint2* tw_i, uint32_t* err,
+                           int grid, cudaStream_t st);
+int persist_grid(int device);
+size_t persist_smem_bytes();
+// column tiles of a power-of-two four-step transform with 2^lgN1 rows
+int col_tiles(int lgN1);
 // u52 boundary (sbg_u52.cu): digits <- limbs; limbs <- redundant digits
 // (scratch: u52_encode_scratch_words(rn) u32)
 cudaError_t launch_u52_decode(uint64_t* d, int64_t n52, const uint64_t* a, int64_t an, cudaStream_t st);

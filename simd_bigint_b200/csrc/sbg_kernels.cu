@@ -16,6 +16,8 @@
 // reads and writes each spectrum once, all levels inside a pass stay on chip.
 #include <cooperative_groups.h>
 
+#include <algorithm>
+
 #include "sbg_internal.h"
 #include "sbg_ntt.cuh"
 
@@ -988,15 +990,25 @@ __global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3_inv_b(const JobD
 #ifndef ROW_MINB
 #define ROW_MINB 4                // resident CTAs per SM the register budget is set for
 #endif
+// shared memory of one row: both operands' planes and the 16 four-step
+// twiddle steps of each direction
+struct RowSmem {
+    uint32_t A[padded_len(ROW_N)];
+    uint32_t B[padded_len(ROW_N)];
+    uint2 f[16];
+    uint2 i[16];
+};
+
+// (scw, scws): the CRT scale of prime q and its Shoup companion
 __device__ __forceinline__ void row_body(int q, int row, uint32_t* __restrict__ YA,
                                          const uint32_t* __restrict__ YB, int sq, int lgN1, int m3,
                                          const FsTables& fsf, const FsTables& fsi,
-                                         const ScaleArg& sc, const uint2* __restrict__ twf,
-                                         const uint2* __restrict__ twi) {
-    __shared__ uint32_t smA[padded_len(ROW_N)];
-    __shared__ uint32_t smB[padded_len(ROW_N)];
-    __shared__ uint2 s_f[16];
-    __shared__ uint2 s_i[16];
+                                         uint32_t scw, uint32_t scws, const uint2* __restrict__ twf,
+                                         const uint2* __restrict__ twi, RowSmem& S) {
+    uint32_t* smA = S.A;
+    uint32_t* smB = S.B;
+    uint2* s_f = S.f;
+    uint2* s_i = S.i;
     const int tid = threadIdx.x;
     const PrimeConst pc = c_pr[q];
     const uint32_t p = pc.p;
@@ -1013,7 +1025,7 @@ __device__ __forceinline__ void row_body(int q, int row, uint32_t* __restrict__ 
         uint32_t e = k1 * 256u * (uint32_t)tid;          // < L: no reduction
         uint32_t v = fs_value(fsf, q, e, p);
         s_f[tid] = make_uint2(v, shoup_fast(v, pc));
-        uint32_t vi = mul_shoup(fs_value(fsi, q, e, p), sc.w[q], sc.ws[q], p);
+        uint32_t vi = mul_shoup(fs_value(fsi, q, e, p), scw, scws, p);
         s_i[tid] = make_uint2(vi, shoup_fast(vi, pc));
     }
     const uint32_t eb = k1 * (uint32_t)tid;
@@ -1115,9 +1127,10 @@ __global__ void __launch_bounds__(256, ROW_MINB) k_row12(uint32_t* __restrict__ 
                                                   int lgN1, int m3, FsTables fsf, FsTables fsi,
                                                   ScaleArg sc, const uint2* __restrict__ twf,
                                                   const uint2* __restrict__ twi) {
+    __shared__ RowSmem S;
     const int n1 = m3 >= 0 ? 3 << m3 : 1 << lgN1;
     const int q = blockIdx.x / n1;
-    row_body(q, blockIdx.x - q * n1, YA, YB, sq, lgN1, m3, fsf, fsi, sc, twf, twi);
+    row_body(q, blockIdx.x - q * n1, YA, YB, sq, lgN1, m3, fsf, fsi, sc.w[q], sc.ws[q], twf, twi, S);
 }
 
 // batched: blocks (job, prime, row), job slowest
@@ -1129,8 +1142,10 @@ __global__ void __launch_bounds__(256, ROW_MINB) k_row12_b(const JobDesc* __rest
     const int per_job = SBG_NP * n1;
     const JobDesc& J = jobs[blockIdx.x / per_job];
     const int r = blockIdx.x % per_job;
+    __shared__ RowSmem S;
     uint32_t* YB = J.ws + (size_t)SBG_NP * n1 * ROW_N;
-    row_body(r / n1, r % n1, J.ws, YB, J.sq, lgN1, m3, fsf, fsi, sc, twf, twi);
+    const int q = r / n1;
+    row_body(q, r % n1, J.ws, YB, J.sq, lgN1, m3, fsf, fsi, sc.w[q], sc.ws[q], twf, twi, S);
 }
 
 // ------------------------------------------------------------------------
@@ -1249,14 +1264,21 @@ __device__ __forceinline__ void sum3(uint64_t lo, uint64_t mid, uint32_t hi, uin
     k += y < s1;
 }
 
+struct CrtSmem {
+    ulonglong2 z[CRT_BLK / 2];                  // limbs before carries
+    uint32_t gp[CRT_T / 32][CRT_NSTEP][2];      // per warp and step: g, p
+    uint32_t warp[CRT_T / 32];
+    uint32_t cin;
+};
+
 __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restrict__ R, int64_t L,
                                          int64_t cmin, int64_t cmax, int64_t off,
                                          uint64_t* __restrict__ out, int64_t nout,
-                                         uint32_t* flags, uint32_t* err) {
-    __shared__ ulonglong2 s_z[CRT_BLK / 2];              // limbs before carries
-    __shared__ uint32_t s_gp[CRT_T / 32][CRT_NSTEP][2];  // per warp and step: g, p
-    __shared__ uint32_t s_warp[CRT_T / 32];
-    __shared__ uint32_t s_cin;
+                                         uint32_t* flags, uint32_t* err, CrtSmem& S) {
+    ulonglong2* s_z = S.z;
+    auto& s_gp = S.gp;
+    uint32_t* s_warp = S.warp;
+    uint32_t& s_cin = S.cin;
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int src1 = (lane + 31) & 31;
@@ -1277,7 +1299,7 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
         if (((j & 3) == 0) && j >= cmin && j + 3 <= cmax) {
 #pragma unroll
             for (int q = 0; q < SBG_NP; ++q) {
-                const uint4 v = __ldg(reinterpret_cast<const uint4*>(R + (size_t)q * L + j));
+                const uint4 v = __ldcg(reinterpret_cast<const uint4*>(R + (size_t)q * L + j));
                 r[0][q] = v.x;
                 r[1][q] = v.y;
                 r[2][q] = v.z;
@@ -1288,7 +1310,7 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
             for (int k = 0; k < CRT_V; ++k) {
                 const bool in = j + k >= cmin && j + k <= cmax;
 #pragma unroll
-                for (int q = 0; q < SBG_NP; ++q) r[k][q] = in ? __ldg(&R[(size_t)q * L + j + k]) : 0u;
+                for (int q = 0; q < SBG_NP; ++q) r[k][q] = in ? __ldcg(&R[(size_t)q * L + j + k]) : 0u;
             }
         }
     };
@@ -1305,7 +1327,7 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
             const int64_t j = seg - 32 + lane + off;
             const bool in = j >= cmin && j <= cmax;
 #pragma unroll
-            for (int q = 0; q < SBG_NP; ++q) r[q] = in ? __ldg(&R[(size_t)q * L + j]) : 0u;
+            for (int q = 0; q < SBG_NP; ++q) r[q] = in ? __ldcg(&R[(size_t)q * L + j]) : 0u;
             if (inj && in) corrupt(j, r[0]);
             garner(r, lo, mid, hi);
         }
@@ -1503,7 +1525,8 @@ __global__ void __launch_bounds__(CRT_T, CRT_MINB) k_crt_carry(const uint32_t* _
     __shared__ uint32_t s_bid;
     if (threadIdx.x == 0) s_bid = atomicAdd(&flags[0], 1u);
     __syncthreads();
-    crt_body(s_bid, R, L, cmin, cmax, off, out, nout, flags, err);
+    __shared__ CrtSmem S;
+    crt_body(s_bid, R, L, cmin, cmax, off, out, nout, flags, err, S);
 }
 
 // batched: blocks_per_job CTAs per job (enough for the longest output of the
@@ -1516,7 +1539,8 @@ __global__ void __launch_bounds__(CRT_T, CRT_MINB) k_crt_carry_b(const JobDesc* 
     __syncthreads();
     const int64_t need = (J.nout + 1 + CRT_BLK - 1) / CRT_BLK;
     if ((int64_t)s_bid >= need) return;
-    crt_body(s_bid, J.ws, L, J.cmin, J.cmax, J.off, J.out, J.nout, J.flags, err);
+    __shared__ CrtSmem S;
+    crt_body(s_bid, J.ws, L, J.cmin, J.cmax, J.off, J.out, J.nout, J.flags, err, S);
 }
 
 // ------------------------------------------------------------------------
@@ -1573,6 +1597,8 @@ static cudaError_t col3_attr() {
         e = cudaFuncSetAttribute(k_col3_inv_b<M3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     return e;
 }
+
+int col_tiles(int lgN1) { return col_ntiles(lgN1); }
 
 cudaError_t set_inject(uint32_t mask) { return cudaMemcpyToSymbol(g_inject, &mask, sizeof(mask)); }
 
@@ -1915,3 +1941,6 @@ cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int6
 }
 
 }  // namespace sbg
+
+#include "sbg_school.cuh"
+#include "sbg_persist.cuh"

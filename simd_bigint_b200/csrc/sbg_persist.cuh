@@ -1,0 +1,208 @@
+// sbg_persist.cuh -- the persistent batch kernel (included by sbg_kernels.cu,
+// whose transform bodies it runs).
+//
+// One launch runs a whole batch of uneven products.  Its CTAs (as many as
+// fit on the device at once) take work items from a queue in device memory,
+// one at a time, by an atomic increment of the queue head.  An item is one
+// stage of one job on one tile: the single-CTA transform of one prime
+// (small lengths), a column-forward tile, a row, a column-inverse tile, a
+// carry-scan block -- or a group of up to eight schoolbook jobs, one warp
+// each.  Every job has a progress counter that each finished item of the job
+// increments; an item carries the counter value its job's earlier stages
+// reach, and the CTA that takes it waits (bounded) until the counter gets
+// there.
+//
+// The host orders the queue so that every item comes after all the items it
+// waits for (stages in order, and a job's carry blocks in block order, which
+// the carry scan's look-back needs).  A CTA takes an item only while it is
+// resident, so every item an item waits for is already held by a running
+// CTA: the waits always end.  Each wait is bounded nevertheless; on expiry
+// the kernel sets the error word's timeout bit and goes on.
+//
+// Jobs are grouped into waves of a bounded workspace footprint (L2 blocking)
+// and the queue is software-pipelined over the waves: step t holds the
+// carry blocks of wave t - 3, the inverse columns of wave t - 2, the rows of
+// wave t - 1 and the forward columns of wave t.  A stage's input was written
+// one step earlier, so it is mostly still in L2, and the items of a step do
+// not wait on each other.
+#pragma once
+
+namespace sbg {
+
+#define PERSIST_WAIT_LIMIT (1 << 25)
+
+// Waits until the job's progress counter reaches `need`.  Bounded, and once
+// any wait of the launch has expired (the error word's timeout bit is set)
+// the others give up at once, so a fault in the queue's order costs one
+// expiry, not one per item.
+__device__ __forceinline__ void persist_wait(const uint32_t* cnt, uint32_t need, uint32_t* err) {
+    const volatile uint32_t* v = cnt;
+    const volatile uint32_t* e = err;
+    int spins = 0;
+    while (*v < need) {
+        if (++spins > PERSIST_WAIT_LIMIT || ((spins & 63) == 0 && (*e & 1u))) {
+            atomicOr(err, 1u);
+            break;
+        }
+        __nanosleep(64);
+    }
+    __threadfence();
+}
+
+template <int LGN1>
+__device__ __forceinline__ void persist_col(const PItem& I, const JobDesc& J, const uint2* __restrict__ twf,
+                                            const uint2* __restrict__ twi) {
+    constexpr int NTILES = col_ntiles(LGN1);
+    if (I.kind == PK_COLF) {
+        const int q = (int)(I.idx % SBG_NP);
+        const int r = (int)(I.idx / SBG_NP);
+        uint32_t* YB = J.ws + ((size_t)SBG_NP << (LGN1 + SBG_ROW_LG));
+        col_fwd_body<LGN1>(q, r % NTILES, 0, r / NTILES, J.a, J.an, J.b, J.bn, twf, J.ws, YB);
+    } else {
+        col_inv_body<LGN1>((int)(I.idx % SBG_NP), (int)(I.idx / SBG_NP), 0, J.ws, twi);
+    }
+}
+
+// One work item (the CTA's whole block takes part); the item's fields come
+// in as warp-uniform values.
+__device__ __forceinline__ void persist_item(uint32_t kind, uint32_t job, uint32_t lg, uint32_t idx,
+                                             const JobDesc* __restrict__ jobs, const PClass* __restrict__ cls,
+                                             const uint2* __restrict__ twf, const uint2* __restrict__ twi,
+                                             uint32_t* err, uint32_t* sm) {
+    switch (kind) {
+        case PK_SCHOOL: {
+            const int w = threadIdx.x >> 5;
+            if (w < (int)idx) {
+                const JobDesc& J = jobs[job + w];
+                uint64_t* sa = reinterpret_cast<uint64_t*>(sm) + w * (2 * SBG_SCHOOL_MAX);
+                school_warp(J.a, (int)J.an, J.b, (int)J.bn, J.out, sa, sa + SBG_SCHOOL_MAX);
+            }
+            break;
+        }
+        case PK_SMALL: {
+            const JobDesc& J = jobs[job];
+            small_body((int)idx, J.a, J.an, J.b, J.bn, J.sq, (int)lg, twf, twi, cls[lg].sc, J.ws);
+            break;
+        }
+        case PK_COLF:
+        case PK_COLI: {
+            const PItem I{job, (uint16_t)kind, (uint16_t)lg, idx, 0};
+            const JobDesc& J = jobs[job];
+            switch ((int)lg - SBG_ROW_LG) {
+                case 1: persist_col<1>(I, J, twf, twi); break;
+                case 2: persist_col<2>(I, J, twf, twi); break;
+                case 3: persist_col<3>(I, J, twf, twi); break;
+                case 4: persist_col<4>(I, J, twf, twi); break;
+                case 5: persist_col<5>(I, J, twf, twi); break;
+                case 6: persist_col<6>(I, J, twf, twi); break;
+                case 7: persist_col<7>(I, J, twf, twi); break;
+                case 8: persist_col<8>(I, J, twf, twi); break;
+                default: break;
+            }
+            break;
+        }
+        case PK_ROW: {
+            const JobDesc& J = jobs[job];
+            const int lgN1 = (int)lg - SBG_ROW_LG;
+            const PClass& C = cls[lg];
+            uint32_t* YB = J.ws + ((size_t)SBG_NP << lg);
+            const int q = (int)idx >> lgN1;
+            row_body(q, (int)idx & ((1 << lgN1) - 1), J.ws, YB, J.sq, lgN1, -1, C.fsf, C.fsi, C.sc.w[q],
+                     C.sc.ws[q], twf, twi, *reinterpret_cast<RowSmem*>(sm));
+            break;
+        }
+        case PK_CRT: {
+            const JobDesc& J = jobs[job];
+            crt_body(idx, J.ws, (int64_t)1 << lg, J.cmin, J.cmax, J.off, J.out, J.nout, J.flags, err,
+                     *reinterpret_cast<CrtSmem*>(sm));
+            break;
+        }
+        default: break;
+    }
+}
+
+// LOOP: persistent CTAs (grid = what fits on the device) take items until
+// the queue is empty; otherwise one item per CTA (grid = the item count),
+// in the same queue order.
+template <bool LOOP>
+__global__ void __launch_bounds__(PERSIST_THREADS, 4)
+    k_persist(const PItem* __restrict__ items, int nitems, const JobDesc* __restrict__ jobs,
+              const PClass* __restrict__ cls, uint32_t* state, const uint2* __restrict__ twf,
+              const uint2* __restrict__ twi, uint32_t* err) {
+    extern __shared__ uint32_t sm[];
+    // the current item, in shared memory so that nothing of it stays live in
+    // registers across the stage bodies
+    __shared__ PItem s_it;
+    __shared__ int s_more;
+    do {
+        if (threadIdx.x == 0) {
+            const int it = (int)atomicAdd(&state[0], 1u);
+            s_more = it < nitems;
+            if (it < nitems) {
+                const PItem I = items[it];
+                s_it = I;
+                if (I.need) persist_wait(&state[1 + I.job], I.need, err);
+            }
+        }
+        __syncthreads();
+        if (!s_more) return;
+        // warp-uniform copies (a warp reduction's result), so that the
+        // bodies' index arithmetic stays on the uniform datapath
+        const uint32_t kind = __reduce_max_sync(0xffffffffu, (uint32_t)s_it.kind);
+        const uint32_t job = __reduce_max_sync(0xffffffffu, s_it.job);
+        persist_item(kind, job, __reduce_max_sync(0xffffffffu, (uint32_t)s_it.lg),
+                     __reduce_max_sync(0xffffffffu, s_it.idx), jobs, cls, twf, twi, err, sm);
+        __syncthreads();
+        if (threadIdx.x == 0 && kind != PK_SCHOOL) {
+            __threadfence();
+            atomicAdd(&state[1 + job], 1u);
+        }
+    } while (LOOP);
+}
+
+size_t persist_smem_bytes() {
+    size_t b = sizeof(RowSmem);
+    b = std::max(b, sizeof(CrtSmem));
+    b = std::max(b, (size_t)2 * padded_len(1 << SBG_SMALL_MAX_LG) * 4);
+    b = std::max(b, (size_t)(PERSIST_THREADS / 32) * 2 * SBG_SCHOOL_MAX * 8);
+    b = std::max(b, (size_t)col_smem_bytes(5));
+    b = std::max(b, (size_t)col_smem_bytes(6));
+    b = std::max(b, (size_t)col_smem_bytes(7));
+    b = std::max(b, (size_t)col_smem_bytes(8));
+    return (b + 255) & ~(size_t)255;
+}
+
+int persist_grid(int device) {
+    static int cached[64] = {};
+    if (device < 0 || device >= 64) return 0;
+    if (cached[device]) return cached[device];
+    const size_t smem = persist_smem_bytes();
+    if (cudaFuncSetAttribute(k_persist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_persist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+        return 0;
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<true>, PERSIST_THREADS, smem) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return 0;
+    cached[device] = std::max(1, per_sm) * sms;
+    return cached[device];
+}
+
+cudaError_t launch_persist(const PItem* items, int nitems, const JobDesc* jobs, const PClass* cls,
+                           uint32_t* state, const uint2* tw_f, const uint2* tw_i, uint32_t* err, int grid,
+                           cudaStream_t st) {
+    if (nitems <= 0) return cudaSuccess;
+    const size_t smem = persist_smem_bytes();
+    if (grid > 0)
+        k_persist<true><<<std::min(grid, nitems), PERSIST_THREADS, smem, st>>>(items, nitems, jobs, cls, state,
+                                                                                tw_f, tw_i, err);
+    else
+        k_persist<false><<<nitems, PERSIST_THREADS, smem, st>>>(items, nitems, jobs, cls, state, tw_f, tw_i,
+                                                                 err);
+    return cudaGetLastError();
+}
+
+}  // namespace sbg

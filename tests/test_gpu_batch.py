@@ -79,12 +79,14 @@ def test_batch_matches_single_products(ctx):
     b.close()
 
 
-def test_batch_graph_replay_and_oracle(ctx):
+@pytest.mark.parametrize("engine", [0, 1, 2], ids=["persistent", "per-class", "queue-per-cta"])
+def test_batch_graph_replay_and_oracle(ctx, engine):
     import simd_bigint_b200 as sbg
     rng = np.random.default_rng(302)
     shapes = _shapes(rng, 40)
     jobs, keep = _mixed_jobs(rng, shapes)
     b = sbg.Batch(ctx, jobs)
+    b.set_engine(engine)
     b.capture()
     for rep in range(3):
         for _, _, _, _, _, tr in keep:
@@ -148,4 +150,34 @@ def test_batch_of_small_products_vs_schoolbook(ctx):
             got = tr.cpu().numpy().view(np.uint64)
             want = O.school_mul(a, a if kind == sbg.JOB_SQR else bb)
             assert np.array_equal(got, want), (kind, an, bn)
+    b.close()
+
+
+@pytest.mark.parametrize("wave_mb", [1, 48])
+def test_persistent_queue_on_a_mixed_size_batch(ctx, wave_mb):
+    """The persistent kernel (one launch, CTAs drawing (job, stage, tile)
+    items from a device queue, per-job progress counters between stages) on
+    a batch of the mixed-size configuration's shape distribution -- every
+    class it runs, squarings, all-0xFF operands -- with small waves (many
+    pipelined steps) and the default ones: every product equals the oracle's."""
+    import simd_bigint_b200 as sbg
+    from simd_bigint_b200.workloads import mixed_batch_shapes
+    rng = np.random.default_rng(305)
+    shapes = [(k, an, bn, "ones" if i % 9 == 0 else "rand")
+              for i, (k, an, bn) in enumerate(mixed_batch_shapes(160, seed=99, lo=8, hi=70000))]
+    shapes += [(sbg.JOB_MUL, 3, 5, "rand"), (sbg.JOB_SQR, 40, 40, "ones"), (sbg.JOB_MUL, 1000, 1, "rand"),
+               (sbg.JOB_MUL, 300000, 200000, "rand")]       # the last one beyond the queue's classes
+    jobs, keep = _mixed_jobs(rng, shapes)
+    b = sbg.Batch(ctx, jobs)
+    b.set_engine(0, wave_mb << 20)
+    b.capture()
+    for rep in range(2):
+        for *_, tr in keep:
+            tr.fill_(-1)
+        b.run()
+        ctx.sync()
+        for (kind, a, bb, ta, tb, tr), (_, _, _, _, an, bn) in zip(keep, jobs):
+            got = tr.cpu().numpy().view(np.uint64)
+            want = O.port_sqr(a) if kind == sbg.JOB_SQR else O.port_mul(a, bb)
+            assert np.array_equal(got, want), (rep, kind, an, bn)
     b.close()
