@@ -13,8 +13,9 @@
 //     U   = T_m * X_h
 //     X   = X_h * B^l + floor(U / B^(2h-l))
 // which keeps D X < B^2n <= D (X + 2) at every level.  The base case (at
-// most SBG_DIV_BASE limbs) is an exact long division, one thread per
-// divisor.  Every product runs on the batch engine, so all divisions of a
+// most SBG_DIV_BASE limbs) is an exact long division, one warp per divisor
+// (block division with 3-by-2 quotient estimates; divisions whose divisor is
+// that short skip the Newton path altogether).  Every product runs on the batch engine, so all divisions of a
 // batch advance one recursion level per round.
 //
 // Division of a 2n-limb N by D: Q0 = N_hi + floor(N_hi * (X - B^n) / B^n)
@@ -344,56 +345,254 @@ struct DivFix {
     int64_t n;
 };
 
-// exact base case: X = floor((B^2m - 1) / A), m+1 limbs (top limb 1), for
-// m <= SBG_DIV_BASE; one thread per divisor, schoolbook long division
-// (Knuth D with a 128/64 trial quotient).
-#define SBG_DIV_BASE 32
-__global__ void k_recip_base(const uint64_t* const* A, const int64_t* m, uint64_t* const* X,
-                             int count, uint32_t* err) {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= count) return;
-    const int64_t n = m[idx];
-    const uint64_t* d = A[idx];
-    uint64_t u[2 * SBG_DIV_BASE + 1];
-    for (int64_t i = 0; i < 2 * n; ++i) u[i] = ~0ull;
-    u[2 * n] = 0;
-    uint64_t* q = X[idx];
-    const uint64_t dh = d[n - 1], dl = n >= 2 ? d[n - 2] : 0;
-    for (int64_t j = n; j >= 0; --j) {
-        // trial quotient from the top two limbs of the remainder
-        const unsigned __int128 num = ((unsigned __int128)u[j + n] << 64) | u[j + n - 1];
-        unsigned __int128 qh = num / dh, rh = num % dh;
-        const uint64_t u2 = (j + n - 2 >= 0) ? u[j + n - 2] : 0;
-        while ((qh >> 64) || (n >= 2 && (unsigned __int128)(uint64_t)qh * dl > ((rh << 64) | u2))) {
-            qh -= 1;
-            rh += dh;
-            if (rh >> 64) break;
+// ---- block division for small divisors -----------------------------------
+// Schoolbook division of an nn-limb N by a normalised m-limb D (m <= 127),
+// one warp per division: the reference's block division (divrem_core,
+// include/divrem.h:117-160, with its 3-by-2 reciprocal seed) restated for a
+// warp.  Each quotient limb is estimated from the remainder's top three limbs
+// and the divisor's top two by the 3-by-2 division of Moeller and Granlund
+// ("Improved division by invariant integers", IEEE Trans. Computers 60(2),
+// 2011: Algorithm 5 div3by2 with the reciprocal of Algorithm 6); the estimate
+// is exact or one too large, so the multiply-subtract of q D is followed by
+// at most one add-back.  Lane l holds limbs 4l .. 4l+3 of the running
+// remainder and of D; the borrow and carry chains of a step are resolved in
+// one go from the lanes' generate / propagate ballots.
+#define SBG_DIV_BASE 127            // largest divisor of the warp division (limbs)
+
+// floor((B^3 - 1) / (d1 B + d0)) - B for d1 >= B/2 (Algorithm 6; its first
+// line, floor((B^2 - 1) / d1) - B, by a 128-by-64 division)
+__device__ __forceinline__ uint64_t recip_3by2(uint64_t d1, uint64_t d0) {
+    const unsigned __int128 num = ((unsigned __int128)(~d1) << 64) | ~0ull;
+    uint64_t v = (uint64_t)(num / d1);
+    uint64_t p = d1 * v;
+    p += d0;
+    if (p < d0) {
+        --v;
+        if (p >= d1) {
+            --v;
+            p -= d1;
         }
-        uint64_t qd = (uint64_t)qh, borrow = 0, cy = 0;
-        for (int64_t i = 0; i < n; ++i) {
-            unsigned __int128 pr = (unsigned __int128)qd * d[i] + cy;
-            cy = (uint64_t)(pr >> 64);
-            uint64_t pl = (uint64_t)pr;
-            uint64_t t = u[i + j] - pl - borrow;
-            borrow = (u[i + j] < pl) || (u[i + j] - pl < borrow);
-            u[i + j] = t;
-        }
-        uint64_t t = u[j + n] - cy - borrow;
-        bool neg = (u[j + n] < cy) || (u[j + n] - cy < borrow);
-        u[j + n] = t;
-        if (neg) {
-            qd -= 1;
-            uint64_t c = 0;
-            for (int64_t i = 0; i < n; ++i) {
-                unsigned __int128 sum = (unsigned __int128)u[i + j] + d[i] + c;
-                u[i + j] = (uint64_t)sum;
-                c = (uint64_t)(sum >> 64);
-            }
-            u[j + n] += c;
-        }
-        q[j] = qd;
+        p -= d1;
     }
-    if (q[n] != 1) atomicOr(err, 8u);
+    const unsigned __int128 t = (unsigned __int128)v * d0;
+    const uint64_t t1 = (uint64_t)(t >> 64), t0 = (uint64_t)t;
+    p += t1;
+    if (p < t1) {
+        --v;
+        if (p > d1 || (p == d1 && t0 >= d0)) --v;
+    }
+    return v;
+}
+
+// floor((u2 B^2 + u1 B + u0) / (d1 B + d0)) for (u2, u1) < (d1, d0) (Algorithm 5)
+__device__ __forceinline__ uint64_t div3by2(uint64_t u2, uint64_t u1, uint64_t u0, uint64_t d1, uint64_t d0,
+                                            uint64_t v) {
+    const unsigned __int128 qq = (unsigned __int128)v * u2 + (((unsigned __int128)u2 << 64) | u1);
+    uint64_t q1 = (uint64_t)(qq >> 64);
+    const uint64_t q0 = (uint64_t)qq;
+    uint64_t r1 = u1 - q1 * d1;
+    const unsigned __int128 t = (unsigned __int128)d0 * q1;
+    unsigned __int128 r = (((unsigned __int128)r1 << 64) | u0) - t - (((unsigned __int128)d1 << 64) | d0);
+    r1 = (uint64_t)(r >> 64);
+    q1 += 1;
+    const unsigned __int128 dd = ((unsigned __int128)d1 << 64) | d0;
+    if (r1 >= q0) {
+        q1 -= 1;
+        r += dd;
+    }
+    if (r >= dd) q1 += 1;
+    return q1;
+}
+
+#define WFULL 0xffffffffu
+
+// limb i (warp-uniform) of a warp-held array
+__device__ __forceinline__ uint64_t wget(const uint64_t (&w)[4], int i) {
+    const int k = i & 3;
+    const uint64_t x = k == 0 ? w[0] : (k == 1 ? w[1] : (k == 2 ? w[2] : w[3]));
+    return __shfl_sync(WFULL, x, i >> 2);
+}
+
+// ripple resolution of a 1-bit chain over the warp's 128 positions: per lane
+// the generate / propagate bits of its 4 limbs; returns the chain's input
+// into this lane's first limb and sets `out` to the chain's output
+__device__ __forceinline__ uint32_t warp_chain(uint32_t gb, uint32_t pb, uint32_t& out) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lG = (pb + (gb << 1)) >> 4, lP = pb == 15u;
+    const uint32_t g = __ballot_sync(WFULL, lG), p = __ballot_sync(WFULL, lP);
+    const uint64_t sum = (uint64_t)p + (g << 1);
+    out = (uint32_t)(sum >> 32) | (g >> 31);
+    return (((uint32_t)sum ^ p) >> lane) & 1u;
+}
+
+// w -= q d over the warp's limbs; true when the result is negative (borrow
+// out of the top).  Limbs above the used range are zero before and are left
+// for the caller to clear.
+__device__ __forceinline__ bool warp_submul(uint64_t (&w)[4], const uint64_t (&d)[4], uint64_t q) {
+    const int lane = threadIdx.x & 31;
+    uint64_t lo[4], hi[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        lo[k] = q * d[k];
+        hi[k] = __umul64hi(q, d[k]);
+    }
+    uint64_t hin = __shfl_up_sync(WFULL, hi[3], 1);
+    if (lane == 0) hin = 0;
+    uint64_t t[4];
+    uint32_t kb[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint64_t hp = k ? hi[k - 1] : hin;
+        const uint64_t s1 = w[k] - lo[k];
+        const uint32_t b1 = w[k] < lo[k];
+        t[k] = s1 - hp;
+        kb[k] = b1 + (s1 < hp);
+    }
+    uint32_t kin = __shfl_up_sync(WFULL, kb[3], 1);
+    if (lane == 0) kin = 0;
+    uint32_t gb = 0, pb = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t kp = k ? kb[k - 1] : kin;
+        const uint64_t z = t[k] - kp;
+        gb |= (uint32_t)(t[k] < kp) << k;
+        pb |= (uint32_t)(z == 0) << k;
+        t[k] = z;
+    }
+    uint32_t neg;
+    uint32_t r = warp_chain(gb, pb, neg);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        w[k] = t[k] - r;
+        r = ((gb >> k) & 1u) | (((pb >> k) & 1u) & r);
+    }
+    return neg != 0;
+}
+
+// w += d over the warp's limbs; the carry out of the top
+__device__ __forceinline__ bool warp_add(uint64_t (&w)[4], const uint64_t (&d)[4]) {
+    uint32_t gb = 0, pb = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint64_t s = w[k] + d[k];
+        gb |= (uint32_t)(s < w[k]) << k;
+        pb |= (uint32_t)(s == ~0ull) << k;
+        w[k] = s;
+    }
+    uint32_t cout;
+    uint32_t c = warp_chain(gb, pb, cout);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint64_t s = w[k];
+        w[k] = s + c;
+        c = ((gb >> k) & 1u) | (((pb >> k) & 1u) & c);
+    }
+    return cout != 0;
+}
+
+// zero the limbs at index > top
+__device__ __forceinline__ void warp_clip(uint64_t (&w)[4], int top) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (4 * lane + k > top) w[k] = 0;
+}
+
+// Q[0 .. nn-m] = floor(N / D), R[0 .. m) = N mod D (R may be null); numerator
+// limb i is nlimb(i) (i < nn).  D normalised, 1 <= m <= SBG_DIV_BASE, nn >= m.
+// Returns false when an estimate needed more than one add-back (cannot
+// happen for a normalised D; reported as an error).
+template <class NF>
+__device__ bool warp_divrem(const uint64_t* __restrict__ D, int m, NF nlimb, int64_t nn, uint64_t* __restrict__ Q,
+                            uint64_t* __restrict__ R) {
+    const int lane = threadIdx.x & 31;
+    uint64_t d[4], w[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int i = 4 * lane + k;
+        d[k] = i < m ? D[i] : 0ull;
+        w[k] = i < m ? nlimb(nn - m + i) : 0ull;
+    }
+    const uint64_t d1 = wget(d, m - 1), d0 = m >= 2 ? wget(d, m - 2) : 0ull;
+    const uint64_t v = recip_3by2(d1, d0);
+    bool ok = true;
+    // top quotient limb: 0 or 1 (the top m limbs of N are below 2 D)
+    {
+        uint64_t qt = 1;
+        if (warp_submul(w, d, 1)) {
+            warp_add(w, d);
+            qt = 0;
+        }
+        warp_clip(w, m);
+        if (lane == 0) Q[nn - m] = qt;
+    }
+    uint64_t nbuf = 0;
+    for (int64_t j = nn - m - 1, s = 0; j >= 0; --j, ++s) {
+        if ((s & 31) == 0) {                       // the next 32 numerator limbs, one per lane
+            const int64_t i = j - lane;
+            nbuf = i >= 0 ? nlimb(i) : 0ull;
+        }
+        // shift the remainder up one limb and bring in N[j]
+        const uint64_t inl = __shfl_sync(WFULL, nbuf, (int)(s & 31));
+        const uint64_t up = __shfl_up_sync(WFULL, w[3], 1);
+        w[3] = w[2];
+        w[2] = w[1];
+        w[1] = w[0];
+        w[0] = lane == 0 ? inl : up;
+        const uint64_t u2 = wget(w, m), u1 = wget(w, m - 1), u0 = m >= 2 ? wget(w, m - 2) : 0ull;
+        uint64_t q = (u2 == d1 && u1 == d0) ? ~0ull : div3by2(u2, u1, u0, d1, d0, v);
+        if (warp_submul(w, d, q)) {
+            q -= 1;
+            if (!warp_add(w, d)) {              // still negative: a second add-back
+                q -= 1;
+                if (!warp_add(w, d)) ok = false;
+            }
+        }
+        warp_clip(w, m);
+        if (lane == 0) Q[j] = q;
+    }
+    if (R) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = 4 * lane + k;
+            if (i < m) R[i] = w[k];
+        }
+    }
+    return ok;
+}
+
+#define WDIV_WARPS 4            // divisions (warps) per CTA
+
+// exact base case of the Newton recursion: X = floor((B^2m - 1) / A), m+1
+// limbs (top limb 1), m <= SBG_DIV_BASE; one warp per divisor
+__global__ void __launch_bounds__(32 * WDIV_WARPS) k_recip_base(const uint64_t* const* A, const int64_t* m,
+                                                              uint64_t* const* X, int count, uint32_t* err) {
+    const int idx = blockIdx.x * WDIV_WARPS + (threadIdx.x >> 5);
+    if (idx >= count) return;
+    const int n = (int)m[idx];
+    uint64_t* q = X[idx];
+    const bool ok = warp_divrem(A[idx], n, [](int64_t) { return ~0ull; }, 2 * (int64_t)n, q, nullptr);
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0 && (!ok || q[n] != 1)) atomicOr(err, 8u);
+}
+
+// a division of the batch that runs entirely as one warp
+struct WarpDiv {
+    const uint64_t* N;
+    const uint64_t* D;
+    uint64_t* Q;            // nn - dn + 1 limbs
+    uint64_t* R;            // dn limbs
+    int64_t nn;
+    int64_t dn;
+};
+
+__global__ void __launch_bounds__(32 * WDIV_WARPS) k_divrem_warp(const WarpDiv* jobs, int count, uint32_t* err) {
+    const int idx = blockIdx.x * WDIV_WARPS + (threadIdx.x >> 5);
+    if (idx >= count) return;
+    const WarpDiv J = jobs[idx];
+    const uint64_t* N = J.N;
+    const bool ok = warp_divrem(J.D, (int)J.dn, [N](int64_t i) { return N[i]; }, J.nn, J.Q, J.R);
+    if ((threadIdx.x & 31) == 0 && !ok) atomicOr(err, 8u);
 }
 
 // step 0 (wrapped first product): T = A X_h lies within 2 B^n of B^(n+h)
@@ -782,7 +981,8 @@ static int div_core(sbg_ctx* c, std::vector<DivInst>& v, uint32_t* err, bool quo
         int64_t* dm = nullptr;
         uint64_t** dX = nullptr;
         if ((rc = upload(c, A, &dA)) || (rc = upload(c, m, &dm)) || (rc = upload(c, X, &dX))) return rc;
-        k_recip_base<<<((int)v.size() + 127) / 128, 128, 0, st>>>(dA, dm, dX, (int)v.size(), err);
+        k_recip_base<<<((int)v.size() + WDIV_WARPS - 1) / WDIV_WARPS, 32 * WDIV_WARPS, 0, st>>>(
+            dA, dm, dX, (int)v.size(), err);
         c->launches += 1;
         if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
     }
@@ -981,12 +1181,32 @@ static int divrem_enqueue(sbg_ctx* c, const sbg_div_job* jobs, int64_t count, bo
     int rc = div_scratch(c, total, &scratch, !keep_err);
     if (rc) return rc;
     *queued = true;
-    std::vector<DivInst> v((size_t)count);
-    std::vector<CopyDesc> cn((size_t)count);
+    // divisors of at most SBG_DIV_BASE limbs: block division, one warp each
+    std::vector<WarpDiv> wd;
+    for (int64_t i = 0; i < count; ++i) {
+        const sbg_div_job& j = jobs[i];
+        if (j.dn <= SBG_DIV_BASE) wd.push_back(WarpDiv{j.np, j.dp, j.qp, j.rp, j.nn, j.dn});
+    }
+    if (!wd.empty()) {
+        WarpDiv* dw = nullptr;
+        if ((rc = upload(c, wd, &dw))) return rc;
+        k_divrem_warp<<<((int)wd.size() + WDIV_WARPS - 1) / WDIV_WARPS, 32 * WDIV_WARPS, 0, c->stream>>>(
+            dw, (int)wd.size(), c->derr);
+        c->launches += 1;
+        if (cudaGetLastError() != cudaSuccess) return SBG_ECUDA;
+        if ((int64_t)wd.size() == count) return SBG_OK;
+    }
+    std::vector<DivInst> v;
+    std::vector<CopyDesc> cn;
+    v.reserve((size_t)count);
+    cn.reserve((size_t)count);
     uint64_t* p = scratch;
     for (int64_t i = 0; i < count; ++i) {
         const sbg_div_job& j = jobs[i];
-        DivInst& d = v[i];
+        if (j.dn <= SBG_DIV_BASE) continue;
+        v.emplace_back();
+        cn.emplace_back();
+        DivInst& d = v.back();
         d.D = j.dp;
         d.n = j.dn;
         d.Qout = j.qp;
@@ -995,7 +1215,7 @@ static int divrem_enqueue(sbg_ctx* c, const sbg_div_job* jobs, int64_t count, bo
         // numerator zero-padded to 2n limbs (one batched copy below)
         uint64_t* Np = p;
         p += 2 * j.dn + 8;
-        cn[i] = CopyDesc{j.np, Np, j.nn, 2 * j.dn};
+        cn.back() = CopyDesc{j.np, Np, j.nn, 2 * j.dn};
         d.N = Np;
         carve(d, p);
     }

@@ -205,3 +205,52 @@ def test_async_batches_back_to_back_match_sync(ctx):
         ctx.divrem_batch(sync_jobs)
         for q, r, q2, r2 in outs:
             assert torch.equal(q, q2) and torch.equal(r, r2)
+
+
+def test_block_division_small_divisors(ctx):
+    """Divisors of at most 127 limbs run as one warp per division (block
+    division with 3-by-2 quotient estimates).  Every size 1..127, numerator
+    lengths from dn to 2 dn, random and adversarial operands: the all-ones
+    numerator, the minimal normalised divisor B^n / 2 (the largest quotient
+    limbs), all-ones divisors (the estimate's equal-top-limbs case), and
+    remainders that need the add-back."""
+    rng = np.random.default_rng(407)
+    for dn in list(range(1, 34)) + [47, 63, 64, 65, 100, 126, 127]:
+        cases = []
+        for nn in sorted({dn, dn + 1, dn + dn // 2, 2 * dn}):
+            N = rng.integers(0, 2**64, nn, dtype=np.uint64)
+            D = rng.integers(0, 2**64, dn, dtype=np.uint64)
+            D[-1] |= np.uint64(1 << 63)
+            cases.append((N, D))
+        minD = np.zeros(dn, np.uint64)
+        minD[-1] = np.uint64(1 << 63)
+        cases += [(O.pattern(2 * dn, "ones"), O.pattern(dn, "ones")), (O.pattern(2 * dn, "ones"), minD)]
+        # top limbs of the running remainder equal to the divisor's
+        D = rng.integers(0, 2**64, dn, dtype=np.uint64)
+        D[-1] |= np.uint64(1 << 63)
+        Dv = O.to_int(D)
+        cases.append((O.from_int(Dv * ((1 << (64 * dn)) - 1) + Dv - 1, 2 * dn), D))
+        for N, D in cases:
+            q, r = _divrem(ctx, N, D)
+            qq, rr = divmod(O.to_int(N), O.to_int(D))
+            assert O.to_int(q) == qq and O.to_int(r) == rr, (dn, len(N))
+
+
+def test_batch_mixing_warp_and_newton_divisions(ctx):
+    import torch
+    rng = np.random.default_rng(408)
+    ns = [1, 5, 64, 127, 128, 500, 127, 3000, 2, 129]
+    jobs, keep = [], []
+    for n in ns:
+        N = rng.integers(0, 2**64, 2 * n, dtype=np.uint64)
+        D = rng.integers(0, 2**64, n, dtype=np.uint64)
+        D[-1] |= np.uint64(1 << 63)
+        tN, tD = _dev(N), _dev(D)
+        q = torch.full((n + 1,), -1, dtype=torch.int64, device="cuda")
+        r = torch.full((n,), -1, dtype=torch.int64, device="cuda")
+        jobs.append((q.data_ptr(), r.data_ptr(), tN.data_ptr(), tD.data_ptr(), 2 * n, n))
+        keep.append((N, D, tN, tD, q, r))
+    ctx.divrem_batch(jobs)
+    for N, D, _, _, q, r in keep:
+        qq, rr = divmod(O.to_int(N), O.to_int(D))
+        assert O.to_int(_host(q)) == qq and O.to_int(_host(r)) == rr, len(D)
