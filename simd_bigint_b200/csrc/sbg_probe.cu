@@ -2,8 +2,10 @@
 //
 // The NTT kernels are bounded by integer issue, not by HBM: every radix-2
 // level costs one Gentleman-Sande butterfly per point pair (bfly_gs in
-// sbg_arith.cuh: IADD3, IADD3, IMNMX on the sum; IADD3, IMAD.HI, IMAD,
-// IMAD, IADD, IMNMX on the difference).  This probe runs that exact
+// sbg_arith.cuh: on the sum an add and a conditional subtract of p; on the
+// difference an add of p, a Shoup product -- a high multiply by the
+// companion, a low multiply by the twiddle, a multiply-subtract of the
+// quotient estimate times p -- and a conditional subtract).  This probe runs that exact
 // butterfly on registers only (16 independent chains per thread, no memory
 // traffic, 4 CTAs of 256 threads per SM) and reports butterflies per second:
 // the compute roofline the benchmark divides the kernels' butterfly rate by.
