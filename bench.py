@@ -159,7 +159,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def dist_init(backend: str | None = None):
+def dist_init(backend: str | None = None, timeout_s: float = 120.0):
     """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE).  The
     products are independent replicas: the only collective is the max over
     ranks of the timings (NCCL on GPUs; gloo where there is none)."""
@@ -174,7 +174,7 @@ def dist_init(backend: str | None = None):
         import torch.distributed as dist
         if backend is None:
             backend = "nccl" if torch.cuda.is_available() else "gloo"
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
         pg = dist
     return ws, rank, local, pg
 

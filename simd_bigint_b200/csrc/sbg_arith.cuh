@@ -96,6 +96,13 @@ __device__ __forceinline__ void bfly_gs(uint32_t& u, uint32_t& v, uint32_t w, ui
     u = red1(s, p);
     v = mul_shoup(d, w, ws, p);
 }
+// Either butterfly with the twiddle 1: (u, v) -> (u + v, u - v), no multiply.
+__device__ __forceinline__ void bfly_triv(uint32_t& u, uint32_t& v, uint32_t p) {
+    uint32_t s = u + v;
+    uint32_t d = u - v + p;                     // [1, 2p)
+    u = red1(s, p);
+    v = red1(d, p);
+}
 // Cooley-Tukey (DIT) butterfly: (u, v) -> (u + v * w, u - v * w).  Exact
 // inverse of bfly_gs with w^-1, up to the factor 2.
 __device__ __forceinline__ void bfly_ct(uint32_t& u, uint32_t& v, uint32_t w, uint32_t ws,

@@ -293,11 +293,12 @@ static int persist_build(sbg_batch* b) {
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
         return code_order_key(b->job_code[x]) > code_order_key(b->job_code[y]);
     });
-    // schoolbook jobs: groups of up to 8 consecutive descriptors, first wave
+    // items that wait for nothing -- whole single-CTA products and groups of
+    // up to 8 consecutive schoolbook products -- go to the end of the queue
+    std::vector<PItem> tail;
     int sch_first = -1, sch_n = 0;
     auto flush_school = [&]() {
-        if (sch_n)
-            waves[0].s[0].push_back(PItem{(uint32_t)sch_first, PK_SCHOOL, SBG_CODE_SCHOOL, (uint32_t)sch_n, 0});
+        if (sch_n) tail.push_back(PItem{(uint32_t)sch_first, PK_SCHOOL, SBG_CODE_SCHOOL, (uint32_t)sch_n, 0});
         sch_first = -1;
         sch_n = 0;
     };
@@ -310,6 +311,12 @@ static int persist_build(sbg_batch* b) {
             ++sch_n;
             continue;
         }
+        const uint32_t nb = (uint32_t)crt_blocks(d.nout);
+        const uint16_t lg = (uint16_t)l;
+        if (l <= SBG_SMALL_MAX_LG) {
+            tail.push_back(PItem{(uint32_t)j, PK_SMALLJOB, lg, nb, 0});
+            continue;
+        }
         const size_t wsb = ws_words(l, d.sq) * 4;
         if (acc && acc + wsb > b->wave_bytes) {
             waves.emplace_back();
@@ -317,13 +324,6 @@ static int persist_build(sbg_batch* b) {
         }
         acc += wsb;
         Wave& w = waves.back();
-        const uint32_t nb = (uint32_t)crt_blocks(d.nout);
-        const uint16_t lg = (uint16_t)l;
-        if (l <= SBG_SMALL_MAX_LG) {
-            for (uint32_t q = 0; q < SBG_NP; ++q) w.s[0].push_back(PItem{(uint32_t)j, PK_SMALL, lg, q, 0});
-            for (uint32_t k = 0; k < nb; ++k) w.s[1].push_back(PItem{(uint32_t)j, PK_CRT, lg, k, SBG_NP});
-            continue;
-        }
         const int lgN1 = l - 12;
         const uint32_t nt = (uint32_t)col_tiles(lgN1);
         const uint32_t nops = d.sq ? 1 : 2;
@@ -342,6 +342,7 @@ static int persist_build(sbg_batch* b) {
             const int w = t - st;
             if (w >= 0 && w < nw) q.insert(q.end(), waves[w].s[st].begin(), waves[w].s[st].end());
         }
+    q.insert(q.end(), tail.begin(), tail.end());
     // class table, items and progress state in one allocation
     std::vector<PClass> cls(SBG_NCODES + 1);
     for (int l = 0; l <= SBG_NCODES; ++l) {

@@ -106,7 +106,8 @@ struct JobDesc {
 // One work item of the persistent batch kernel: a stage of one job (or a
 // group of up to 8 schoolbook jobs).  `need` is the value the job's progress
 // counter must reach before the item may start (its earlier stages done).
-enum PKind : uint16_t { PK_SCHOOL = 0, PK_SMALL = 1, PK_COLF = 2, PK_ROW = 3, PK_COLI = 4, PK_CRT = 5 };
+enum PKind : uint16_t { PK_SCHOOL = 0, PK_SMALL = 1, PK_COLF = 2, PK_ROW = 3, PK_COLI = 4, PK_CRT = 5,
+                        PK_SMALLJOB = 6 };
 struct PItem {
     uint32_t job;           // index into the batch's JobDesc array (first job of a group)
     uint16_t kind;          // PKind

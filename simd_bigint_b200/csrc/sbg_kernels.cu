@@ -289,9 +289,9 @@ __device__ __forceinline__ void col_pass_pair(uint32_t* sm, const uint64_t* __re
             }
         }
         if constexpr (FWD)
-            dif_regs2<R>(x, y, tw, j0, ST, LGM, p);
+            dif_regs2<R, ST == 1>(x, y, tw, j0, ST, LGM, p);
         else
-            dit_regs2<R>(x, y, tw, j0, ST, LGM, p);
+            dit_regs2<R, ST == 1>(x, y, tw, j0, ST, LGM, p);
         if constexpr (DST_G) {
             const int64_t n0 = ((int64_t)(i0 + row0) << SBG_ROW_LG) + c0 + g0;
 #pragma unroll
@@ -363,9 +363,9 @@ __device__ __forceinline__ void col_pass_lane(uint32_t* sm, const uint64_t* __re
             for (int t = 0; t < R; ++t) x[t] = s0[ST * t];
         }
         if constexpr (FWD)
-            dif_regs<R>(x, tw, j0, ST, LGM, p);
+            dif_regs<R, ST == 1>(x, tw, j0, ST, LGM, p);
         else
-            dit_regs<R>(x, tw, j0, ST, LGM, p);
+            dit_regs<R, ST == 1>(x, tw, j0, ST, LGM, p);
         if constexpr (DST_G) {
             const int64_t n0 = ((int64_t)(i0 + row0) << SBG_ROW_LG) + c0 + col;
 #pragma unroll
@@ -523,6 +523,30 @@ __device__ __forceinline__ void col_cross_inv(uint32_t* sm, uint32_t* __restrict
     }
 }
 
+// L2 prefetch of the rows a later tile's CTAs will read.  The column passes
+// read strided row pieces (one per row, 32 KB apart), whose L2 misses the
+// CTA waits for; the CTAs of tile t + SBG_COL_PREFETCH start about a wave
+// later, so their rows are requested now and are in L2 when they need them.
+// One CTA per (slab, tile) prefetches (prime 0 for the operands, which all
+// five primes read; every prime for its own residue plane).
+#ifndef SBG_COL_PREFETCH
+#define SBG_COL_PREFETCH 16         // tiles ahead; 0 turns the prefetch off
+#endif
+template <int LGN1, class T>
+__device__ __forceinline__ void col_prefetch(const T* __restrict__ X, int64_t xn, int tile, int slab) {
+    if constexpr (SBG_COL_PREFETCH > 0) {
+        constexpr int LGS = col_lgs(LGN1);
+        constexpr int LGW = col_lgw(LGN1);
+        const int t2 = tile + SBG_COL_PREFETCH;
+        if (t2 >= col_ntiles(LGN1)) return;
+        const int64_t c0 = (int64_t)t2 << LGW;
+        for (int i = threadIdx.x; i < (1 << LGS); i += COL_THREADS) {
+            const int64_t n = ((int64_t)((slab << LGS) + i) << SBG_ROW_LG) + c0;
+            if (n < xn) asm volatile("prefetch.global.L2 [%0];" ::"l"(X + n));
+        }
+    }
+}
+
 // K1: limbs -> residues -> column DIF (bit-reversed rows) for one operand,
 // one prime, one tile (one slab of it when the column spans a cluster).
 template <int LGN1>
@@ -541,6 +565,7 @@ __device__ __forceinline__ void col_fwd_body(int q, int tile, int slab, int op,
     const PrimeConst pc = c_pr[q];
     const uint2* tw = twf + (size_t)q * SBG_TW_N;
     const int c0 = tile << col_lgw(LGN1);
+    if (q == 0) col_prefetch<LGN1>(X, xn, tile, slab);
     if constexpr (LGC == 0) {
         col_slab_fwd<col_lanes(LGN1), LGS, true, true>(sm, X, xn, Y, c0, 0, tw, pc);
     } else {
@@ -599,6 +624,7 @@ __device__ __forceinline__ void col_inv_body(int q, int tile, int slab, uint32_t
     const PrimeConst pc = c_pr[q];
     const uint2* tw = twi + (size_t)q * SBG_TW_N;
     const int c0 = tile << col_lgw(LGN1);
+    col_prefetch<LGN1>(Y, (int64_t)1 << (LGN1 + SBG_ROW_LG), tile, slab);
     if constexpr (LGC == 0) {
         col_slab_inv<col_lanes(LGN1), LGS, true, true>(sm, Y, c0, 0, tw, pc);
     } else {
@@ -1085,15 +1111,15 @@ __device__ __forceinline__ void row_body(int q, int row, uint32_t* __restrict__ 
             if (!sq) xb[t] = smB[pad_idx(i0 + t)];
         }
         if (sq) {
-            dif_regs<16>(xa, tf, 0, 1, 4, p);
+            dif_regs<16, true>(xa, tf, 0, 1, 4, p);
 #pragma unroll
             for (int t = 0; t < 16; ++t) xa[t] = mont_mul(xa[t], xa[t], p, pc.pinv);
         } else {
-            dif_regs2<16>(xa, xb, tf, 0, 1, 4, p);
+            dif_regs2<16, true>(xa, xb, tf, 0, 1, 4, p);
 #pragma unroll
             for (int t = 0; t < 16; ++t) xa[t] = mont_mul(xa[t], xb[t], p, pc.pinv);
         }
-        dit_regs<16>(xa, ti, 0, 1, 4, p);
+        dit_regs<16, true>(xa, ti, 0, 1, 4, p);
 #pragma unroll
         for (int t = 0; t < 16; ++t) smA[pad_idx(i0 + t)] = xa[t];
     }

@@ -38,8 +38,10 @@ struct RLog {
     static constexpr int v = (R == 2) ? 1 : (R == 4) ? 2 : (R == 8) ? 3 : (R == 16) ? 4 : 5;
 };
 
-// forward DIF levels of one group (block size 2^lgM, stride st)
-template <int R>
+// forward DIF levels of one group (block size 2^lgM, stride st).  J0Z: the
+// caller's j0 is 0, so the butterflies at tin = 0 have the twiddle 1 and
+// skip the multiply (and the table load).
+template <int R, bool J0Z = false>
 __device__ __forceinline__ void dif_regs(uint32_t (&x)[R], const uint2* __restrict__ tw, int j0,
                                          int st, int lgM, uint32_t p) {
 #pragma unroll
@@ -48,6 +50,10 @@ __device__ __forceinline__ void dif_regs(uint32_t (&x)[R], const uint2* __restri
         for (int t = 0; t < R; ++t) {
             if (t & h) continue;
             int tin = t & (2 * h - 1);
+            if (J0Z && tin == 0) {
+                bfly_triv(x[t], x[t + h], p);
+                continue;
+            }
             uint2 w = __ldg(&tw[tw_idx(lgM - l, j0 + st * tin)]);
             bfly_gs(x[t], x[t + h], w.x, w.y, p);
         }
@@ -55,7 +61,7 @@ __device__ __forceinline__ void dif_regs(uint32_t (&x)[R], const uint2* __restri
 }
 
 // two groups sharing (j0, st, lgM): one twiddle load serves both
-template <int R>
+template <int R, bool J0Z = false>
 __device__ __forceinline__ void dif_regs2(uint32_t (&x)[R], uint32_t (&y)[R],
                                           const uint2* __restrict__ tw, int j0, int st, int lgM,
                                           uint32_t p) {
@@ -65,6 +71,11 @@ __device__ __forceinline__ void dif_regs2(uint32_t (&x)[R], uint32_t (&y)[R],
         for (int t = 0; t < R; ++t) {
             if (t & h) continue;
             int tin = t & (2 * h - 1);
+            if (J0Z && tin == 0) {
+                bfly_triv(x[t], x[t + h], p);
+                bfly_triv(y[t], y[t + h], p);
+                continue;
+            }
             uint2 w = __ldg(&tw[tw_idx(lgM - l, j0 + st * tin)]);
             bfly_gs(x[t], x[t + h], w.x, w.y, p);
             bfly_gs(y[t], y[t + h], w.x, w.y, p);
@@ -73,7 +84,7 @@ __device__ __forceinline__ void dif_regs2(uint32_t (&x)[R], uint32_t (&y)[R],
 }
 
 // inverse: the forward group's levels in reverse, Cooley-Tukey with w^-1
-template <int R>
+template <int R, bool J0Z = false>
 __device__ __forceinline__ void dit_regs(uint32_t (&x)[R], const uint2* __restrict__ twi, int j0,
                                          int st, int lgM, uint32_t p) {
     constexpr int r = RLog<R>::v;
@@ -84,13 +95,17 @@ __device__ __forceinline__ void dit_regs(uint32_t (&x)[R], const uint2* __restri
         for (int t = 0; t < R; ++t) {
             if (t & h) continue;
             int tin = t & (2 * h - 1);
+            if (J0Z && tin == 0) {
+                bfly_triv(x[t], x[t + h], p);
+                continue;
+            }
             uint2 w = __ldg(&twi[tw_idx(lgM - l, j0 + st * tin)]);
             bfly_ct(x[t], x[t + h], w.x, w.y, p);
         }
     }
 }
 
-template <int R>
+template <int R, bool J0Z = false>
 __device__ __forceinline__ void dit_regs2(uint32_t (&x)[R], uint32_t (&y)[R],
                                           const uint2* __restrict__ twi, int j0, int st, int lgM,
                                           uint32_t p) {
@@ -102,6 +117,11 @@ __device__ __forceinline__ void dit_regs2(uint32_t (&x)[R], uint32_t (&y)[R],
         for (int t = 0; t < R; ++t) {
             if (t & h) continue;
             int tin = t & (2 * h - 1);
+            if (J0Z && tin == 0) {
+                bfly_triv(x[t], x[t + h], p);
+                bfly_triv(y[t], y[t + h], p);
+                continue;
+            }
             uint2 w = __ldg(&twi[tw_idx(lgM - l, j0 + st * tin)]);
             bfly_ct(x[t], x[t + h], w.x, w.y, p);
             bfly_ct(y[t], y[t + h], w.x, w.y, p);

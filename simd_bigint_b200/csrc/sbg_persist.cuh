@@ -4,10 +4,10 @@
 // One launch runs a whole batch of uneven products.  Its CTAs (as many as
 // fit on the device at once) take work items from a queue in device memory,
 // one at a time, by an atomic increment of the queue head.  An item is one
-// stage of one job on one tile: the single-CTA transform of one prime
-// (small lengths), a column-forward tile, a row, a column-inverse tile, a
-// carry-scan block -- or a group of up to eight schoolbook jobs, one warp
-// each.  Every job has a progress counter that each finished item of the job
+// stage of one job on one tile -- a column-forward tile, a row, a
+// column-inverse tile, a carry-scan block -- or a whole short product: a
+// single-CTA product (five transforms of at most 2^12 points and its carry
+// blocks) or a group of up to eight schoolbook products, one warp each.  Every job has a progress counter that each finished item of the job
 // increments; an item carries the counter value its job's earlier stages
 // reach, and the CTA that takes it waits (bounded) until the counter gets
 // there.
@@ -24,7 +24,9 @@
 // carry blocks of wave t - 3, the inverse columns of wave t - 2, the rows of
 // wave t - 1 and the forward columns of wave t.  A stage's input was written
 // one step earlier, so it is mostly still in L2, and the items of a step do
-// not wait on each other.
+// not wait on each other.  The whole short products, which wait for
+// nothing, come last: they fill the CTAs that the last waves' stages leave
+// idle.
 #pragma once
 
 namespace sbg {
@@ -82,6 +84,23 @@ __device__ __forceinline__ void persist_item(uint32_t kind, uint32_t job, uint32
         case PK_SMALL: {
             const JobDesc& J = jobs[job];
             small_body((int)idx, J.a, J.an, J.b, J.bn, J.sq, (int)lg, twf, twi, cls[lg].sc, J.ws);
+            break;
+        }
+        case PK_SMALLJOB: {
+            // a whole single-CTA product: the five primes' transforms, then
+            // its carry blocks in order (each block's look-back finds its
+            // predecessor's flag already published)
+            const JobDesc& J = jobs[job];
+            for (int q = 0; q < SBG_NP; ++q) {
+                small_body(q, J.a, J.an, J.b, J.bn, J.sq, (int)lg, twf, twi, cls[lg].sc, J.ws);
+                __syncthreads();
+            }
+            __threadfence_block();
+            for (uint32_t k = 0; k < idx; ++k) {
+                crt_body(k, J.ws, (int64_t)1 << lg, J.cmin, J.cmax, J.off, J.out, J.nout, J.flags, err,
+                         *reinterpret_cast<CrtSmem*>(sm));
+                __syncthreads();
+            }
             break;
         }
         case PK_COLF:
@@ -153,7 +172,7 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 4)
         persist_item(kind, job, __reduce_max_sync(0xffffffffu, (uint32_t)s_it.lg),
                      __reduce_max_sync(0xffffffffu, s_it.idx), jobs, cls, twf, twi, err, sm);
         __syncthreads();
-        if (threadIdx.x == 0 && kind != PK_SCHOOL) {
+        if (threadIdx.x == 0 && kind != PK_SCHOOL && kind != PK_SMALLJOB) {
             __threadfence();
             atomicAdd(&state[1 + job], 1u);
         }

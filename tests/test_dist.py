@@ -63,3 +63,38 @@ def test_reference_arm_under_torchrun_two_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["cores"] >= 1
+
+
+def _rank_dies(rank: int, port: int, q):
+    import importlib.util
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE="2", RANK=str(rank),
+                      LOCAL_RANK=str(rank))
+    spec = importlib.util.spec_from_file_location("bench_mod", ROOT / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    ws, r, local, pg = bench.dist_init(backend="gloo", timeout_s=20)
+    if r == 1:
+        os._exit(3)                 # a rank that dies between steps, with nothing in flight
+    try:
+        bench.barrier_max(pg, 1.0, "cpu")
+        q.put((r, "no error"))
+    except Exception as e:          # the survivor learns of it at its next collective
+        q.put((r, type(e).__name__))
+
+
+def test_a_dead_rank_ends_the_next_collective_with_an_error():
+    """Failure detection on the host: rank 1 exits between steps; rank 0's
+    next collective (the max over ranks of the timings) ends with an error
+    instead of waiting for ever."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_rank_dies, args=(r, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    r, what = q.get(timeout=120)
+    for p in ps:
+        p.join(timeout=60)
+    assert r == 0 and what != "no error"
+    assert ps[1].exitcode == 3
