@@ -550,6 +550,10 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
     jobs = [(kind, ob + 8 * ro, ib + 8 * ao, ib + 8 * (bo if kind != sbg.JOB_SQR else ao), an, bn)
             for (kind, an, bn), ao, bo, ro in zip(shapes, a_off, b_off, r_off)]
     batch = sbg.Batch(ctx, jobs)
+    # the library's own choice of engine for this batch (timed on the device)
+    tuned_ms = batch.autotune()
+    engine_names = ("persistent_queue", "per_class_graph", "queue_one_cta_per_item")
+    tuned = int(np.argmin(tuned_ms))
     batch.capture()
     clocks = ClockSampler(local)
     if rank == 0:
@@ -584,8 +588,10 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
     # the same batch on the other engines: one launch per stage per length
     # class (captured graph), and the queue with one CTA per item; each
     # checked against the default engine's products
-    engines = {"persistent_queue": {"ms": round(ms_step, 4), "launches_per_step": batch_launches / args.steps}}
-    for eng, name in ((1, "per_class_graph"), (2, "queue_one_cta_per_item")):
+    engines = {engine_names[tuned]: {"ms": round(ms_step, 4), "launches_per_step": batch_launches / args.steps}}
+    for eng, name in enumerate(engine_names):
+        if eng == tuned:
+            continue
         batch.set_engine(eng)
         batch.capture()
         d_out.fill_(-1)
@@ -596,7 +602,7 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
         exact = exact and same
         ms_e, l_e = timed_runs()
         engines[name] = {"ms": round(ms_e, 4), "launches_per_step": l_e / args.steps, "same_products": same}
-    batch.set_engine(0)
+    batch.set_engine(tuned)
     batch.capture()
     # one multiply per launch over the same batch
     L = sbg.lib()
@@ -622,6 +628,7 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
     jobs2 = [(kind, ob2 + 8 * ro, ib2 + 8 * ao, ib2 + 8 * (bo if kind != sbg.JOB_SQR else ao), an, bn)
              for (kind, an, bn), ao, bo, ro in zip(shapes, a_off, b_off, r_off)]
     batch2 = sbg.Batch(ctx, jobs2)
+    batch2.set_engine(tuned)
     batch2.capture()
     sets = [(d_in, d_out, batch), (d_in2, d_out2, batch2)]
     s_in = torch.cuda.Stream(device=dev)
@@ -680,7 +687,8 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
         "bit_exact": bool(exact),
         "one_per_launch": {"value": round(single, 2), "unit": "Mlimb/s", "ms": round(ms_single, 3),
                            "ratio_batched_vs_single": round(value / ws / single, 2)},
-        "engine": "persistent kernel over a device work-item queue (one launch per batch)",
+        "engine": {"chosen": engine_names[tuned], "by": "sbg_batch_autotune (each engine timed on this batch)",
+                   "autotune_ms": [round(x, 4) for x in tuned_ms]},
         "engines": {k: {**v, "value": round(total / (v["ms"] * 1e-3) / 1e6, 2), "unit": "Mlimb/s",
                         "ratio_vs_one_per_launch": round(total / (v["ms"] * 1e-3) / 1e6 / single, 2)}
                     for k, v in engines.items()},

@@ -135,6 +135,8 @@ def lib(build_if_missing: bool = False):
         L.sbg_mul_noalloc.restype = C.c_int
         L.sbg_batch_set_engine.argtypes = [_vp, C.c_int, _i64]
         L.sbg_batch_set_engine.restype = C.c_int
+        L.sbg_batch_autotune.argtypes = [_vp, C.POINTER(C.c_double)]
+        L.sbg_batch_autotune.restype = C.c_int
         L.sbg_u52_from_u64.argtypes = [_vp, _vp, _i64, _vp, _i64]
         L.sbg_u52_from_u64.restype = C.c_int
         L.sbg_u64_from_u52.argtypes = [_vp, _vp, _i64, _vp, _i64, C.c_int]
@@ -377,6 +379,13 @@ class Batch:
         per item.  wave_bytes: the queue's L2 blocking (0: keep).  Drops a
         captured graph (capture again)."""
         _check(self._L.sbg_batch_set_engine(self.handle, engine, wave_bytes), "sbg_batch_set_engine")
+
+    def autotune(self) -> list[float]:
+        """Times each engine on this batch and keeps the fastest; returns the
+        per-run milliseconds of engines 0, 1, 2."""
+        ms = (C.c_double * 3)()
+        _check(self._L.sbg_batch_autotune(self.handle, ms), "sbg_batch_autotune")
+        return list(ms)
 
     def run(self):
         _check(self._L.sbg_batch_run(self.handle), "sbg_batch_run")

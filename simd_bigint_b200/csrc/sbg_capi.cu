@@ -196,7 +196,7 @@ struct sbg_batch {
     uint32_t* d_state = nullptr;         // queue head + one progress counter per job
     size_t state_words = 0;
     PClass* d_cls = nullptr;
-    size_t wave_bytes = (size_t)48 << 20;
+    size_t wave_bytes = (size_t)16 << 20;
     int grid = 0;
 };
 
@@ -874,6 +874,40 @@ int sbg_batch_set_engine(sbg_batch* b, int engine, int64_t wave_bytes) {
         return persist_build(b);
     }
     return SBG_OK;
+}
+
+int sbg_batch_autotune(sbg_batch* b, double* ms) {
+    if (!b) return SBG_EINVAL;
+    sbg_ctx* c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    double best = 0.0;
+    int best_engine = 0, st = SBG_OK;
+    for (int eng = 0; eng < 3 && !st; ++eng) {
+        if ((st = sbg_batch_set_engine(b, eng, 0))) break;
+        for (int w = 0; w < 2 && !st; ++w) st = batch_launch(b, nullptr);     // warm-up
+        if (st) break;
+        if ((st = cuda_fail(cudaEventRecord(e0, c->stream), "event"))) break;
+        for (int r = 0; r < 3 && !st; ++r) st = batch_launch(b, nullptr);
+        if (st) break;
+        float t = 0.f;
+        if ((st = cuda_fail(cudaEventRecord(e1, c->stream), "event")) ||
+            (st = cuda_fail(cudaEventSynchronize(e1), "event")) ||
+            (st = cuda_fail(cudaEventElapsedTime(&t, e0, e1), "event")))
+            break;
+        const double m = t / 3.0;
+        if (ms) ms[eng] = m;
+        if (eng == 0 || m < best) {
+            best = m;
+            best_engine = eng;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    return sbg_batch_set_engine(b, best_engine, 0);
 }
 
 int64_t sbg_ctx_launches(sbg_ctx* c) { return c ? c->launches.load() + c->ring.pulls : 0; }

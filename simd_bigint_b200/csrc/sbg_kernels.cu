@@ -523,30 +523,6 @@ __device__ __forceinline__ void col_cross_inv(uint32_t* sm, uint32_t* __restrict
     }
 }
 
-// L2 prefetch of the rows a later tile's CTAs will read.  The column passes
-// read strided row pieces (one per row, 32 KB apart), whose L2 misses the
-// CTA waits for; the CTAs of tile t + SBG_COL_PREFETCH start about a wave
-// later, so their rows are requested now and are in L2 when they need them.
-// One CTA per (slab, tile) prefetches (prime 0 for the operands, which all
-// five primes read; every prime for its own residue plane).
-#ifndef SBG_COL_PREFETCH
-#define SBG_COL_PREFETCH 16         // tiles ahead; 0 turns the prefetch off
-#endif
-template <int LGN1, class T>
-__device__ __forceinline__ void col_prefetch(const T* __restrict__ X, int64_t xn, int tile, int slab) {
-    if constexpr (SBG_COL_PREFETCH > 0) {
-        constexpr int LGS = col_lgs(LGN1);
-        constexpr int LGW = col_lgw(LGN1);
-        const int t2 = tile + SBG_COL_PREFETCH;
-        if (t2 >= col_ntiles(LGN1)) return;
-        const int64_t c0 = (int64_t)t2 << LGW;
-        for (int i = threadIdx.x; i < (1 << LGS); i += COL_THREADS) {
-            const int64_t n = ((int64_t)((slab << LGS) + i) << SBG_ROW_LG) + c0;
-            if (n < xn) asm volatile("prefetch.global.L2 [%0];" ::"l"(X + n));
-        }
-    }
-}
-
 // K1: limbs -> residues -> column DIF (bit-reversed rows) for one operand,
 // one prime, one tile (one slab of it when the column spans a cluster).
 template <int LGN1>
@@ -565,7 +541,6 @@ __device__ __forceinline__ void col_fwd_body(int q, int tile, int slab, int op,
     const PrimeConst pc = c_pr[q];
     const uint2* tw = twf + (size_t)q * SBG_TW_N;
     const int c0 = tile << col_lgw(LGN1);
-    if (q == 0) col_prefetch<LGN1>(X, xn, tile, slab);
     if constexpr (LGC == 0) {
         col_slab_fwd<col_lanes(LGN1), LGS, true, true>(sm, X, xn, Y, c0, 0, tw, pc);
     } else {
@@ -624,7 +599,6 @@ __device__ __forceinline__ void col_inv_body(int q, int tile, int slab, uint32_t
     const PrimeConst pc = c_pr[q];
     const uint2* tw = twi + (size_t)q * SBG_TW_N;
     const int c0 = tile << col_lgw(LGN1);
-    col_prefetch<LGN1>(Y, (int64_t)1 << (LGN1 + SBG_ROW_LG), tile, slab);
     if constexpr (LGC == 0) {
         col_slab_inv<col_lanes(LGN1), LGS, true, true>(sm, Y, c0, 0, tw, pc);
     } else {

@@ -37,19 +37,36 @@ namespace sbg {
 // any wait of the launch has expired (the error word's timeout bit is set)
 // the others give up at once, so a fault in the queue's order costs one
 // expiry, not one per item.
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ void persist_wait(const uint32_t* cnt, uint32_t need, uint32_t* err) {
-    const volatile uint32_t* v = cnt;
     const volatile uint32_t* e = err;
     int spins = 0;
-    while (*v < need) {
+    while (ld_acquire(cnt) < need) {
         if (++spins > PERSIST_WAIT_LIMIT || ((spins & 63) == 0 && (*e & 1u))) {
             atomicOr(err, 1u);
             break;
         }
         __nanosleep(64);
     }
-    __threadfence();
 }
+
+// A finished item: the CTA's writes (ordered before this by the barrier the
+// caller passed) are released to the device with the counter increment; no
+// return value is waited for.
+__device__ __forceinline__ void persist_signal(uint32_t* cnt) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
+}
+
+// items a persistent CTA takes per queue-head increment (held items run in
+// queue order, so the waits' progress argument is unchanged).  Measured on
+// B200: taking 4 at a time made the mixed batch 1.7x slower than taking one
+// (a CTA sits on items that idle CTAs could run), so one it is.
+#define PERSIST_GRAB 1
 
 template <int LGN1>
 __device__ __forceinline__ void persist_col(const PItem& I, const JobDesc& J, const uint2* __restrict__ twf,
@@ -149,16 +166,25 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 4)
               const PClass* __restrict__ cls, uint32_t* state, const uint2* __restrict__ twf,
               const uint2* __restrict__ twi, uint32_t* err) {
     extern __shared__ uint32_t sm[];
-    // the current item, in shared memory so that nothing of it stays live in
-    // registers across the stage bodies
+    // the held items and the current one, in shared memory so that nothing of
+    // them stays live in registers across the stage bodies
+    constexpr int GRAB = LOOP ? PERSIST_GRAB : 1;
+    __shared__ PItem s_q[GRAB];
     __shared__ PItem s_it;
-    __shared__ int s_more;
+    __shared__ int s_more, s_k, s_n;
+    if (threadIdx.x == 0) s_k = s_n = 0;
     do {
         if (threadIdx.x == 0) {
-            const int it = (int)atomicAdd(&state[0], 1u);
-            s_more = it < nitems;
-            if (it < nitems) {
-                const PItem I = items[it];
+            if (s_k == s_n) {                   // take the next block of tickets
+                const int base = (int)atomicAdd(&state[0], (uint32_t)GRAB);
+                const int n = max(0, min(GRAB, nitems - base));
+                for (int i = 0; i < n; ++i) s_q[i] = items[base + i];
+                s_n = n;
+                s_k = 0;
+            }
+            s_more = s_k < s_n;
+            if (s_more) {
+                const PItem I = s_q[s_k++];
                 s_it = I;
                 if (I.need) persist_wait(&state[1 + I.job], I.need, err);
             }
@@ -172,10 +198,7 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 4)
         persist_item(kind, job, __reduce_max_sync(0xffffffffu, (uint32_t)s_it.lg),
                      __reduce_max_sync(0xffffffffu, s_it.idx), jobs, cls, twf, twi, err, sm);
         __syncthreads();
-        if (threadIdx.x == 0 && kind != PK_SCHOOL && kind != PK_SMALLJOB) {
-            __threadfence();
-            atomicAdd(&state[1 + job], 1u);
-        }
+        if (threadIdx.x == 0 && kind != PK_SCHOOL && kind != PK_SMALLJOB) persist_signal(&state[1 + job]);
     } while (LOOP);
 }
 
