@@ -589,10 +589,11 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
     # class (captured graph), and the queue with one CTA per item; each
     # checked against the default engine's products
     engines = {engine_names[tuned]: {"ms": round(ms_step, 4), "launches_per_step": batch_launches / args.steps}}
+    waves = (64 << 20, 0, 16 << 20)          # each queue engine at its better wave size
     for eng, name in enumerate(engine_names):
         if eng == tuned:
             continue
-        batch.set_engine(eng)
+        batch.set_engine(eng, waves[eng])
         batch.capture()
         d_out.fill_(-1)
         for _ in range(args.warmup):

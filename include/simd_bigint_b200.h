@@ -175,14 +175,15 @@ void sbg_batch_destroy(sbg_batch *batch);
  * and 3 * 2^k classes keep per-class launches beside it).  1: one launch per
  * stage per length class for every class.  2: the same queue and kernel,
  * one CTA per item instead of persistent CTAs.  wave_bytes (0: keep the
- * current, default 16 MB) bounds the transform workspace of the jobs whose
+ * current, default 64 MB) bounds the transform workspace of the jobs whose
  * stages the queue interleaves (L2 blocking).  Drops a captured graph:
  * capture again.  No counterpart in the reference. */
 int sbg_batch_set_engine(sbg_batch *batch, int engine, int64_t wave_bytes);
-/* Times three runs of the batch on each engine (after two warm-up runs; the
- * products are written each time) and keeps the fastest; ms (optional, 3
- * doubles) receives the per-run milliseconds of engines 0, 1, 2.  Capture
- * the graph afterwards.  No counterpart in the reference. */
+/* Times three runs of the batch on each engine (the queue engines at 16 and
+ * 64 MB waves; after two warm-up runs; the products are written each time)
+ * and keeps the fastest; ms (optional, 3 doubles) receives the best per-run
+ * milliseconds of engines 0, 1, 2.  Capture the graph afterwards.  No
+ * counterpart in the reference. */
 int sbg_batch_autotune(sbg_batch *batch, double *ms);
 /* One-shot batch through the context's reusable product arena (no per-call
  * allocation once it has grown): returns when the products are written. */

@@ -196,7 +196,7 @@ struct sbg_batch {
     uint32_t* d_state = nullptr;         // queue head + one progress counter per job
     size_t state_words = 0;
     PClass* d_cls = nullptr;
-    size_t wave_bytes = (size_t)16 << 20;
+    size_t wave_bytes = (size_t)64 << 20;
     int grid = 0;
 };
 
@@ -327,11 +327,12 @@ static int persist_build(sbg_batch* b) {
         const int lgN1 = l - 12;
         const uint32_t nt = (uint32_t)col_tiles(lgN1);
         const uint32_t nops = d.sq ? 1 : 2;
-        const uint32_t n_colf = nops * nt * SBG_NP, n_row = (uint32_t)SBG_NP << lgN1, n_coli = nt * SBG_NP;
+        const uint32_t n_colf = nops * nt * SBG_NP, n_row = ((uint32_t)SBG_NP << lgN1) / PERSIST_ROWS,
+                       n_coli = nt * SBG_NP, n_crt = (nb + PERSIST_CRT - 1) / PERSIST_CRT;
         for (uint32_t i = 0; i < n_colf; ++i) w.s[0].push_back(PItem{(uint32_t)j, PK_COLF, lg, i, 0});
         for (uint32_t i = 0; i < n_row; ++i) w.s[1].push_back(PItem{(uint32_t)j, PK_ROW, lg, i, n_colf});
         for (uint32_t i = 0; i < n_coli; ++i) w.s[2].push_back(PItem{(uint32_t)j, PK_COLI, lg, i, n_colf + n_row});
-        for (uint32_t k = 0; k < nb; ++k)
+        for (uint32_t k = 0; k < n_crt; ++k)
             w.s[3].push_back(PItem{(uint32_t)j, PK_CRT, lg, k, n_colf + n_row + n_coli});
     }
     flush_school();
@@ -876,6 +877,9 @@ int sbg_batch_set_engine(sbg_batch* b, int engine, int64_t wave_bytes) {
     return SBG_OK;
 }
 
+// Times the engines on the batch -- the queue engines at two wave sizes
+// (their best waves differ: 64 MB for the persistent CTAs, 16 MB for one CTA
+// per item on B200) -- and keeps the fastest.
 int sbg_batch_autotune(sbg_batch* b, double* ms) {
     if (!b) return SBG_EINVAL;
     sbg_ctx* c = b->ctx;
@@ -883,10 +887,16 @@ int sbg_batch_autotune(sbg_batch* b, double* ms) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    double best = 0.0;
-    int best_engine = 0, st = SBG_OK;
-    for (int eng = 0; eng < 3 && !st; ++eng) {
-        if ((st = sbg_batch_set_engine(b, eng, 0))) break;
+    struct Cfg {
+        int engine;
+        int64_t wave;
+    };
+    const Cfg cfgs[5] = {{0, (int64_t)64 << 20}, {0, (int64_t)16 << 20}, {1, 0},
+                         {2, (int64_t)16 << 20}, {2, (int64_t)64 << 20}};
+    double best = 0.0, eng_ms[3] = {0.0, 0.0, 0.0};
+    int best_i = 0, st = SBG_OK;
+    for (int i = 0; i < 5 && !st; ++i) {
+        if ((st = sbg_batch_set_engine(b, cfgs[i].engine, cfgs[i].wave))) break;
         for (int w = 0; w < 2 && !st; ++w) st = batch_launch(b, nullptr);     // warm-up
         if (st) break;
         if ((st = cuda_fail(cudaEventRecord(e0, c->stream), "event"))) break;
@@ -898,16 +908,19 @@ int sbg_batch_autotune(sbg_batch* b, double* ms) {
             (st = cuda_fail(cudaEventElapsedTime(&t, e0, e1), "event")))
             break;
         const double m = t / 3.0;
-        if (ms) ms[eng] = m;
-        if (eng == 0 || m < best) {
+        const int e = cfgs[i].engine;
+        if (eng_ms[e] == 0.0 || m < eng_ms[e]) eng_ms[e] = m;
+        if (i == 0 || m < best) {
             best = m;
-            best_engine = eng;
+            best_i = i;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st) return st;
-    return sbg_batch_set_engine(b, best_engine, 0);
+    if (ms)
+        for (int e = 0; e < 3; ++e) ms[e] = eng_ms[e];
+    return sbg_batch_set_engine(b, cfgs[best_i].engine, cfgs[best_i].wave ? cfgs[best_i].wave : 0);
 }
 
 int64_t sbg_ctx_launches(sbg_ctx* c) { return c ? c->launches.load() + c->ring.pulls : 0; }

@@ -186,10 +186,14 @@ __host__ __device__ constexpr int col_ld(int lgN1) { return col_ld_of(col_lanes(
 // the remainder first costs an extra shared-memory round trip; both were
 // slower on B200.)
 __host__ __device__ constexpr int col_np(int lg) { return num_passes(lg); }
-__host__ __device__ constexpr int prl(int lg, int k) { return k < (lg >> 2) ? 4 : (lg & 3); }
-__host__ __device__ constexpr int lgm_of(int lg, int k) {
+// rf: the remainder pass first instead of last (the slabs of clustered
+// columns: the inverse then reads global memory with a radix-16 pass)
+__host__ __device__ constexpr int prl(int lg, int k, bool rf = false) {
+    return (rf && (lg & 3)) ? (k == 0 ? (lg & 3) : 4) : (k < (lg >> 2) ? 4 : (lg & 3));
+}
+__host__ __device__ constexpr int lgm_of(int lg, int k, bool rf = false) {
     int m = lg;
-    for (int i = 0; i < k; ++i) m -= prl(lg, i);
+    for (int i = 0; i < k; ++i) m -= prl(lg, i, rf);
     return m;
 }
 __host__ __device__ constexpr int col_smem_bytes(int lgN1) {
@@ -230,13 +234,13 @@ __device__ __forceinline__ void load_limb_pair(const uint64_t* __restrict__ X, i
 // Pass K (0-based, forward numbering) of the DIF/DIT of length 2^LGS on the
 // slab whose first row is row0.  SRC_G: read from global (limbs when FWD,
 // residues otherwise); DST_G: write residues to global; else shared memory.
-template <int LGS, int K, bool FWD, bool SRC_G, bool DST_G>
+template <int LGS, int K, bool FWD, bool SRC_G, bool DST_G, bool RF = false>
 __device__ __forceinline__ void col_pass_pair(uint32_t* sm, const uint64_t* __restrict__ X,
                                            int64_t xn, uint32_t* __restrict__ Y, int c0, int row0,
                                            const uint2* __restrict__ tw, const PrimeConst& pc) {
-    constexpr int r = prl(LGS, K);
+    constexpr int r = prl(LGS, K, RF);
     constexpr int R = 1 << r;
-    constexpr int LGM = lgm_of(LGS, K);
+    constexpr int LGM = lgm_of(LGS, K, RF);
     constexpr int LGST = LGM - r;
     constexpr int ST = 1 << LGST;
     constexpr int LGW = col_lgw_of(false, LGS);
@@ -320,13 +324,13 @@ __device__ __forceinline__ uint32_t load_limb(const uint64_t* __restrict__ X, in
 // group, one column per lane).  NSUB = 3: three 2^LGS-row slabs stacked in
 // the planes (the thirds of a 3 * 2^m column held by one CTA), transformed
 // independently.
-template <int LGS, int K, bool FWD, bool SRC_G, bool DST_G, int NSUB = 1>
+template <int LGS, int K, bool FWD, bool SRC_G, bool DST_G, int NSUB = 1, bool RF = false>
 __device__ __forceinline__ void col_pass_lane(uint32_t* sm, const uint64_t* __restrict__ X,
                                            int64_t xn, uint32_t* __restrict__ Y, int c0, int row0,
                                            const uint2* __restrict__ tw, const PrimeConst& pc) {
-    constexpr int r = prl(LGS, K);
+    constexpr int r = prl(LGS, K, RF);
     constexpr int R = 1 << r;
-    constexpr int LGM = lgm_of(LGS, K);
+    constexpr int LGM = lgm_of(LGS, K, RF);
     constexpr int LGST = LGM - r;
     constexpr int ST = 1 << LGST;
     constexpr int LGW = NSUB == 1 ? col_lgw_of(true, LGS) : col3s_lgw(LGS);
@@ -382,58 +386,63 @@ __device__ __forceinline__ void col_pass_lane(uint32_t* sm, const uint64_t* __re
 // slab whose first row is row0, in the mapping LANES selects.  SRC_G: read
 // from global (limbs when FWD, residues otherwise); DST_G: write residues to
 // global; else shared memory.
-template <bool LANES, int LGS, int K, bool FWD, bool SRC_G, bool DST_G, int NSUB = 1>
+template <bool LANES, int LGS, int K, bool FWD, bool SRC_G, bool DST_G, int NSUB = 1, bool RF = false>
 __device__ __forceinline__ void col_pass_t(uint32_t* sm, const uint64_t* __restrict__ X,
                                            int64_t xn, uint32_t* __restrict__ Y, int c0, int row0,
                                            const uint2* __restrict__ tw, const PrimeConst& pc) {
     if constexpr (LANES) {
-        col_pass_lane<LGS, K, FWD, SRC_G, DST_G, NSUB>(sm, X, xn, Y, c0, row0, tw, pc);
+        col_pass_lane<LGS, K, FWD, SRC_G, DST_G, NSUB, RF>(sm, X, xn, Y, c0, row0, tw, pc);
     } else {
         static_assert(NSUB == 1, "stacked slabs use the lane mapping");
-        col_pass_pair<LGS, K, FWD, SRC_G, DST_G>(sm, X, xn, Y, c0, row0, tw, pc);
+        col_pass_pair<LGS, K, FWD, SRC_G, DST_G, RF>(sm, X, xn, Y, c0, row0, tw, pc);
     }
 }
 
 // The local passes of a slab: forward K = 0 .. NP-1, inverse NP-1 .. 0.
 // FIRST_G / LAST_G: whether the first / last pass touches global memory.
-template <bool LANES, int LGS, bool FIRST_G, bool LAST_G, int NSUB = 1>
+template <bool LANES, int LGS, bool FIRST_G, bool LAST_G, int NSUB = 1, bool RF = false>
 __device__ __forceinline__ void col_slab_fwd(uint32_t* sm, const uint64_t* __restrict__ X, int64_t xn,
                                              uint32_t* __restrict__ Y, int c0, int row0,
                                              const uint2* __restrict__ tw, const PrimeConst& pc) {
     constexpr int NP = col_np(LGS);
-    col_pass_t<LANES, LGS, 0, true, FIRST_G, LAST_G && NP == 1, NSUB>(sm, X, xn, Y, c0, row0, tw, pc);
+    col_pass_t<LANES, LGS, 0, true, FIRST_G, LAST_G && NP == 1, NSUB, RF>(sm, X, xn, Y, c0, row0, tw, pc);
     if constexpr (NP > 1) {
         __syncthreads();
-        col_pass_t<LANES, LGS, 1, true, false, LAST_G && NP == 2, NSUB>(sm, X, xn, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 1, true, false, LAST_G && NP == 2, NSUB, RF>(sm, X, xn, Y, c0, row0, tw, pc);
     }
     if constexpr (NP > 2) {
         __syncthreads();
-        col_pass_t<LANES, LGS, 2, true, false, LAST_G && NP == 3, NSUB>(sm, X, xn, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 2, true, false, LAST_G && NP == 3, NSUB, RF>(sm, X, xn, Y, c0, row0, tw, pc);
     }
     if constexpr (NP > 3) {
         __syncthreads();
-        col_pass_t<LANES, LGS, 3, true, false, LAST_G && NP == 4, NSUB>(sm, X, xn, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 3, true, false, LAST_G && NP == 4, NSUB, RF>(sm, X, xn, Y, c0, row0, tw, pc);
     }
 }
 
-template <bool LANES, int LGS, bool FIRST_G, bool LAST_G, int NSUB = 1>
+template <bool LANES, int LGS, bool FIRST_G, bool LAST_G, int NSUB = 1, bool RF = false>
 __device__ __forceinline__ void col_slab_inv(uint32_t* sm, uint32_t* __restrict__ Y, int c0, int row0,
                                              const uint2* __restrict__ tw, const PrimeConst& pc) {
     constexpr int NP = col_np(LGS);
     if constexpr (NP > 3) {
-        col_pass_t<LANES, LGS, 3, false, FIRST_G, false, NSUB>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 3, false, FIRST_G, false, NSUB, RF>(sm, nullptr, 0, Y, c0, row0, tw, pc);
         __syncthreads();
     }
     if constexpr (NP > 2) {
-        col_pass_t<LANES, LGS, 2, false, FIRST_G && NP == 3, false, NSUB>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 2, false, FIRST_G && NP == 3, false, NSUB, RF>(sm, nullptr, 0, Y, c0, row0, tw, pc);
         __syncthreads();
     }
     if constexpr (NP > 1) {
-        col_pass_t<LANES, LGS, 1, false, FIRST_G && NP == 2, false, NSUB>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+        col_pass_t<LANES, LGS, 1, false, FIRST_G && NP == 2, false, NSUB, RF>(sm, nullptr, 0, Y, c0, row0, tw, pc);
         __syncthreads();
     }
-    col_pass_t<LANES, LGS, 0, false, FIRST_G && NP == 1, LAST_G, NSUB>(sm, nullptr, 0, Y, c0, row0, tw, pc);
+    col_pass_t<LANES, LGS, 0, false, FIRST_G && NP == 1, LAST_G, NSUB, RF>(sm, nullptr, 0, Y, c0, row0, tw, pc);
 }
+
+// clustered columns: slab passes with the remainder first (0: last)
+#ifndef SBG_COL_REMFIRST
+#define SBG_COL_REMFIRST 1
+#endif
 
 // cluster barrier; RELEASE publishes this CTA's shared-memory stores (local
 // and remote) to the cluster, otherwise it only waits for every CTA to arrive
@@ -547,7 +556,8 @@ __device__ __forceinline__ void col_fwd_body(int q, int tile, int slab, int op,
         cluster_barrier<false>();       // every CTA of the cluster is running
         col_cross_fwd<LGN1>(sm, X, xn, c0, slab, tw, pc);
         cluster_barrier<true>();        // all slabs complete in shared memory
-        col_slab_fwd<col_lanes(LGN1), LGS, false, true>(sm, X, xn, Y, c0, slab << LGS, tw, pc);
+        col_slab_fwd<col_lanes(LGN1), LGS, false, true, 1, SBG_COL_REMFIRST != 0>(sm, X, xn, Y, c0, slab << LGS,
+                                                                                  tw, pc);
     }
 }
 
@@ -602,7 +612,7 @@ __device__ __forceinline__ void col_inv_body(int q, int tile, int slab, uint32_t
     if constexpr (LGC == 0) {
         col_slab_inv<col_lanes(LGN1), LGS, true, true>(sm, Y, c0, 0, tw, pc);
     } else {
-        col_slab_inv<col_lanes(LGN1), LGS, true, false>(sm, Y, c0, slab << LGS, tw, pc);
+        col_slab_inv<col_lanes(LGN1), LGS, true, false, 1, SBG_COL_REMFIRST != 0>(sm, Y, c0, slab << LGS, tw, pc);
         cluster_barrier<true>();        // all slabs complete in shared memory
         col_cross_inv<LGN1>(sm, Y, c0, slab, tw, pc);
         cluster_barrier<false>();       // peers read this CTA's slab until here

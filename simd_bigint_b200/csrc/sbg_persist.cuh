@@ -62,11 +62,13 @@ __device__ __forceinline__ void persist_signal(uint32_t* cnt) {
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
 }
 
-// items a persistent CTA takes per queue-head increment (held items run in
-// queue order, so the waits' progress argument is unchanged).  Measured on
-// B200: taking 4 at a time made the mixed batch 1.7x slower than taking one
-// (a CTA sits on items that idle CTAs could run), so one it is.
-#define PERSIST_GRAB 1
+// A persistent CTA takes one item per queue-head increment (taking 4 at a
+// time made the mixed batch 1.7x slower on B200: a CTA sits on items that
+// idle CTAs could run) and, with PERSIST_PREFETCH, takes its next item while
+// it runs the current one.
+#ifndef PERSIST_PREFETCH
+#define PERSIST_PREFETCH 1
+#endif
 
 template <int LGN1>
 __device__ __forceinline__ void persist_col(const PItem& I, const JobDesc& J, const uint2* __restrict__ twf,
@@ -138,19 +140,29 @@ __device__ __forceinline__ void persist_item(uint32_t kind, uint32_t job, uint32
             break;
         }
         case PK_ROW: {
+            // PERSIST_ROWS consecutive rows of one prime (2^lgN1 >= 2 rows)
             const JobDesc& J = jobs[job];
             const int lgN1 = (int)lg - SBG_ROW_LG;
             const PClass& C = cls[lg];
             uint32_t* YB = J.ws + ((size_t)SBG_NP << lg);
-            const int q = (int)idx >> lgN1;
-            row_body(q, (int)idx & ((1 << lgN1) - 1), J.ws, YB, J.sq, lgN1, -1, C.fsf, C.fsi, C.sc.w[q],
-                     C.sc.ws[q], twf, twi, *reinterpret_cast<RowSmem*>(sm));
+            for (int k = 0; k < PERSIST_ROWS; ++k) {
+                const int r = (int)idx * PERSIST_ROWS + k;
+                const int q = r >> lgN1;
+                row_body(q, r & ((1 << lgN1) - 1), J.ws, YB, J.sq, lgN1, -1, C.fsf, C.fsi, C.sc.w[q],
+                         C.sc.ws[q], twf, twi, *reinterpret_cast<RowSmem*>(sm));
+                __syncthreads();
+            }
             break;
         }
         case PK_CRT: {
+            // up to PERSIST_CRT consecutive carry blocks, in block order
             const JobDesc& J = jobs[job];
-            crt_body(idx, J.ws, (int64_t)1 << lg, J.cmin, J.cmax, J.off, J.out, J.nout, J.flags, err,
-                     *reinterpret_cast<CrtSmem*>(sm));
+            const uint32_t nb = (uint32_t)((J.nout + 1 + CRT_BLK - 1) / CRT_BLK);
+            for (uint32_t k = idx * PERSIST_CRT; k < nb && k < (idx + 1) * PERSIST_CRT; ++k) {
+                crt_body(k, J.ws, (int64_t)1 << lg, J.cmin, J.cmax, J.off, J.out, J.nout, J.flags, err,
+                         *reinterpret_cast<CrtSmem*>(sm));
+                __syncthreads();
+            }
             break;
         }
         default: break;
@@ -160,37 +172,43 @@ __device__ __forceinline__ void persist_item(uint32_t kind, uint32_t job, uint32
 // LOOP: persistent CTAs (grid = what fits on the device) take items until
 // the queue is empty; otherwise one item per CTA (grid = the item count),
 // in the same queue order.
+#ifndef PERSIST_MINB
+#define PERSIST_MINB 4             // resident CTAs per SM the register budget is set for
+#endif
 template <bool LOOP>
-__global__ void __launch_bounds__(PERSIST_THREADS, 4)
+__global__ void __launch_bounds__(PERSIST_THREADS, PERSIST_MINB)
     k_persist(const PItem* __restrict__ items, int nitems, const JobDesc* __restrict__ jobs,
               const PClass* __restrict__ cls, uint32_t* state, const uint2* __restrict__ twf,
               const uint2* __restrict__ twi, uint32_t* err) {
     extern __shared__ uint32_t sm[];
-    // the held items and the current one, in shared memory so that nothing of
-    // them stays live in registers across the stage bodies
-    constexpr int GRAB = LOOP ? PERSIST_GRAB : 1;
-    __shared__ PItem s_q[GRAB];
-    __shared__ PItem s_it;
-    __shared__ int s_more, s_k, s_n;
-    if (threadIdx.x == 0) s_k = s_n = 0;
+    // the current item and the next one, in shared memory so that nothing of
+    // them stays live in registers across the stage bodies.  A persistent
+    // CTA takes its next item (queue-head increment and item load) at the
+    // start of the current one, so those round trips overlap the body; it
+    // runs the two in queue order, so the waits' progress argument holds.
+    __shared__ PItem s_it, s_nx;
+    __shared__ int s_more, s_hasnx;
+    if (threadIdx.x == 0) {
+        const int it = (int)atomicAdd(&state[0], 1u);
+        s_hasnx = it < nitems;
+        if (it < nitems) s_nx = items[it];
+    }
     do {
         if (threadIdx.x == 0) {
-            if (s_k == s_n) {                   // take the next block of tickets
-                const int base = (int)atomicAdd(&state[0], (uint32_t)GRAB);
-                const int n = max(0, min(GRAB, nitems - base));
-                for (int i = 0; i < n; ++i) s_q[i] = items[base + i];
-                s_n = n;
-                s_k = 0;
-            }
-            s_more = s_k < s_n;
+            s_more = s_hasnx;
             if (s_more) {
-                const PItem I = s_q[s_k++];
+                const PItem I = s_nx;
                 s_it = I;
                 if (I.need) persist_wait(&state[1 + I.job], I.need, err);
             }
         }
         __syncthreads();
         if (!s_more) return;
+        if (LOOP && PERSIST_PREFETCH && threadIdx.x == 0) {
+            const int it = (int)atomicAdd(&state[0], 1u);
+            s_hasnx = it < nitems;
+            if (it < nitems) s_nx = items[it];
+        }
         // warp-uniform copies (a warp reduction's result), so that the
         // bodies' index arithmetic stays on the uniform datapath
         const uint32_t kind = __reduce_max_sync(0xffffffffu, (uint32_t)s_it.kind);
@@ -198,7 +216,14 @@ __global__ void __launch_bounds__(PERSIST_THREADS, 4)
         persist_item(kind, job, __reduce_max_sync(0xffffffffu, (uint32_t)s_it.lg),
                      __reduce_max_sync(0xffffffffu, s_it.idx), jobs, cls, twf, twi, err, sm);
         __syncthreads();
-        if (threadIdx.x == 0 && kind != PK_SCHOOL && kind != PK_SMALLJOB) persist_signal(&state[1 + job]);
+        if (threadIdx.x == 0) {
+            if (kind != PK_SCHOOL && kind != PK_SMALLJOB) persist_signal(&state[1 + job]);
+            if (LOOP && !PERSIST_PREFETCH) {
+                const int it = (int)atomicAdd(&state[0], 1u);
+                s_hasnx = it < nitems;
+                if (it < nitems) s_nx = items[it];
+            }
+        }
     } while (LOOP);
 }
 

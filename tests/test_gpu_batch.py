@@ -181,3 +181,31 @@ def test_persistent_queue_on_a_mixed_size_batch(ctx, wave_mb):
             want = O.port_sqr(a) if kind == sbg.JOB_SQR else O.port_mul(a, bb)
             assert np.array_equal(got, want), (rep, kind, an, bn)
     b.close()
+
+
+def test_engine_autotune_keeps_products_exact(ctx):
+    """sbg_batch_autotune times the three engines on the batch and keeps the
+    fastest; the products it leaves behind, and those of the captured graph
+    on the chosen engine, equal the oracle's."""
+    import simd_bigint_b200 as sbg
+    rng = np.random.default_rng(306)
+    shapes = _shapes(rng, 60)
+    jobs, keep = _mixed_jobs(rng, shapes)
+    b = sbg.Batch(ctx, jobs)
+    ms = b.autotune()
+    assert len(ms) == 3 and all(m > 0 for m in ms)
+    b.capture()
+    for *_, tr in keep:
+        tr.fill_(-1)
+    b.run()
+    ctx.sync()
+    for (kind, a, bb, ta, tb, tr), (_, _, _, _, an, bn) in zip(keep, jobs):
+        got = tr.cpu().numpy().view(np.uint64)
+        if kind == sbg.JOB_MUL:
+            want = O.port_mul(a, bb)
+        elif kind == sbg.JOB_SQR:
+            want = O.port_sqr(a)
+        else:
+            want = O.mulmid(a, bb, "ntt")
+        assert np.array_equal(got, want), (kind, an, bn)
+    b.close()
