@@ -1401,7 +1401,7 @@ def run_extras(args, ws, rank, local, pg) -> dict:
             "engine": b.get("engine"), "engines": b.get("engines"), "config": b["config"]["workload"],
             "steps": ab.steps}
     asv = copy.copy(args)
-    asv.requests, asv.sweep_requests, asv.serve_fracs = 20000, 6000, (0.6,)
+    asv.requests, asv.sweep_requests, asv.serve_fracs = 60000, 10000, (0.6,)
     asv.warmup = 3
     sv = run_serve(asv, ws, rank, local, pg)
     if sv is not None:

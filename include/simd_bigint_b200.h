@@ -168,13 +168,14 @@ int sbg_batch_capture(sbg_batch *batch);
 int sbg_batch_run(sbg_batch *batch);
 /* Waits for queued runs, then frees. */
 void sbg_batch_destroy(sbg_batch *batch);
-/* Batch engine.  0 (default): ONE persistent kernel whose CTAs take work
- * items -- (job, stage, tile) -- from a queue in device memory, waiting on
- * per-job progress counters between a job's stages; it runs the schoolbook,
+/* Batch engine.  0: ONE persistent kernel whose CTAs take work items --
+ * (job, stage, tile) -- from a queue in device memory, waiting on per-job
+ * progress counters between a job's stages; it runs the schoolbook,
  * single-CTA and power-of-two four-step classes up to 2^20 points (longer
- * and 3 * 2^k classes keep per-class launches beside it).  1: one launch per
- * stage per length class for every class.  2: the same queue and kernel,
- * one CTA per item instead of persistent CTAs.  wave_bytes (0: keep the
+ * and 3 * 2^k classes keep per-class launches beside it).  1 (default): one
+ * launch per stage per length class for every class, the classes on forked
+ * streams.  2: the same queue and kernel as 0, one CTA per item instead of
+ * persistent CTAs.  sbg_batch_autotune picks one by timing.  wave_bytes (0: keep the
  * current, default 64 MB) bounds the transform workspace of the jobs whose
  * stages the queue interleaves (L2 blocking).  Drops a captured graph:
  * capture again.  No counterpart in the reference. */

@@ -374,9 +374,9 @@ class Batch:
         _check(self._L.sbg_batch_capture(self.handle), "sbg_batch_capture")
 
     def set_engine(self, engine: int, wave_bytes: int = 0):
-        """0: the persistent kernel over a device work-item queue (default),
-        1: one launch per stage per length class, 2: the queue with one CTA
-        per item.  wave_bytes: the queue's L2 blocking (0: keep).  Drops a
+        """0: the persistent kernel over a device work-item queue, 1: one
+        launch per stage per length class (default), 2: the queue with one
+        CTA per item.  wave_bytes: the queue's L2 blocking (0: keep).  Drops a
         captured graph (capture again)."""
         _check(self._L.sbg_batch_set_engine(self.handle, engine, wave_bytes), "sbg_batch_set_engine")
 
