@@ -139,7 +139,10 @@ __device__ __forceinline__ uint32_t fs_value(const FsTables& fs, int q, uint32_t
 //  * column pairs (longer columns, M up to 2^10, W = 2^13 / M): a thread owns
 //    two adjacent columns of one group, so one twiddle load serves two
 //    butterflies and the global accesses are 16-byte (two limbs) or 8-byte
-//    (two residues) row pieces; planes padded one word per 16.
+//    (two residues) row pieces.  The pair's two columns sit side by side in
+//    shared memory (one 8-byte word per row, planes padded one word per
+//    16 rows), so every shared-memory and distributed-shared-memory access
+//    moves both columns in one 64-bit instruction.
 // Columns of more than 2^10 rows (transform lengths 2^23..2^25) are split
 // over a thread-block cluster of C = N1 / 2^10 CTAs, one slab of 2^10 rows
 // each, exchanging through distributed shared memory: the top lg C DIF levels
@@ -175,8 +178,10 @@ __host__ __device__ constexpr int col_lgw(int lgN1) { return col_lgw_of(col_lane
 // single-CTA 3 * 2^m columns (m <= SBG_COL3S_MAX): W = 2^(12 - m) columns of 3 * 2^m rows
 #define SBG_COL3S_MAX 7
 __host__ __device__ constexpr int col3s_lgw(int m) { return 12 - m; }
-// Plane strides: lanes, M + 1 (odd); pairs, padded length + 32/W, so that a
-// warp's W/2 column pairs x 64/W consecutive rows fall in distinct banks.
+// Plane strides: lanes, M + 1 words (odd); pairs, padded length + 32/W
+// 8-byte words, so that each half-warp's W/2 column pairs x 32/W consecutive
+// rows (a 64-bit access is served half a warp at a time) fall in distinct
+// bank pairs.
 __host__ __device__ constexpr int col_ld_of(bool lanes, int lgs) {
     return lanes ? (1 << lgs) + 1 : padded_len(1 << lgs) + (32 >> col_lgw_of(false, lgs));
 }
@@ -284,12 +289,12 @@ __device__ __forceinline__ void col_pass_pair(uint32_t* sm, const uint64_t* __re
                 }
             }
         } else {
-            const uint32_t* s0 = sm + g0 * LD;
+            const uint2* s0 = reinterpret_cast<const uint2*>(sm) + cp * LD;
 #pragma unroll
             for (int t = 0; t < R; ++t) {
-                const int a = padded_at<LGST>(i0, t);
-                x[t] = s0[a];
-                y[t] = s0[LD + a];
+                const uint2 v = s0[padded_at<LGST>(i0, t)];
+                x[t] = v.x;
+                y[t] = v.y;
             }
         }
         if constexpr (FWD)
@@ -304,13 +309,9 @@ __device__ __forceinline__ void col_pass_pair(uint32_t* sm, const uint64_t* __re
                 *reinterpret_cast<uint2*>(Y + n) = make_uint2(x[t], y[t]);
             }
         } else {
-            uint32_t* s0 = sm + g0 * LD;
+            uint2* s0 = reinterpret_cast<uint2*>(sm) + cp * LD;
 #pragma unroll
-            for (int t = 0; t < R; ++t) {
-                const int a = padded_at<LGST>(i0, t);
-                s0[a] = x[t];
-                s0[LD + a] = y[t];
-            }
+            for (int t = 0; t < R; ++t) s0[padded_at<LGST>(i0, t)] = make_uint2(x[t], y[t]);
         }
     }
 }
@@ -455,6 +456,25 @@ __device__ __forceinline__ void cluster_barrier() {
     asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
+// Distributed shared memory by explicit shared::cluster accesses: the
+// address of this CTA's shared word p in the shared memory of cluster CTA
+// `rank`, and 64-bit stores and loads there.
+__device__ __forceinline__ uint32_t dsmem_addr(const void* p, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n"
+                 : "=r"(r)
+                 : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void dsmem_st2(uint32_t a, uint32_t x, uint32_t y) {
+    asm volatile("st.shared::cluster.v2.u32 [%0], {%1, %2};\n" ::"r"(a), "r"(x), "r"(y) : "memory");
+}
+__device__ __forceinline__ uint2 dsmem_ld2(uint32_t a) {
+    uint2 v;
+    asm volatile("ld.shared::cluster.v2.u32 {%0, %1}, [%2];\n" : "=r"(v.x), "=r"(v.y) : "r"(a) : "memory");
+    return v;
+}
+
 // Cluster levels (forward): this CTA's share of the radix-C groups
 // {r + M t : t < C}, rows r in [slab * M / C, (slab + 1) * M / C) of every
 // column pair, read from global, DIF'd, and scattered into the owning slabs.
@@ -472,26 +492,21 @@ __device__ __forceinline__ void col_cross_fwd(uint32_t* sm, const uint64_t* __re
     constexpr int TOTAL = RPS << (LGW - 1);
     static_assert(TOTAL % COL_THREADS == 0, "cluster groups must fill the CTA");
     constexpr int ITER = TOTAL / COL_THREADS;
-    cg::cluster_group cl = cg::this_cluster();
     const bool al16 = (reinterpret_cast<uintptr_t>(X) & 15) == 0;
 #pragma unroll
     for (int it = 0; it < ITER; ++it) {
         const int gid = threadIdx.x + it * COL_THREADS;
-        const int g0 = 2 * (gid & ((1 << (LGW - 1)) - 1));
+        const int cp = gid & ((1 << (LGW - 1)) - 1);
         const int r = slab * RPS + (gid >> (LGW - 1));
         uint32_t x[C], y[C];
-        const int64_t n0 = ((int64_t)r << SBG_ROW_LG) + c0 + g0;
+        const int64_t n0 = ((int64_t)r << SBG_ROW_LG) + c0 + 2 * cp;
 #pragma unroll
         for (int t = 0; t < C; ++t)
             load_limb_pair(X, xn, n0 + ((int64_t)(M * t) << SBG_ROW_LG), al16, pc, x[t], y[t]);
         dif_regs2<C>(x, y, tw, r, M, LGN1, pc.p);
-        const int a = g0 * LD + pad_idx(r);
+        const uint2* a = reinterpret_cast<const uint2*>(sm) + cp * LD + pad_idx(r);
 #pragma unroll
-        for (int t = 0; t < C; ++t) {
-            uint32_t* d = cl.map_shared_rank(sm, t);
-            d[a] = x[t];
-            d[a + LD] = y[t];
-        }
+        for (int t = 0; t < C; ++t) dsmem_st2(dsmem_addr(a, t), x[t], y[t]);
     }
 }
 
@@ -510,22 +525,21 @@ __device__ __forceinline__ void col_cross_inv(uint32_t* sm, uint32_t* __restrict
     constexpr int TOTAL = RPS << (LGW - 1);
     static_assert(TOTAL % COL_THREADS == 0, "cluster groups must fill the CTA");
     constexpr int ITER = TOTAL / COL_THREADS;
-    cg::cluster_group cl = cg::this_cluster();
 #pragma unroll
     for (int it = 0; it < ITER; ++it) {
         const int gid = threadIdx.x + it * COL_THREADS;
-        const int g0 = 2 * (gid & ((1 << (LGW - 1)) - 1));
+        const int cp = gid & ((1 << (LGW - 1)) - 1);
         const int r = slab * RPS + (gid >> (LGW - 1));
         uint32_t x[C], y[C];
-        const int a = g0 * LD + pad_idx(r);
+        const uint2* a = reinterpret_cast<const uint2*>(sm) + cp * LD + pad_idx(r);
 #pragma unroll
         for (int t = 0; t < C; ++t) {
-            const uint32_t* s = cl.map_shared_rank(sm, t);
-            x[t] = s[a];
-            y[t] = s[a + LD];
+            const uint2 v = dsmem_ld2(dsmem_addr(a, t));
+            x[t] = v.x;
+            y[t] = v.y;
         }
         dit_regs2<C>(x, y, tw, r, M, LGN1, pc.p);
-        const int64_t n0 = ((int64_t)r << SBG_ROW_LG) + c0 + g0;
+        const int64_t n0 = ((int64_t)r << SBG_ROW_LG) + c0 + 2 * cp;
 #pragma unroll
         for (int t = 0; t < C; ++t)
             *reinterpret_cast<uint2*>(Y + n0 + ((int64_t)(M * t) << SBG_ROW_LG)) = make_uint2(x[t], y[t]);
@@ -693,10 +707,11 @@ __host__ __device__ constexpr int col3_smem_bytes(int m) {
 __host__ __device__ constexpr int col3_ntiles(int m) { return 1 << (SBG_ROW_LG - col3_lgw(m)); }
 #define SBG_COL3_CASES(X) X(8) X(9) X(10) X(11)
 
-// shared-memory address of (column, row) in a slab's planes
+// shared-memory word of (column, row) in a slab's planes (column pairs: the
+// pair's plane of 8-byte words, the column's half of the row's word)
 template <bool LANES, int LD>
 __device__ __forceinline__ int slab_addr(int col, int r) {
-    return col * LD + (LANES ? r : pad_idx(r));
+    return LANES ? col * LD + r : (col >> 1) * (2 * LD) + 2 * pad_idx(r) + (col & 1);
 }
 
 // cross-slab levels, forward: this CTA's share of rows r of a slab (split
