@@ -162,8 +162,18 @@ __device__ __forceinline__ uint32_t fs_value(const FsTables& fs, int q, uint32_t
 #endif
 #define SBG_COL_LANE_MAX_LG 8
 #define COL_THREADS 256
+// resident CTAs per SM the register budget is set for: forward columns 5
+// (48 registers; their cross-slab loads wait longest, and more CTAs hide
+// them: 2^25 points 1.28 -> 1.21 ms against 4), inverse columns 4 (64
+// registers; at 5 they spill and slow down)
 #ifndef COL_MINB
 #define COL_MINB 4
+#endif
+#ifndef COL_FWD_MINB
+#define COL_FWD_MINB 5
+#endif
+#ifndef COL3_FWD_MINB
+#define COL3_FWD_MINB COL_MINB
 #endif
 __host__ __device__ constexpr bool col_lanes(int lgN1) { return lgN1 <= SBG_COL_LANE_MAX_LG; }
 __host__ __device__ constexpr int col_lgc(int lgN1) {
@@ -578,7 +588,7 @@ __device__ __forceinline__ void col_fwd_body(int q, int tile, int slab, int op,
 // Block order: cluster slab fastest, then prime, so the five primes' CTAs of
 // one tile run together and share its limbs through L2.
 template <int LGN1>
-__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col_fwd(const uint64_t* __restrict__ a, int64_t an,
+__global__ void __launch_bounds__(COL_THREADS, COL_FWD_MINB) k_col_fwd(const uint64_t* __restrict__ a, int64_t an,
                                                     const uint64_t* __restrict__ b, int64_t bn,
                                                     const uint2* __restrict__ twf,
                                                     uint32_t* __restrict__ YA,
@@ -595,7 +605,7 @@ __global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col_fwd(const uint64_
 // batched: blocks (job, operand, tile, prime, slab), job slowest; the second
 // operand's blocks of a squaring exit at once (whole clusters together)
 template <int LGN1>
-__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col_fwd_b(const JobDesc* __restrict__ jobs,
+__global__ void __launch_bounds__(COL_THREADS, COL_FWD_MINB) k_col_fwd_b(const JobDesc* __restrict__ jobs,
                                                       const uint2* __restrict__ twf) {
     constexpr int LGC = col_lgc(LGN1);
     constexpr int NTILES = col_ntiles(LGN1);
@@ -904,7 +914,7 @@ __device__ __forceinline__ void col3s_inv_body(int q, int tile, uint32_t* __rest
 
 // blocks: prime fastest, then tile, operand
 template <int M3>
-__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3s_fwd(const uint64_t* __restrict__ a, int64_t an,
+__global__ void __launch_bounds__(COL_THREADS, COL3_FWD_MINB) k_col3s_fwd(const uint64_t* __restrict__ a, int64_t an,
                                                                    const uint64_t* __restrict__ b, int64_t bn,
                                                                    const uint2* __restrict__ twf, Radix3Arg r3,
                                                                    uint32_t* __restrict__ YA,
@@ -916,7 +926,7 @@ __global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3s_fwd(const uint6
 }
 
 template <int M3>
-__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3s_fwd_b(const JobDesc* __restrict__ jobs,
+__global__ void __launch_bounds__(COL_THREADS, COL3_FWD_MINB) k_col3s_fwd_b(const JobDesc* __restrict__ jobs,
                                                                      const uint2* __restrict__ twf, Radix3Arg r3) {
     constexpr int NTILES = col3s_ntiles(M3);
     constexpr int PER_JOB = SBG_NP * 2 * NTILES;
@@ -948,7 +958,7 @@ __global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3s_inv_b(const Job
 
 // blocks: slab fastest (a cluster), then prime, tile, operand
 template <int M3>
-__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3_fwd(const uint64_t* __restrict__ a, int64_t an,
+__global__ void __launch_bounds__(COL_THREADS, COL3_FWD_MINB) k_col3_fwd(const uint64_t* __restrict__ a, int64_t an,
                                                                   const uint64_t* __restrict__ b, int64_t bn,
                                                                   const uint2* __restrict__ twf, Radix3Arg r3,
                                                                   uint32_t* __restrict__ YA,
@@ -963,7 +973,7 @@ __global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3_fwd(const uint64
 }
 
 template <int M3>
-__global__ void __launch_bounds__(COL_THREADS, COL_MINB) k_col3_fwd_b(const JobDesc* __restrict__ jobs,
+__global__ void __launch_bounds__(COL_THREADS, COL3_FWD_MINB) k_col3_fwd_b(const JobDesc* __restrict__ jobs,
                                                                     const uint2* __restrict__ twf, Radix3Arg r3) {
     constexpr int C = col3_csize(M3);
     constexpr int NTILES = col3_ntiles(M3);
@@ -1737,6 +1747,7 @@ static cudaError_t launch_col(void (*kern)(KArgs...), int lgN1, int64_t blocks, 
                               Args... args) {
     return launch_colx(kern, blocks, col_smem_bytes(lgN1), 1 << col_lgc(lgN1), st, args...);
 }
+
 
 static Radix3Arg radix3_arg(const LenPlan* lp, bool inverse) {
     Radix3Arg r{};
