@@ -1299,17 +1299,23 @@ __device__ __forceinline__ void sum3(uint64_t lo, uint64_t mid, uint32_t hi, uin
     k += y < s1;
 }
 
-struct CrtSmem {
-    ulonglong2 z[CRT_BLK / 2];                  // limbs before carries
-    uint32_t gp[CRT_T / 32][CRT_NSTEP][2];      // per warp and step: g, p
+// NSTEP: steps of 128 limbs per warp (a block covers 8 * 128 * NSTEP limbs)
+template <int NSTEP>
+struct CrtSmemT {
+    ulonglong2 z[(CRT_T / 32) * 32 * CRT_V * NSTEP / 2];   // limbs before carries
+    uint32_t gp[CRT_T / 32][NSTEP][2];                     // per warp and step: g, p
     uint32_t warp[CRT_T / 32];
     uint32_t cin;
 };
+using CrtSmem = CrtSmemT<CRT_NSTEP>;
 
-__device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restrict__ R, int64_t L,
-                                         int64_t cmin, int64_t cmax, int64_t off,
-                                         uint64_t* __restrict__ out, int64_t nout,
-                                         uint32_t* flags, uint32_t* err, CrtSmem& S) {
+template <int NSTEP>
+__device__ __forceinline__ void crt_body_t(uint32_t bid, const uint32_t* __restrict__ R, int64_t L,
+                                           int64_t cmin, int64_t cmax, int64_t off,
+                                           uint64_t* __restrict__ out, int64_t nout,
+                                           uint32_t* flags, uint32_t* err, CrtSmemT<NSTEP>& S) {
+    constexpr int SEG = 32 * CRT_V * NSTEP;                // limbs per warp
+    constexpr int BLK = (CRT_T / 32) * SEG;                // limbs per block
     ulonglong2* s_z = S.z;
     auto& s_gp = S.gp;
     uint32_t* s_warp = S.warp;
@@ -1317,7 +1323,7 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int src1 = (lane + 31) & 31;
-    const int64_t seg = (int64_t)bid * CRT_BLK + (int64_t)wid * CRT_SEG;
+    const int64_t seg = (int64_t)bid * BLK + (int64_t)wid * SEG;
     const uint32_t inj = *(volatile uint32_t*)&g_inject;
     // injected residue corruption: the top coefficient (the product then
     // spills) or a middle one (a wrong product no device check sees)
@@ -1326,7 +1332,7 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
             ((inj & SBG_INJECT_MID) && j == cmin + (cmax - cmin) / 2))
             r0 ^= 1u;
     };
-    ulonglong2* zs = s_z + wid * (CRT_SEG / 2);         // unit (2 s + half) * 32 + lane
+    ulonglong2* zs = s_z + wid * (SEG / 2);         // unit (2 s + half) * 32 + lane
     // residues of the coefficients j = m + off of limbs m .. m+3; zero outside
     // [cmin, cmax], which Garner maps to lo = mid = hi = 0
     auto fetch4 = [&](int64_t m, uint32_t (&r)[CRT_V][SBG_NP]) {
@@ -1383,7 +1389,7 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
     // a runtime loop: each step holds four Garner reconstructions, and
     // unrolling the steps quadruples the code the warps fetch
 #pragma unroll 1
-    for (int s = 0; s < CRT_NSTEP; ++s) {
+    for (int s = 0; s < NSTEP; ++s) {
         const int64_t m0 = seg + 128 * s + 4 * lane;
         uint32_t r[CRT_V][SBG_NP];
         fetch4(m0, r);
@@ -1524,7 +1530,7 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
     uint32_t cin = (wpre & 1u) | ((wpre >> 1) & s_cin);
     const bool al16 = (reinterpret_cast<uintptr_t>(out) & 15) == 0;
 #pragma unroll
-    for (int s = 0; s < CRT_NSTEP; ++s) {
+    for (int s = 0; s < NSTEP; ++s) {
         const uint32_t g = s_gp[wid][s][0], p = s_gp[wid][s][1];
         const uint64_t sum = (uint64_t)p + ((g << 1) | cin);
         const uint32_t c = (((uint32_t)sum ^ p) >> lane) & 1u;
@@ -1553,6 +1559,13 @@ __device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restric
 
 // Block order comes from an atomic ticket (flags[0]), not blockIdx, so every
 // block's look-back predecessors were scheduled before it.
+__device__ __forceinline__ void crt_body(uint32_t bid, const uint32_t* __restrict__ R, int64_t L,
+                                         int64_t cmin, int64_t cmax, int64_t off,
+                                         uint64_t* __restrict__ out, int64_t nout,
+                                         uint32_t* flags, uint32_t* err, CrtSmem& S) {
+    crt_body_t<CRT_NSTEP>(bid, R, L, cmin, cmax, off, out, nout, flags, err, S);
+}
+
 __global__ void __launch_bounds__(CRT_T, CRT_MINB) k_crt_carry(const uint32_t* __restrict__ R, int64_t L,
                                                      int64_t cmin, int64_t cmax, int64_t off,
                                                      uint64_t* __restrict__ out, int64_t nout,
@@ -1562,6 +1575,26 @@ __global__ void __launch_bounds__(CRT_T, CRT_MINB) k_crt_carry(const uint32_t* _
     __syncthreads();
     __shared__ CrtSmem S;
     crt_body(s_bid, R, L, cmin, cmax, off, out, nout, flags, err, S);
+}
+
+// Short single products: one step of 128 limbs per warp (1024 limbs a
+// block), four times the blocks of k_crt_carry, so a short carry scan is
+// spread over more SMs (16384 x 16384 limbs: 14.7 -> 10.3 us); long ones
+// keep four steps, which fetch and compose fewer neighbour terms per limb.
+#define CRT_SHORT_NSTEP 1
+#define CRT_SHORT_BLK ((CRT_T / 32) * 32 * CRT_V * CRT_SHORT_NSTEP)
+#ifndef CRT_SHORT_MAX
+#define CRT_SHORT_MAX (1 << 17)                 // product limbs up to which the short scan runs
+#endif
+__global__ void __launch_bounds__(CRT_T, CRT_MINB) k_crt_carry_s(const uint32_t* __restrict__ R, int64_t L,
+                                                       int64_t cmin, int64_t cmax, int64_t off,
+                                                       uint64_t* __restrict__ out, int64_t nout,
+                                                       uint32_t* flags, uint32_t* err) {
+    __shared__ uint32_t s_bid;
+    if (threadIdx.x == 0) s_bid = atomicAdd(&flags[0], 1u);
+    __syncthreads();
+    __shared__ CrtSmemT<CRT_SHORT_NSTEP> S;
+    crt_body_t<CRT_SHORT_NSTEP>(s_bid, R, L, cmin, cmax, off, out, nout, flags, err, S);
 }
 
 // batched: blocks_per_job CTAs per job (enough for the longest output of the
@@ -1959,7 +1992,14 @@ cudaError_t launch_batch_class(const JobDesc* djobs, int njobs, int lgL, const L
     return cudaGetLastError();
 }
 
-size_t carry_flag_words(int64_t nout) { return 1 + (size_t)((nout + CRT_BLK) / CRT_BLK) + 1; }
+// ticket + one flag per block + the error word's slot, for either block
+// size; monotone in nout, so a workspace reserved for a product length
+// covers every shorter one
+size_t carry_flag_words(int64_t nout) {
+    const int64_t nshort = nout < CRT_SHORT_MAX ? nout : CRT_SHORT_MAX;
+    const int64_t b = std::max((nshort + CRT_SHORT_BLK) / CRT_SHORT_BLK, (nout + CRT_BLK) / CRT_BLK);
+    return 1 + (size_t)b + 1;
+}
 
 cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int64_t cmin,
                              int64_t cmax, int64_t off, uint64_t* out, int64_t nout,
@@ -1967,11 +2007,16 @@ cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int6
                              KTimer* kt) {
     (void)lp;
     // blocks cover limbs [0, nout] (limb nout is the spill check)
-    int64_t nblk = (nout + 1 + CRT_BLK - 1) / CRT_BLK;
+    const bool shortp = nout <= CRT_SHORT_MAX;
+    const int64_t blk = shortp ? CRT_SHORT_BLK : CRT_BLK;
+    int64_t nblk = (nout + 1 + blk - 1) / blk;
     cudaError_t e = cudaMemsetAsync(flags, 0, (1 + nblk) * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     KT_BEGIN(kt, KID_CRT, st);
-    k_crt_carry<<<(unsigned)nblk, CRT_T, 0, st>>>(R, code_len(lgL), cmin, cmax, off, out, nout, flags, err);
+    if (shortp)
+        k_crt_carry_s<<<(unsigned)nblk, CRT_T, 0, st>>>(R, code_len(lgL), cmin, cmax, off, out, nout, flags, err);
+    else
+        k_crt_carry<<<(unsigned)nblk, CRT_T, 0, st>>>(R, code_len(lgL), cmin, cmax, off, out, nout, flags, err);
     KT_END(kt, KID_CRT, st);
     return cudaGetLastError();
 }
