@@ -282,13 +282,18 @@ __device__ __forceinline__ void col_pass_pair(uint32_t* sm, const uint64_t* __re
         const int i0 = (blk << LGM) + j0;
         const int g0 = 2 * cp;
         uint32_t x[R], y[R];
+        // first forward pass of a zero-padded operand: its upper half rows are empty
+        bool hz = false;
         if constexpr (SRC_G) {
             const int64_t n0 = ((int64_t)(i0 + row0) << SBG_ROW_LG) + c0 + g0;
             if constexpr (FWD) {
                 const bool al16 = (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+                if constexpr (K == 0 && R >= 2) hz = n0 + ((int64_t)(ST * (R / 2)) << SBG_ROW_LG) >= xn;
 #pragma unroll
-                for (int t = 0; t < R; ++t)
+                for (int t = 0; t < R; ++t) {
+                    if (hz && t >= R / 2) break;
                     load_limb_pair(X, xn, n0 + ((int64_t)(ST * t) << SBG_ROW_LG), al16, pc, x[t], y[t]);
+                }
             } else {
 #pragma unroll
                 for (int t = 0; t < R; ++t) {
@@ -307,10 +312,16 @@ __device__ __forceinline__ void col_pass_pair(uint32_t* sm, const uint64_t* __re
                 y[t] = v.y;
             }
         }
-        if constexpr (FWD)
+        if constexpr (FWD && SRC_G && K == 0) {
+            if (hz)
+                dif_regs2<R, ST == 1, true>(x, y, tw, j0, ST, LGM, p);
+            else
+                dif_regs2<R, ST == 1>(x, y, tw, j0, ST, LGM, p);
+        } else if constexpr (FWD) {
             dif_regs2<R, ST == 1>(x, y, tw, j0, ST, LGM, p);
-        else
+        } else {
             dit_regs2<R, ST == 1>(x, y, tw, j0, ST, LGM, p);
+        }
         if constexpr (DST_G) {
             const int64_t n0 = ((int64_t)(i0 + row0) << SBG_ROW_LG) + c0 + g0;
 #pragma unroll
@@ -362,10 +373,14 @@ __device__ __forceinline__ void col_pass_lane(uint32_t* sm, const uint64_t* __re
         const int j0 = grp & (ST - 1);
         const int i0 = ((gid >> LGT1) << LGS) + ((grp >> LGST) << LGM) + j0;
         uint32_t x[R];
+        // first forward pass of a zero-padded operand: its upper half rows are empty
+        bool hz = false;
         if constexpr (SRC_G) {
             const int64_t n0 = ((int64_t)(i0 + row0) << SBG_ROW_LG) + c0 + col;
+            if constexpr (FWD && K == 0 && NSUB == 1) hz = n0 + ((int64_t)(ST * (R / 2)) << SBG_ROW_LG) >= xn;
 #pragma unroll
             for (int t = 0; t < R; ++t) {
+                if (hz && t >= R / 2) break;
                 const int64_t n = n0 + ((int64_t)(ST * t) << SBG_ROW_LG);
                 if constexpr (FWD)
                     x[t] = load_limb(X, xn, n, pc);
@@ -377,10 +392,16 @@ __device__ __forceinline__ void col_pass_lane(uint32_t* sm, const uint64_t* __re
 #pragma unroll
             for (int t = 0; t < R; ++t) x[t] = s0[ST * t];
         }
-        if constexpr (FWD)
+        if constexpr (FWD && SRC_G && K == 0 && NSUB == 1) {
+            if (hz)
+                dif_regs<R, ST == 1, true>(x, tw, j0, ST, LGM, p);
+            else
+                dif_regs<R, ST == 1>(x, tw, j0, ST, LGM, p);
+        } else if constexpr (FWD) {
             dif_regs<R, ST == 1>(x, tw, j0, ST, LGM, p);
-        else
+        } else {
             dit_regs<R, ST == 1>(x, tw, j0, ST, LGM, p);
+        }
         if constexpr (DST_G) {
             const int64_t n0 = ((int64_t)(i0 + row0) << SBG_ROW_LG) + c0 + col;
 #pragma unroll
@@ -510,10 +531,19 @@ __device__ __forceinline__ void col_cross_fwd(uint32_t* sm, const uint64_t* __re
         const int r = slab * RPS + (gid >> (LGW - 1));
         uint32_t x[C], y[C];
         const int64_t n0 = ((int64_t)r << SBG_ROW_LG) + c0 + 2 * cp;
+        // a zero-padded operand (the usual case: an operand of at most half
+        // the transform) has nothing in rows r + M t, t >= C / 2
+        if (n0 + ((int64_t)(M * (C / 2)) << SBG_ROW_LG) >= xn) {
 #pragma unroll
-        for (int t = 0; t < C; ++t)
-            load_limb_pair(X, xn, n0 + ((int64_t)(M * t) << SBG_ROW_LG), al16, pc, x[t], y[t]);
-        dif_regs2<C>(x, y, tw, r, M, LGN1, pc.p);
+            for (int t = 0; t < C / 2; ++t)
+                load_limb_pair(X, xn, n0 + ((int64_t)(M * t) << SBG_ROW_LG), al16, pc, x[t], y[t]);
+            dif_regs2<C, false, true>(x, y, tw, r, M, LGN1, pc.p);
+        } else {
+#pragma unroll
+            for (int t = 0; t < C; ++t)
+                load_limb_pair(X, xn, n0 + ((int64_t)(M * t) << SBG_ROW_LG), al16, pc, x[t], y[t]);
+            dif_regs2<C>(x, y, tw, r, M, LGN1, pc.p);
+        }
         const uint2* a = reinterpret_cast<const uint2*>(sm) + cp * LD + pad_idx(r);
 #pragma unroll
         for (int t = 0; t < C; ++t) dsmem_st2(dsmem_addr(a, t), x[t], y[t]);

@@ -41,11 +41,19 @@ struct RLog {
 // forward DIF levels of one group (block size 2^lgM, stride st).  J0Z: the
 // caller's j0 is 0, so the butterflies at tin = 0 have the twiddle 1 and
 // skip the multiply (and the table load).
-template <int R, bool J0Z = false>
+// HZ: the upper half of the inputs is zero (see dif_regs2).
+template <int R, bool J0Z = false, bool HZ = false>
 __device__ __forceinline__ void dif_regs(uint32_t (&x)[R], const uint2* __restrict__ tw, int j0,
                                          int st, int lgM, uint32_t p) {
+    if constexpr (HZ) {
 #pragma unroll
-    for (int h = R / 2, l = 0; h >= 1; h >>= 1, ++l) {
+        for (int t = 0; t < R / 2; ++t) {
+            uint2 w = __ldg(&tw[tw_idx(lgM, j0 + st * t)]);
+            x[t + R / 2] = mul_shoup(x[t], w.x, w.y, p);
+        }
+    }
+#pragma unroll
+    for (int h = HZ ? R / 4 : R / 2, l = HZ ? 1 : 0; h >= 1; h >>= 1, ++l) {
 #pragma unroll
         for (int t = 0; t < R; ++t) {
             if (t & h) continue;
@@ -60,13 +68,23 @@ __device__ __forceinline__ void dif_regs(uint32_t (&x)[R], const uint2* __restri
     }
 }
 
-// two groups sharing (j0, st, lgM): one twiddle load serves both
-template <int R, bool J0Z = false>
+// two groups sharing (j0, st, lgM): one twiddle load serves both.  HZ: the
+// upper half of both groups' inputs is zero (a zero-padded operand), so the
+// first level is (u, 0) -> (u, u w): one multiply, no add or reduction.
+template <int R, bool J0Z = false, bool HZ = false>
 __device__ __forceinline__ void dif_regs2(uint32_t (&x)[R], uint32_t (&y)[R],
                                           const uint2* __restrict__ tw, int j0, int st, int lgM,
                                           uint32_t p) {
+    if constexpr (HZ) {
 #pragma unroll
-    for (int h = R / 2, l = 0; h >= 1; h >>= 1, ++l) {
+        for (int t = 0; t < R / 2; ++t) {
+            uint2 w = __ldg(&tw[tw_idx(lgM, j0 + st * t)]);
+            x[t + R / 2] = mul_shoup(x[t], w.x, w.y, p);
+            y[t + R / 2] = mul_shoup(y[t], w.x, w.y, p);
+        }
+    }
+#pragma unroll
+    for (int h = HZ ? R / 4 : R / 2, l = HZ ? 1 : 0; h >= 1; h >>= 1, ++l) {
 #pragma unroll
         for (int t = 0; t < R; ++t) {
             if (t & h) continue;
