@@ -558,8 +558,7 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
     clocks = ClockSampler(local)
     if rank == 0:
         clocks.start()
-    for _ in range(args.warmup):
-        batch.run()
+    batch.run()
     ctx.sync()
     # bit-exactness of the timed products: every job through the modular spot check
     got = d_out.cpu().numpy().view(np.uint64)
@@ -570,6 +569,10 @@ def run_batch(args, ws, rank, local, pg) -> dict | None:
         if not product_ok(a, b, got[ro:ro + an + bn]):
             exact = False
             break
+    # warm-up right before the timed region (the GPU has not idled)
+    for _ in range(args.warmup):
+        batch.run()
+    ctx.sync()
     if pg is not None:
         pg.barrier()
     torch.cuda.synchronize()
@@ -795,9 +798,8 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
     clocks = ClockSampler(local)
     if rank == 0:
         clocks.start()
-    warm = max(1, min(args.warmup, 2))
-    for _ in range(warm):
-        ctx.divrem_batch(jobs)
+    warm = max(1, args.warmup)
+    ctx.divrem_batch(jobs)
     # Q D + R == N (modulo 2^61-1 and 2^64-1) and R < D for every division
     exact = True
     for N, D, q, r in zip(hostN, hostD, tQ, tR):
@@ -810,6 +812,9 @@ def run_div(args, ws, rank, local, pg) -> dict | None:
         if len(hi) == 0 or R[hi[-1]] > D[hi[-1]]:
             exact = False
     steps = max(1, min(args.steps, 5))
+    # warm-up right before the timed region (the GPU has not idled)
+    for _ in range(warm):
+        ctx.divrem_batch(jobs)
     if pg is not None:
         pg.barrier()
     torch.cuda.synchronize()
@@ -1242,10 +1247,9 @@ def run_ours(args, ws, rank, local, pg) -> dict | None:
     clocks = ClockSampler(local)
     if rank == 0:
         clocks.start()
-    for _ in range(args.warmup):
-        step()
+    step()
     ctx.sync()
-    # bit-exactness of what is timed: the warm-up product against the
+    # bit-exactness of what is timed: the first product against the
     # reference's own digest for these operands, plus the modular checks
     # (2^61-1, 2^64-1, the low limb, and random primes from a logged seed)
     got = tr.cpu().numpy().view(np.uint64)
@@ -1260,6 +1264,11 @@ def run_ours(args, ws, rank, local, pg) -> dict | None:
               "spot_seed": spot_seed, "spot_primes": primes,
               "spot_ok": spot_check_primes(a, bb, got, primes)}
     exact = bool(parity["modular_2p61m1_2p64m1"] and parity["spot_ok"] and parity["reference_match"] is not False)
+    # the warm-up steps run after the host-side checks, right before the
+    # timed region, so it starts on a GPU that has not idled
+    for _ in range(args.warmup):
+        step()
+    ctx.sync()
 
     # ---- device-timed region (operands resident in HBM) ----
     if pg is not None:

@@ -6,7 +6,10 @@ command, for capturing them under a profiler:
 Cases (operands seeded, resident on cuda:0, each call repeated `repeats`
 times, 3 by default, so a capture can skip the first launch):
 
-    small     one 1500 x 1500-limb product (single-CTA transforms, k_small)
+    small     one 1500 x 1500-limb product (single-CTA transforms, k_small,
+              the short-product carry scan k_crt_carry_s)
+    mid       one 16384 x 16384-limb product (four-step kernels at 2^15
+              points, k_crt_carry_s)
     school    one 40 x 60-limb product (schoolbook warp, k_school)
     batch     a 512-product mixed batch on the per-class engine (k_*_b)
     persist   the same batch on the persistent queue kernel (k_persist)
@@ -57,8 +60,8 @@ def main(argv: list[str]) -> int:
     rng = np.random.default_rng(2027)
     ctx = sbg.Context(0)
     ok = True
-    if case in ("small", "school"):
-        an, bn = (1500, 1500) if case == "small" else (40, 60)
+    if case in ("small", "school", "mid"):
+        an, bn = {"small": (1500, 1500), "school": (40, 60), "mid": (16384, 16384)}[case]
         a, b = rng.integers(0, 2**64, an, dtype=np.uint64), rng.integers(0, 2**64, bn, dtype=np.uint64)
         ta, tb = _t(a), _t(b)
         r = torch.empty(an + bn, dtype=torch.int64, device="cuda")
