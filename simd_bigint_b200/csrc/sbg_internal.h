@@ -186,9 +186,12 @@ cudaError_t gen_len_tables(LenPlan* lp, cudaStream_t st);
 // ws_words(code) u32.  `err` is a device word that receives sticky error bits.
 // Every `lgL` below is a length code.
 size_t ws_words(int lgL, int sq);
+// b_ready (optional): an event the second operand's arrival is recorded
+// on; the first operand's forward transform does not wait for it.
 cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_t bn, int sq,
                         int lgL, const LenPlan* lp, const uint2* tw_f, const uint2* tw_i,
-                        uint32_t* ws, cudaStream_t st, KTimer* kt = nullptr);
+                        uint32_t* ws, cudaStream_t st, KTimer* kt = nullptr,
+                        cudaEvent_t b_ready = nullptr);
 // CRT + carry of residues R (5 x L u32) into out[0..nout): out[m] = limb (m + off)
 // of sum_{cmin <= j <= cmax} c_j * 2^(64 j).
 cudaError_t launch_crt_carry(const uint32_t* R, int lgL, const LenPlan* lp, int64_t cmin,
@@ -331,9 +334,12 @@ struct sbg_ctx {
     uint32_t* flags = nullptr;      // carry look-back flags
     size_t flags_cap = 0;
     uint32_t* err = nullptr;        // sticky device error bits
-    // staging for the host-pointer drop-ins
+    // staging for the host-pointer drop-ins, the stream their uploads run on
+    // and the events that mark each operand's arrival
     uint64_t* d_stage = nullptr;
     size_t stage_cap = 0;
+    cudaStream_t s_stage = nullptr;
+    cudaEvent_t stage_a = nullptr, stage_b = nullptr, stage_go = nullptr;
     sbg::EventTimer* timer = nullptr;    // non-null while kernel timing is on
     // queued product lists (Newton division): grow-only arena for the
     // transforms and carry flags, descriptor ring, forked streams

@@ -1824,8 +1824,15 @@ static Radix3Arg radix3_arg(const LenPlan* lp, bool inverse) {
 
 cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_t bn, int sq,
                         int lgL, const LenPlan* lp, const uint2* tw_f, const uint2* tw_i,
-                        uint32_t* ws, cudaStream_t st, KTimer* kt) {
+                        uint32_t* ws, cudaStream_t st, KTimer* kt, cudaEvent_t b_ready) {
     const size_t L = (size_t)code_len(lgL);
+    // the first operand's forward columns may start before the second
+    // operand has arrived only on the power-of-two four-step path
+    const bool split = b_ready && !sq && lgL > SBG_SMALL_MAX_LG && lp->m3 < 0;
+    if (b_ready && !split) {
+        cudaError_t e = cudaStreamWaitEvent(st, b_ready, 0);
+        if (e != cudaSuccess) return e;
+    }
     uint32_t* YA = ws;
     uint32_t* YB = ws + SBG_NP * L;
     ScaleArg sc;
@@ -1897,9 +1904,16 @@ cudaError_t launch_conv(const uint64_t* a, int64_t an, const uint64_t* b, int64_
     const int64_t col_blocks = ((int64_t)col_ntiles(lgN1) * SBG_NP) << col_lgc(lgN1);
     KT_BEGIN(kt, KID_COL_FWD, st);
     switch (lgN1) {
-#define SBG_LAUNCH_F(n)                                                                      \
-    case n:                                                                                  \
-        e = launch_col(k_col_fwd<n>, n, nops * col_blocks, st, a, an, b, bn, tw_f, YA, YB, nops); \
+#define SBG_LAUNCH_F(n)                                                                          \
+    case n:                                                                                      \
+        if (split) {                                                                             \
+            e = launch_col(k_col_fwd<n>, n, col_blocks, st, a, an, a, an, tw_f, YA, YA, 1);        \
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b_ready, 0);                        \
+            if (e == cudaSuccess)                                                                \
+                e = launch_col(k_col_fwd<n>, n, col_blocks, st, b, bn, b, bn, tw_f, YB, YB, 1);    \
+        } else {                                                                                 \
+            e = launch_col(k_col_fwd<n>, n, nops * col_blocks, st, a, an, b, bn, tw_f, YA, YB, nops); \
+        }                                                                                        \
         break;
         SBG_COL_CASES(SBG_LAUNCH_F)
 #undef SBG_LAUNCH_F
