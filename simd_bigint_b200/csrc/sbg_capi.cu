@@ -1054,6 +1054,7 @@ static int ensure_stage(sbg_ctx* c, size_t limbs) {
 static int dropin(uint64_t* rp, const uint64_t* ap, int64_t an, const uint64_t* bp, int64_t bn,
                   int sq) {
     if (!rp || !ap || an <= 0 || (!sq && (!bp || bn <= 0))) return 0;
+    if (an + (sq ? an : bn) - 1 > ((int64_t)1 << SBG_MAX_LG)) return 0;    // beyond the band
     sbg_ctx* c = default_ctx();
     if (!c) return 0;
     std::lock_guard<std::mutex> g(g_ctx_mu);
@@ -1087,7 +1088,6 @@ static int dropin(uint64_t* rp, const uint64_t* ap, int64_t an, const uint64_t* 
                 cudaEventRecord(c->stage_b, c->s_stage) != cudaSuccess ||
                 cudaStreamWaitEvent(c->stream, c->stage_a, 0) != cudaSuccess)
                 return 0;
-            if (an + bn - 1 > ((int64_t)1 << SBG_MAX_LG)) return 0;
             const int lgL = conv_lg(an + bn - 1, c->len3_mask);
             st = run_conv(c, dr, da, an, db, bn, 0, lgL, 0, an + bn - 2, 0, an + bn, c->stage_b);
         } else {

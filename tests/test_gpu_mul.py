@@ -127,6 +127,22 @@ def test_band_rejection(ctx):
     assert e.value.status == 1
 
 
+def test_dropin_band_rejection_then_exact_product(ctx):
+    """sbg_nt_mul returns 0 beyond the band (as the reference's nt_mul,
+    include/ntmul.h:50-57), before staging anything, and the next in-band
+    call on host arrays (the overlapped-upload path, >= 2^20 limbs) is exact."""
+    sbg = sbg_mod()
+    n = 1 << 24
+    a = np.zeros(n + 1, dtype=np.uint64)
+    r = np.zeros(2 * n + 2, dtype=np.uint64)
+    assert sbg.nt_mul(r, a, n + 1, a, n + 1) == 0
+    rng = np.random.default_rng(77)
+    x, y = rand_limbs(1 << 19, rng), rand_limbs((1 << 19) + 7, rng)
+    got = np.zeros(len(x) + len(y), dtype=np.uint64)
+    assert sbg.nt_mul(got, x, len(x), y, len(y)) == 1
+    assert spot_check(x, y, got)
+
+
 def _device_mul(ctx, a, b):
     import torch
     ta = torch.from_numpy(a.view(np.int64)).cuda()
