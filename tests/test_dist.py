@@ -63,6 +63,13 @@ def test_reference_arm_under_torchrun_two_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["cores"] >= 1
+    # the contract's keys, in the metric and unit of our own line for this workload
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["metric"] == "product Mlimb/s" and d["unit"] == "Mlimb/s" and d["higher_is_better"] is True
+    assert d["e2e"]["value"] == d["value"] and d["e2e"]["unit"] == d["unit"]
+    assert d["parity"]["golden_match"] is True       # the reference's product is the committed digest
 
 
 def _rank_dies(rank: int, port: int, q):
